@@ -1,0 +1,231 @@
+/* splatkit-b200: the C ABI of the B200 splat frame pipeline.
+ *
+ * The entry points mirror the reference's renderer surface, splatkit::SplatRenderer
+ * (packages/splatkit-engine/include/splatkit/rendering/SplatRenderer.h:36-160), and the
+ * components its GPU tests drive directly (MetalVisibilityPass, MetalRadixSort,
+ * MetalLodSelection). Plain C types only: host arrays are caller-owned and only read during a
+ * call; device pointers (sk_*_device entry points) are CUDA device addresses the caller owns.
+ *
+ * Threading: one context per host thread for render calls ("render thread only",
+ * SplatRenderer.h:32). sk_get_stats may be called from any thread.
+ *
+ * Errors: every call returns an sk_status. After a CUDA error the context latches failed and
+ * every later call returns SK_E_DEVICE (MetalFrameLoop's failure latch,
+ * splatkit-ios/.../metal/presentation/MetalFrameLoop.h:51-55). sk_last_error gives the text.
+ * A failed upload keeps the previous world (SplatRenderer.h:85-87).
+ */
+#ifndef SPLATKIT_B200_H
+#define SPLATKIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t sk_status;
+#define SK_OK 0
+#define SK_E_INVALID 1     /* bad argument, range or world; nothing was changed */
+#define SK_E_OOM 2         /* device allocation failed; the previous state is kept */
+#define SK_E_ADMISSION 3   /* a request does not fit the memory budget */
+#define SK_E_DEVICE 4      /* CUDA error; the context is latched failed */
+#define SK_E_TIMEOUT 5     /* a bounded device wait gave up (the frame is wrong) */
+#define SK_E_UNSUPPORTED 6 /* a feature this build leaves out */
+#define SK_E_NO_WORLD 7    /* no world uploaded */
+
+#define SK_FORMAT_RGBA8 0   /* 4 bytes per pixel, row 0 on top */
+#define SK_FORMAT_RGBA32F 1 /* 16 bytes per pixel, row 0 on top */
+#define SK_FORMAT_BGRA8 2   /* the reference's capture layout (MetalFrameCaptureTest.mm:57) */
+
+typedef struct sk_context sk_context;
+
+typedef struct {
+  int32_t device;                /* CUDA device ordinal */
+  uint32_t width, height;        /* draw extent of the headless target */
+  int32_t image_format;          /* SK_FORMAT_RGBA8 or SK_FORMAT_RGBA32F on the device */
+  uint32_t time_stages;          /* 1: record per-stage CUDA events (stats); 0: none */
+} sk_config;
+
+/* A SplatCloud (packages/splat-core/include/splat/formats/SplatCloud.h:30-51), structure of
+ * arrays: count positions (xyz), covariances (xx, xy, xz, yy, yz, zz), colours (rgb in [0,1]),
+ * alphas, and for sh_degree > 0, 3 * ((d+1)^2 - 1) harmonics floats per splat, channel fastest. */
+typedef struct {
+  const float* positions;
+  const float* covariances;
+  const float* colors;
+  const float* alphas;
+  const float* sh;
+  uint32_t count;
+  int32_t sh_degree;
+} sk_cloud_view;
+
+/* LodNode (packages/splat-core/include/splat/lod/LodTree.h:13-23), 24 bytes. */
+typedef struct {
+  float position[3];
+  float size;
+  uint32_t child_start;
+  uint32_t child_count;
+} sk_lod_node;
+
+/* LodCluster (LodTree.h:28-35), 64 bytes. */
+typedef struct {
+  float center[3], radius;
+  float extent[3], error;
+  float color_variance, opacity;
+  uint32_t node, child_start, child_count, leaf_start, leaf_count, subtree_leaves;
+} sk_lod_cluster;
+
+/* A LodTree (LodTree.h:47-55): the nodes as a cloud in layout order, the BFS layout, and the
+ * selection data (clusters + leaf references). cluster_count 0: the selection data is built
+ * at upload (MetalLodSelection.mm:68-74). */
+typedef struct {
+  sk_cloud_view nodes;
+  const sk_lod_node* layout;
+  uint32_t node_count;
+  uint32_t leaf_count;
+  const sk_lod_cluster* clusters;
+  uint32_t cluster_count;
+  const uint32_t* leaves;
+  uint32_t leaf_ref_count;
+} sk_lod_view;
+
+typedef struct {
+  uint32_t offset;
+  uint32_t count;
+} sk_range;
+
+/* SplatRenderer::Frame (SplatRenderer.h:111-131) for the GPU order source. */
+typedef struct {
+  float view[16];  /* column major */
+  float proj[16];  /* [0,1] depth perspective (Mat4::perspective) */
+  float camera_position[3];
+  float reveal_level; /* +inf when idle */
+  const sk_range* ranges;
+  uint32_t range_count;
+  int32_t sh_degree; /* capped by the world */
+} sk_frame;
+
+/* RenderPolicy (packages/splatkit-engine/include/splatkit/rendering/RenderPolicy.h:17-40). */
+typedef struct {
+  float lod_error_pixels;
+  uint32_t lod_splat_limit;
+  float alpha_threshold;
+  float subpixel_threshold;
+  uint32_t enable_frustum_culling;
+  uint32_t enable_early_termination;
+  uint32_t sort_depth_bits; /* 16 or 32 */
+  double background[3];
+} sk_policy;
+
+/* DeviceCapabilities (RenderPolicy.h:42-62), the fields this backend reports. */
+typedef struct {
+  uint32_t max_lod_capacity_splats;
+  uint32_t min_residency_capacity_splats;
+  uint32_t max_residency_capacity_splats;
+  uint32_t supports_subgroups;
+  uint32_t max_texture_dimension;
+  uint32_t sorts_on_gpu;
+  uint32_t selects_lod_on_gpu;
+  uint64_t total_memory;
+} sk_capabilities;
+
+/* Frame statistics: the SplatRenderer getters (SplatRenderer.h:135-149) plus counters. */
+typedef struct {
+  uint64_t submitted_frames;
+  uint64_t completed_frames;
+  double gpu_ms;     /* whole frame */
+  double select_ms;  /* LOD cut */
+  double cull_ms;    /* visibility */
+  double sort_ms;    /* depth sort */
+  double bin_ms;     /* binning + tile sort */
+  double composite_ms;
+  uint32_t draw_count;     /* survivors of the cull */
+  uint32_t selected_count; /* LOD cut size */
+  uint32_t lod_limited;
+  uint32_t lod_evaluated;
+  uint32_t instances;      /* tile instances */
+  uint32_t device_error;   /* SK_DEVERR bits of the last frame */
+  uint64_t fragments;      /* blended pixel x splat pairs */
+  float lod_pixels;        /* the adapted LOD threshold in use */
+  uint32_t pad;
+} sk_stats;
+
+/* ---- context (SplatRenderer lifetime, deviceCapabilities, applyRenderPolicy) ---------- */
+sk_status sk_create(const sk_config* config, sk_context** out);
+void sk_destroy(sk_context* ctx);
+const char* sk_last_error(const sk_context* ctx);
+sk_status sk_resize(sk_context* ctx, uint32_t width, uint32_t height);         /* drawExtent */
+sk_status sk_device_capabilities(sk_context* ctx, sk_capabilities* out);        /* :56 */
+sk_status sk_apply_render_policy(sk_context* ctx, const sk_policy* policy);     /* :62 */
+void sk_default_policy(sk_policy* out);                                         /* RenderPolicy{} */
+sk_status sk_available_memory(sk_context* ctx, uint64_t* bytes);                /* :70 */
+int32_t sk_gpu_failed(sk_context* ctx);                                         /* :74 */
+
+/* ---- worlds (SplatRenderer.h:85-97) ----------------------------------------------- */
+sk_status sk_upload_world(sk_context* ctx, const sk_cloud_view* cloud, int32_t max_sh_degree);
+sk_status sk_upload_lod_world(sk_context* ctx, const sk_lod_view* tree, int32_t max_sh_degree,
+                              uint32_t budget);
+sk_status sk_create_slab(sk_context* ctx, uint32_t capacity, int32_t sh_degree);
+sk_status sk_upload_tile(sk_context* ctx, uint32_t offset, const sk_cloud_view* cloud);
+sk_status sk_world_info(sk_context* ctx, uint32_t* count, int32_t* sh_degree);
+
+/* ---- the frame (SplatRenderer::draw, :134) ------------------------------------------- */
+/* Enqueues LOD cut, cull, sort, binning and composite; returns without waiting. */
+sk_status sk_draw(sk_context* ctx, const sk_frame* frame);
+/* Waits for the last frame and copies its image (captureNextFrame). */
+sk_status sk_read_image(sk_context* ctx, void* host, size_t bytes, int32_t format);
+sk_status sk_wait_idle(sk_context* ctx);
+sk_status sk_get_stats(sk_context* ctx, sk_stats* out);
+
+/* Readbacks of the last frame for parity checks: the survivors in source order (keys and
+ * 32-byte projected records), the depth order (indices into the projected records) and the
+ * LOD cut. Each returns the element count in *count and copies min(count, capacity). */
+sk_status sk_read_visible(sk_context* ctx, uint32_t* keys, void* projected, uint32_t capacity,
+                          uint32_t* count);
+sk_status sk_read_order(sk_context* ctx, uint32_t* order, uint32_t capacity, uint32_t* count);
+sk_status sk_read_cut(sk_context* ctx, uint32_t* indices, uint32_t capacity, uint32_t* count,
+                      uint32_t* lod_counters6);
+
+/* ---- component operators over caller device memory ----------------------------------- */
+/* MetalRadixSort (splatkit-ios/.../metal/sort/MetalRadixSort.h:13-54): stable ascending argsort
+ * of min(*d_count, capacity) keys (d_count is a device word), 16 or 32 bits; d_keys is left
+ * unchanged; d_order receives the key positions in sorted order. d_workspace holds
+ * sk_sort_workspace_bytes(capacity) device bytes; calls on one workspace must be
+ * stream-ordered. d_error (device word) receives SK_DEVERR bits. stream: a cudaStream_t. */
+size_t sk_sort_workspace_bytes(uint32_t capacity);
+sk_status sk_radix_argsort_device(const uint32_t* d_keys, const uint32_t* d_count,
+                                  uint32_t capacity, int32_t bits, uint32_t* d_order,
+                                  void* d_workspace, size_t workspace_bytes, uint32_t* d_error,
+                                  void* stream);
+
+/* ---- host-side world preparation (no device needed) ----------------------------------- */
+/* Harmonics words per splat in the device layout: the reference's packed stride
+ * (GpuLayout.cpp:66-70) rounded up to whole 16-byte groups. */
+uint32_t sk_sh_device_stride(int32_t degree);
+/* packSplatRange (splatkit-engine/src/rendering/GpuLayout.cpp:122-137): records
+ * [offset, offset + count) of the cloud as 32-byte GpuSplat records. */
+sk_status sk_pack_splats(const sk_cloud_view* cloud, uint32_t offset, uint32_t count, void* out);
+/* packShRange float16 (GpuLayout.cpp:92-113) at `stride` words per splat (>= packed stride). */
+sk_status sk_pack_sh(const sk_cloud_view* cloud, int32_t degree, uint32_t offset, uint32_t count,
+                     uint32_t* out, uint32_t stride);
+/* buildLodSelectionData (splat-core/src/lod/LodSelection.cpp:47-133). Pass null outputs to
+ * learn the counts first. */
+sk_status sk_build_lod_selection(const sk_lod_view* tree, sk_lod_cluster* clusters,
+                                 uint32_t cluster_capacity, uint32_t* cluster_count,
+                                 uint32_t* leaves, uint32_t leaf_capacity, uint32_t* leaf_count);
+/* The deepest node depth of a BFS-laid-out tree (validateLodTree's value,
+ * splat-core/src/lod/LodFile.cpp:336-344), or -1 when the topology is invalid. */
+int64_t sk_lod_depth(const sk_lod_node* layout, uint32_t node_count, uint32_t leaf_count);
+/* gpuWorldBytes (GpuLayout.cpp:72-77): the device bytes a world of this shape is priced at. */
+uint64_t sk_world_bytes(uint64_t records, int32_t sh_degree, uint64_t draw_capacity,
+                        uint64_t clusters, uint64_t leaf_refs);
+/* LodThreshold::update (splatkit-engine/include/splatkit/rendering/LodThreshold.h:27-36) on
+ * state[0] = policy pixels, state[1] = current pixels; returns the new threshold. */
+float sk_lod_threshold_update(float* state, uint32_t selected, uint32_t limited, uint32_t limit);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPLATKIT_B200_H */

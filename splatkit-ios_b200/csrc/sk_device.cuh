@@ -1,0 +1,199 @@
+// Device-side building blocks shared by the splat kernels: records, the per-view camera,
+// IEEE helpers, the project's own binary16 conversion and natural log, and the decoupled
+// look-back used by every order-preserving scan (visibility compaction, radix scatter,
+// tile binning, LOD rounds).
+//
+// Bit-exactness contract: the cull/projection and LOD kernels are compiled with -fmad=false
+// and IEEE divide/sqrt, and every expression keeps the operand order written here, so each
+// product and sum rounds on its own. The composite kernel does its coverage decision with
+// explicit __fmul_rn/__fadd_rn intrinsics for the same reason.
+#pragma once
+#include <cstdint>
+
+#include "sk_layout.h"
+
+namespace sk {
+
+// ---- bit casts -------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t asU(float f) { return __float_as_uint(f); }
+__device__ __forceinline__ float asF(uint32_t u) { return __uint_as_float(u); }
+
+__device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t lanemaskLt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// ---- binary16, round to nearest even, saturating to 65504, NaN kept -----------------
+// The reference's float -> half packing rule (splat-core/include/splat/math/Half.h:12-38),
+// written from the IEEE encodings.
+__device__ __forceinline__ uint32_t floatToHalf(float v) {
+  const uint32_t x = asU(v);
+  const uint32_t sign = (x >> 16) & 0x8000u;
+  const uint32_t ax = x & 0x7fffffffu;
+  const uint32_t e = ax >> 23;
+  const uint32_t mant = ax & 0x7fffffu;
+  if (e == 0xffu) return sign | (mant ? 0x7e00u : 0x7bffu);
+  if (e < 113u) {
+    const uint32_t shift = 126u - e;
+    if (shift > 24u) return sign;
+    const uint32_t full = mant | 0x800000u;
+    const uint32_t h = full >> shift;
+    const uint32_t rem = full & ((1u << shift) - 1u);
+    const uint32_t mid = 1u << (shift - 1u);
+    const uint32_t up = (rem > mid || (rem == mid && (h & 1u))) ? 1u : 0u;
+    return sign | (h + up);
+  }
+  uint32_t h = ((e - 112u) << 10) | (mant >> 13);
+  const uint32_t rem = mant & 0x1fffu;
+  if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) ++h;
+  if (h >= 0x7c00u) h = 0x7bffu;
+  return sign | h;
+}
+
+__device__ __forceinline__ float halfToFloat(uint32_t h) {
+  const uint32_t sign = (h & 0x8000u) << 16;
+  const uint32_t e = (h >> 10) & 0x1fu;
+  const uint32_t m = h & 0x3ffu;
+  if (e == 0) return asF(asU(__fmul_rn(static_cast<float>(m), 5.9604644775390625e-08f)) | sign);
+  if (e == 31) return asF(sign | 0x7f800000u | (m << 13));
+  return asF(sign | ((e + 112u) << 23) | (m << 13));
+}
+
+__device__ __forceinline__ float lowHalf(uint32_t w) { return halfToFloat(w & 0xffffu); }
+__device__ __forceinline__ float highHalf(uint32_t w) { return halfToFloat(w >> 16); }
+__device__ __forceinline__ uint32_t packHalf2(float lo, float hi) {
+  return floatToHalf(lo) | (floatToHalf(hi) << 16);
+}
+__device__ __forceinline__ float halfRound(float v) { return halfToFloat(floatToHalf(v)); }
+
+// ---- natural log ----------------------------------------------------------------------
+// Exponent/mantissa reduction to m in (sqrt(1/2), sqrt(2)], ln m = 2 atanh((m-1)/(m+1))
+// (Abramowitz & Stegun 4.1.27) summed as f - s (f - R), and ln 2 split in a 16-bit head and
+// a tail (Cody & Waite). Only rounded multiplies, adds and one IEEE divide: identical on the
+// host and here. Within 1 ulp of the true log over the range the cull uses.
+__device__ __forceinline__ float lnF32(float x) {
+  if (x != x) return x;
+  if (x < 0.0f) return __int_as_float(0x7fc00000);
+  if (x == 0.0f) return -__int_as_float(0x7f800000);
+  if (x == __int_as_float(0x7f800000)) return x;
+  uint32_t bits = asU(x);
+  int e = 0;
+  if (bits < 0x00800000u) {
+    x = __fmul_rn(x, 8388608.0f);
+    bits = asU(x);
+    e = -23;
+  }
+  e += static_cast<int>(bits >> 23) - 127;
+  uint32_t mb = (bits & 0x007fffffu) | 0x3f800000u;
+  if (mb > 0x3fb504f3u) {
+    mb -= 0x00800000u;
+    e += 1;
+  }
+  const float m = asF(mb);
+  const float f = __fsub_rn(m, 1.0f);
+  const float s = __fdiv_rn(f, __fadd_rn(2.0f, f));
+  const float z = __fmul_rn(s, s);
+  float r = 0.15384615384615385f;
+  r = __fadd_rn(__fmul_rn(r, z), 0.18181818181818182f);
+  r = __fadd_rn(__fmul_rn(r, z), 0.22222222222222222f);
+  r = __fadd_rn(__fmul_rn(r, z), 0.2857142857142857f);
+  r = __fadd_rn(__fmul_rn(r, z), 0.4f);
+  r = __fadd_rn(__fmul_rn(r, z), 0.6666666666666666f);
+  r = __fmul_rn(r, z);
+  const float lnm = __fsub_rn(f, __fmul_rn(s, __fsub_rn(f, r)));
+  const float fe = static_cast<float>(e);
+  return __fadd_rn(__fmul_rn(fe, 0.693145751953125f),
+                   __fadd_rn(lnm, __fmul_rn(fe, 1.428606820309417e-06f)));
+}
+
+// ---- decoupled look-back ----------------------------------------------------------------
+// A status word is [epoch:30 | flag:2 | value:32]. flag 1: the tile's own aggregate; flag 2:
+// its inclusive prefix. Each launch uses a fresh epoch, so words left by earlier launches read
+// as "not ready" and the status array never needs clearing. Every wait is bounded: after
+// kSpinLimit polls the kernel records SK_DEVERR_LOOKBACK in the error word and carries on,
+// so a lost predecessor costs a wrong frame and an error status, never a hung GPU.
+constexpr uint32_t kFlagAggregate = 1u;
+constexpr uint32_t kFlagPrefix = 2u;
+constexpr uint32_t kSpinLimit = 1u << 21;
+
+__device__ __forceinline__ uint64_t makeStatus(uint32_t epoch, uint32_t flag, uint32_t value) {
+  return (static_cast<uint64_t>(epoch) << 34) | (static_cast<uint64_t>(flag) << 32) | value;
+}
+__device__ __forceinline__ void storeStatus(uint64_t* p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t loadStatus(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits (bounded) until `p` holds a word of this epoch; returns it, or an aggregate of 0 with
+// the error recorded when the wait gives up.
+__device__ __forceinline__ uint64_t waitStatus(const uint64_t* p, uint32_t epoch,
+                                               uint32_t* error) {
+  for (uint32_t spin = 0; spin < kSpinLimit; ++spin) {
+    const uint64_t w = loadStatus(p);
+    if (static_cast<uint32_t>(w >> 34) == (epoch & 0x3fffffffu) && ((w >> 32) & 3u) != 0u) return w;
+    if (spin > 64) __nanosleep(64);
+  }
+  atomicOr(error, SK_DEVERR_LOOKBACK);
+  return makeStatus(epoch, kFlagPrefix, 0u);
+}
+
+// Look-back for one running sum, done by one warp: returns the exclusive prefix of `tile`.
+// Lane i inspects predecessor (start - i); the window moves back 32 tiles at a time until a
+// predecessor's inclusive prefix is found. All lanes return the same value.
+__device__ __forceinline__ uint32_t warpLookback(const uint64_t* status, uint32_t tile,
+                                                 uint32_t epoch, uint32_t* error) {
+  uint32_t exclusive = 0;
+  int start = static_cast<int>(tile) - 1;
+  const uint32_t lane = laneId();
+  while (start >= 0) {
+    const int j = start - static_cast<int>(lane);
+    uint64_t w = 0;
+    if (j >= 0) w = waitStatus(status + j, epoch, error);
+    const uint32_t flag = j >= 0 ? static_cast<uint32_t>((w >> 32) & 3u) : kFlagPrefix;
+    const uint32_t value = j >= 0 ? static_cast<uint32_t>(w) : 0u;
+    const uint32_t prefixMask = __ballot_sync(0xffffffffu, flag == kFlagPrefix);
+    // the nearest predecessor holding a prefix closes the window
+    const uint32_t stop = prefixMask ? (__ffs(prefixMask) - 1) : 32u;
+    uint32_t mine = lane <= stop ? value : 0u;
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    exclusive += mine;
+    if (prefixMask) break;
+    start -= 32;
+  }
+  return exclusive;
+}
+
+// The dynamic tile index: tiles are handed out in the order blocks start, which is what makes
+// waiting on a lower tile safe. The last block to finish resets both counters for the next
+// launch on this stream (no spin: a plain arrival count).
+__device__ __forceinline__ uint32_t takeTile(uint32_t* counters) {
+  __shared__ uint32_t tile;
+  if (threadIdx.x == 0) tile = atomicAdd(&counters[0], 1u);
+  __syncthreads();
+  return tile;
+}
+// Returns true in the block that arrived last (after every other block finished its writes).
+__device__ __forceinline__ bool finishTile(uint32_t* counters) {
+  __shared__ uint32_t last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const uint32_t arrived = atomicAdd(&counters[1], 1u);
+    last = arrived == gridDim.x - 1 ? 1u : 0u;
+    if (last) {
+      counters[0] = 0;
+      counters[1] = 0;
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return last != 0u;
+}
+
+}  // namespace sk

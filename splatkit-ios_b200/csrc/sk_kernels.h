@@ -1,0 +1,135 @@
+// Kernel launch interfaces (host side). Each launcher enqueues on `stream` and returns the
+// launch status; none synchronises. Sizes that only the GPU knows (survivor count, instance
+// count, LOD cut size) are passed as device pointers and every grid is sized by a host-known
+// capacity, so a whole frame enqueues without a host round trip.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "sk_layout.h"
+
+namespace sk {
+
+// ---- visibility (visibility.cu) --------------------------------------------------------
+struct VisibilityArgs {
+  const GpuSplat* splats;
+  const uint32_t* sh;  // device stride shDeviceStride(degree) words per splat
+  uint32_t worldCount;
+  const Range* ranges;  // ranges mode
+  const uint32_t* rangeStarts;
+  uint32_t rangeCount;
+  const uint32_t* indices;     // indexed (LOD) mode
+  const uint32_t* indexCount;  // indexed mode: entries in indices (device)
+  uint32_t total;              // ranges mode: sum of counts; indexed mode: capacity bound
+  uint32_t* keys;
+  Projected* projected;
+  uint32_t* visibleCount;
+  uint64_t* status;    // one word per 1024-splat tile
+  uint32_t* counters;  // two words
+  uint32_t epoch;
+  uint32_t* error;
+};
+uint32_t visibilityTileSplats();
+cudaError_t launchVisibility(const Camera& cam, const VisibilityArgs& args, int shDegree,
+                             bool key16, bool indexed, cudaStream_t stream);
+
+// ---- radix sort (radix_sort.cu) --------------------------------------------------------
+// Stable ascending sort of `count` (key, value) pairs with 8-bit digits: one histogram pass,
+// then one onesweep scatter pass per digit. valuesIn null: values are the key positions.
+// keysIn is left untouched; keysOut (optional) receives the sorted keys.
+struct SortArgs {
+  const uint32_t* keysIn;
+  const uint32_t* valuesIn;
+  uint32_t* keysOut;
+  uint32_t* valuesOut;
+  const uint32_t* count;  // device
+  uint32_t capacity;      // count is clamped to this
+  int bits;               // 16 or 32
+  // workspace (sortWorkspaceBytes)
+  uint32_t* keysA;
+  uint32_t* keysB;
+  uint32_t* valuesTmp;
+  uint32_t* histogram;  // 2 * 4 * 256 words
+  uint64_t* status;     // sortTiles(capacity) * 256 words
+  uint32_t* counters;   // 2 * 5 words
+  uint32_t epoch;       // uses epoch .. epoch + 3
+  uint32_t* error;
+};
+uint32_t sortTileKeys();
+size_t sortWorkspaceBytes(uint32_t capacity);
+// Carves the workspace into the SortArgs fields.
+void sortBindWorkspace(SortArgs& args, void* workspace, uint32_t capacity);
+cudaError_t launchSort(const SortArgs& args, cudaStream_t stream);
+// Clears the counters and histogram accumulators of a bound workspace.
+cudaError_t sortResetWorkspace(const SortArgs& args, cudaStream_t stream);
+
+// ---- tile binning (binning.cu) ---------------------------------------------------------
+struct BinArgs {
+  const Projected* projected;
+  const uint32_t* order;  // depth order (indices into projected)
+  const uint32_t* count;  // survivors (device)
+  uint32_t capacity;      // bound on count
+  uint32_t width, height, tilesX, tilesY;
+  uint32_t* instanceKeys;    // tile id per instance
+  uint32_t* instanceValues;  // projected index per instance
+  uint32_t instanceCapacity;
+  uint32_t* instanceCount;  // FrameCounters.instances
+  uint32_t* overflow;       // FrameCounters.overflow
+  uint64_t* status;
+  uint32_t* counters;
+  uint32_t epoch;
+  uint32_t* error;
+};
+cudaError_t launchBinning(const BinArgs& args, cudaStream_t stream);
+
+// Tile [start, end) ranges from the tile-sorted instance keys. ranges: tilesX * tilesY uint2,
+// cleared by the launcher.
+cudaError_t launchTileRanges(const uint32_t* sortedKeys, const uint32_t* instanceCount,
+                             uint32_t instanceCapacity, uint2* ranges, uint32_t tiles,
+                             cudaStream_t stream);
+
+// ---- composite (composite.cu) ----------------------------------------------------------
+enum PixelFormat : int { kRgba8 = 0, kRgba32f = 1 };
+struct CompositeArgs {
+  const Projected* projected;
+  const uint32_t* values;  // tile-sorted projected indices
+  const uint2* ranges;
+  uint32_t width, height, tilesX, tilesY;
+  float background[3];
+  int opaque;
+  float cutoff;  // transmittance below which a pixel stops
+  void* image;   // row 0 on top
+  int format;
+  uint32_t* fragments;  // FrameCounters.fragments_lo/hi (64-bit add)
+};
+cudaError_t launchComposite(const CompositeArgs& args, cudaStream_t stream);
+
+// ---- LOD selection (lod.cu) ------------------------------------------------------------
+struct LodArgs {
+  const LodCluster* clusters;
+  const uint32_t* leaves;
+  uint32_t clusterCount;
+  uint32_t capacity;  // indices buffer size and the guard's bound
+  uint32_t limit;     // splats one selection may emit (<= capacity)
+  float pixelLimit;
+  float colorWeight;
+  uint32_t cull;
+  uint32_t rounds;
+  uint32_t frontierCapacity;
+  uint32_t* frontier[2];
+  uint2* costs;     // (extra | flags, exclusive prefix of extra)
+  uint4* offsets;   // (kids, splats, packets exclusive, flags)
+  uint4* packets;   // (leafStart, count, destination, 1)
+  uint32_t* indices;
+  LodState* state;
+  uint64_t* status;  // 3 arrays of lodTiles(frontierCapacity) words
+  uint32_t* counters;
+  uint32_t epoch;  // uses epoch .. epoch + 2 * rounds
+  uint32_t* error;
+  uint32_t* report;  // six words copied from the state at the end (FrameCounters.lod)
+};
+uint32_t lodTileClusters();
+cudaError_t launchLodSelect(const Camera& cam, const LodArgs& args, cudaStream_t stream);
+
+}  // namespace sk

@@ -1,0 +1,358 @@
+// The visibility pass: per splat, reveal clip, opacity cut, view transform, near/far test,
+// 2D covariance, ellipse axes, quad radius, edge margin, sub-pixel cut, SH colour and depth
+// key; survivors compacted in SOURCE order.
+//
+// Follows splatkit-ios/Sources/SplatKitCore/rendering/metal/layout/SplatProjection.metalh:6-141
+// and .../metal/cull/SplatVisibility.metal:16-106. The reference compacts with one atomic per
+// SIMD group, so its survivor order depends on scheduling; here each 1024-splat tile counts
+// its survivors, takes its offset by decoupled look-back and writes them in source order, so
+// the sorted order downstream is deterministic and equal to a stable sort of (key, source
+// position).
+//
+// Built with -fmad=false: every product and sum rounds on its own, in the order written.
+#include <cuda_runtime.h>
+
+#include "sk_device.cuh"
+#include "sk_kernels.h"
+
+namespace sk {
+namespace {
+
+constexpr float kQuadMinAlpha = 2.0f / 255.0f;
+constexpr float kBoundsRadius = 2.5f;
+constexpr float kLodBoundsRadius = 5.0f;
+constexpr float kMaxPixelRadius = 512.0f;
+constexpr float kLowPassVariance = 0.3f;
+constexpr float kProjectionFovClamp = 1.3f;
+constexpr uint32_t kDepthKeyShift = 11;
+constexpr uint32_t kDepthKeyMax = 65535;
+
+constexpr uint32_t kThreads = 256;
+constexpr uint32_t kItems = 4;
+constexpr uint32_t kTileSplats = kThreads * kItems;
+
+__device__ __forceinline__ void mulPoint(const float* m, float x, float y, float z, float w,
+                                         float* o) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r) o[r] = ((m[r] * x + m[4 + r] * y) + m[8 + r] * z) + m[12 + r] * w;
+}
+
+template <int D>
+struct ShWords {
+  static constexpr uint32_t kWords = shDeviceStride(D);
+  uint32_t w[kWords > 0 ? kWords : 1];
+  __device__ __forceinline__ void load(const uint32_t* sh, uint32_t index) {
+    if constexpr (kWords > 0) {
+      const uint4* p = reinterpret_cast<const uint4*>(sh + static_cast<size_t>(index) * kWords);
+#pragma unroll
+      for (uint32_t i = 0; i < kWords / 4; ++i) {
+        const uint4 v = __ldg(p + i);
+        w[i * 4 + 0] = v.x, w[i * 4 + 1] = v.y, w[i * 4 + 2] = v.z, w[i * 4 + 3] = v.w;
+      }
+    }
+  }
+  __device__ __forceinline__ float at(uint32_t k, uint32_t ch) const {
+    const uint32_t h = k * 3u + ch;
+    return (h & 1u) ? highHalf(w[h >> 1]) : lowHalf(w[h >> 1]);
+  }
+};
+
+// SplatProjection.metalh:50-76, summed in the order the oracle writes.
+template <int D>
+__device__ __forceinline__ void shColor(const ShWords<D>& s, float x, float y, float z,
+                                        float* rgb) {
+  const float C1 = 0.4886025119f;
+  const float b0 = (-C1) * y, b1 = C1 * z, b2 = C1 * x;
+  float q3 = 0, q4 = 0, q5 = 0, q6 = 0, q7 = 0;
+  float q8 = 0, q9 = 0, q10 = 0, q11 = 0, q12 = 0, q13 = 0, q14 = 0;
+  if constexpr (D >= 2) {
+    const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+    q3 = 1.0925484306f * xy;
+    q4 = -1.0925484306f * yz;
+    q5 = 0.3153915653f * (((2.0f * zz) - xx) - yy);
+    q6 = -1.0925484306f * xz;
+    q7 = 0.5462742153f * (xx - yy);
+    if constexpr (D >= 3) {
+      q8 = (-0.5900435899f * y) * ((3.0f * xx) - yy);
+      q9 = (2.8906114426f * xy) * z;
+      q10 = (-0.4570457995f * y) * (((4.0f * zz) - xx) - yy);
+      q11 = (0.3731763326f * z) * (((2.0f * zz) - (3.0f * xx)) - (3.0f * yy));
+      q12 = (-0.4570457995f * x) * (((4.0f * zz) - xx) - yy);
+      q13 = (1.4453057213f * z) * (xx - yy);
+      q14 = (-0.5900435899f * x) * (xx - (3.0f * yy));
+    }
+  }
+#pragma unroll
+  for (uint32_t ch = 0; ch < 3; ++ch) {
+    float c = (b0 * s.at(0, ch) + b1 * s.at(1, ch)) - b2 * s.at(2, ch);
+    if constexpr (D >= 2) {
+      const float s2 =
+          (((q3 * s.at(3, ch) + q4 * s.at(4, ch)) + q5 * s.at(5, ch)) + q6 * s.at(6, ch)) +
+          q7 * s.at(7, ch);
+      c = c + s2;
+      if constexpr (D >= 3) {
+        const float s3 = (((((q8 * s.at(8, ch) + q9 * s.at(9, ch)) + q10 * s.at(10, ch)) +
+                            q11 * s.at(11, ch)) +
+                           q12 * s.at(12, ch)) +
+                          q13 * s.at(13, ch)) +
+                         q14 * s.at(14, ch);
+        c = c + s3;
+      }
+    }
+    rgb[ch] = c;
+  }
+}
+
+// SplatProjection.metalh:78-141 and SplatVisibility.metal:86-92. Writes the 8 words of a
+// Projected record and the depth key; returns whether the splat survives.
+template <int D, bool kKey16>
+__device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, const uint4 hi,
+                                             uint32_t index, const uint32_t* sh,
+                                             uint32_t& key, uint32_t* out) {
+  const float px = asF(lo.x), py = asF(lo.y), pz = asF(lo.z);
+  const uint32_t rgba8 = lo.w;
+  const uint32_t cov0 = hi.x, cov1 = hi.y, cov2 = hi.z, lodAlpha = hi.w;
+  if (!(cam.reveal[0] - py >= 0.0f)) return false;
+  const float ca = static_cast<float>(rgba8 >> 24) / 255.0f;
+  const float alpha = lodAlpha != 0u ? asF(lodAlpha) : ca;
+  if (alpha < kQuadMinAlpha) return false;
+
+  float v[4];
+  mulPoint(cam.view, px, py, pz, 1.0f, v);
+  if (v[2] >= 0.0f) return false;
+  float clip[4];
+  mulPoint(cam.proj, v[0], v[1], v[2], v[3], clip);
+  if (clip[2] < 0.0f || clip[2] > clip[3]) return false;
+  if (clip[3] <= cam.proj[14] / cam.proj[10]) return false;
+
+  // projectCovariance (SplatProjection.metalh:6-24)
+  const float vz = v[2];
+  const float invZ = 1.0f / vz;
+  const float invZ2 = invZ * invZ;
+  const float limX = kProjectionFovClamp * cam.tanHalfFov[0];
+  const float limY = kProjectionFovClamp * cam.tanHalfFov[1];
+  const float vx = fminf(fmaxf(v[0] * invZ, -limX), limX) * vz;
+  const float vy = fminf(fmaxf(v[1] * invZ, -limY), limY) * vz;
+  const float fx = cam.focal[0], fy = cam.focal[1];
+  const float j00 = fx * invZ;
+  const float j11 = fy * invZ;
+  const float j02 = ((-fx) * vx) * invZ2;
+  const float j12 = ((-fy) * vy) * invZ2;
+  float t0[3], t1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    t0[c] = j00 * cam.view[c * 4 + 0] + j02 * cam.view[c * 4 + 2];
+    t1[c] = j11 * cam.view[c * 4 + 1] + j12 * cam.view[c * 4 + 2];
+  }
+  const float xx = lowHalf(cov0), xy = highHalf(cov0), xz = lowHalf(cov1);
+  const float yy = highHalf(cov1), yz = lowHalf(cov2), zz = highHalf(cov2);
+  const float V[3][3] = {{xx, xy, xz}, {xy, yy, yz}, {xz, yz, zz}};
+  float m0[3], m1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    m0[c] = (t0[0] * V[0][c] + t0[1] * V[1][c]) + t0[2] * V[2][c];
+    m1[c] = (t1[0] * V[0][c] + t1[1] * V[1][c]) + t1[2] * V[2][c];
+  }
+  const float ca2 = ((m0[0] * t0[0] + m0[1] * t0[1]) + m0[2] * t0[2]) + kLowPassVariance;
+  const float cb2 = (m1[0] * t0[0] + m1[1] * t0[1]) + m1[2] * t0[2];
+  const float cd2 = ((m1[0] * t1[0] + m1[1] * t1[1]) + m1[2] * t1[2]) + kLowPassVariance;
+
+  // ellipseAxes (SplatProjection.metalh:26-37)
+  const float det = ca2 * cd2 - cb2 * cb2;
+  const float mean = 0.5f * (ca2 + cd2);
+  const float dist = fmaxf(0.1f, sqrtf(fmaxf(mean * mean - det, 0.0f)));
+  const float lambda1 = mean + dist;
+  const float lambda2 = mean - dist;
+  float e1x, e1y;
+  if (cb2 == 0.0f) {
+    e1x = (ca2 > cd2) ? 1.0f : 0.0f;
+    e1y = (ca2 > cd2) ? 0.0f : 1.0f;
+  } else {
+    const float nx = cb2, ny = cd2 - lambda2;
+    const float len = sqrtf(nx * nx + ny * ny);
+    e1x = nx / len;
+    e1y = ny / len;
+  }
+  const float s1 = sqrtf(lambda1);
+  const float s2 = sqrtf(fmaxf(lambda2, 0.0f));
+  const float a1x = e1x * s1, a1y = e1y * s1;
+  const float a2x = e1y * s2, a2y = (-e1x) * s2;
+
+  float radius = fminf(lodAlpha != 0u ? kLodBoundsRadius : kBoundsRadius,
+                       sqrtf(2.0f * lnF32(fmaxf(alpha / kQuadMinAlpha, 1.0f))));
+  const float sigmaPixels = sqrtf(fmaxf(a1x * a1x + a1y * a1y, a2x * a2x + a2y * a2y));
+  radius = fminf(radius, kMaxPixelRadius / fmaxf(sigmaPixels, 1e-6f));
+
+  const uint32_t axis1 = packHalf2(a1x, a1y);
+  const uint32_t axis2 = packHalf2(a2x, a2y);
+  const float extX = radius * (fabsf(lowHalf(axis1)) + fabsf(lowHalf(axis2)));
+  const float extY = radius * (fabsf(highHalf(axis1)) + fabsf(highHalf(axis2)));
+  const float marginX = (((extX + 0.5f) * 2.0f) * clip[3]) / cam.screenSize[0];
+  const float marginY = (((extY + 0.5f) * 2.0f) * clip[3]) / cam.screenSize[1];
+  if (fabsf(clip[0]) > clip[3] + marginX || fabsf(clip[1]) > clip[3] + marginY) return false;
+
+  const float halfDifference = 0.5f * (ca2 - cd2);
+  const float sourceVariance =
+      (0.5f * (ca2 + cd2) + sqrtf(fmaxf(halfDifference * halfDifference + cb2 * cb2, 0.0f))) -
+      kLowPassVariance;
+  if (!(sqrtf(fmaxf(sourceVariance, 0.0f)) * radius >= cam.minPixelRadius)) return false;
+
+  const float depth = -v[2];
+  if (!isfinite(depth)) return false;
+
+  float rgb[3] = {static_cast<float>(rgba8 & 0xffu) / 255.0f,
+                  static_cast<float>((rgba8 >> 8) & 0xffu) / 255.0f,
+                  static_cast<float>((rgba8 >> 16) & 0xffu) / 255.0f};
+  if constexpr (D >= 1) {
+    ShWords<D> words;
+    words.load(sh, index);
+    const float dx = px - cam.cameraPosition[0];
+    const float dy = py - cam.cameraPosition[1];
+    const float dz = pz - cam.cameraPosition[2];
+    const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
+    float c[3];
+    shColor<D>(words, dx / len, dy / len, dz / len, c);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) rgb[j] = fmaxf(rgb[j] + c[j], 0.0f);
+  }
+
+  if constexpr (kKey16) {
+    const float zNear = cam.proj[14] / cam.proj[10];
+    const uint32_t steps = asU(fmaxf(depth, zNear)) - asU(zNear);
+    key = min(steps >> kDepthKeyShift, kDepthKeyMax);
+  } else {
+    key = asU(depth);
+  }
+  out[0] = asU(clip[0] / clip[3]);
+  out[1] = asU(clip[1] / clip[3]);
+  out[2] = axis1;
+  out[3] = axis2;
+  out[4] = packHalf2(rgb[0], rgb[1]);
+  out[5] = packHalf2(rgb[2], alpha);
+  out[6] = asU(radius);
+  out[7] = index;
+  return true;
+}
+
+__device__ __forceinline__ uint32_t sourceIndex(const VisibilityArgs& a, uint32_t t) {
+  if (a.rangeCount == 1) return a.ranges[0].offset + t;
+  // SplatVisibility.metal:30-37: the range whose start is the last one <= t.
+  uint32_t lo = 0, hi = a.rangeCount;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (a.rangeStarts[mid] <= t) lo = mid; else hi = mid;
+  }
+  return a.ranges[lo].offset + (t - a.rangeStarts[lo]);
+}
+
+template <int D, bool kKey16, bool kIndexed>
+__global__ void __launch_bounds__(kThreads)
+    visibilityKernel(const __grid_constant__ Camera cam, const __grid_constant__ VisibilityArgs a) {
+  __shared__ uint32_t warpBase[kThreads / 32];
+  __shared__ uint32_t tileBase;
+  const uint32_t tile = takeTile(a.counters);
+  const uint32_t total = kIndexed ? min(*a.indexCount, a.total) : a.total;
+  const uint32_t tiles = (total + kTileSplats - 1) / kTileSplats;
+  if (tile < tiles) {
+    const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+    uint32_t key[kItems];
+    uint32_t rec[kItems][8];
+    uint32_t rowMask[kItems];
+#pragma unroll
+    for (uint32_t r = 0; r < kItems; ++r) {
+      const uint32_t t = tile * kTileSplats + warp * (32 * kItems) + r * 32 + lane;
+      bool visible = false;
+      if (t < total) {
+        const uint32_t index = kIndexed ? a.indices[t] : sourceIndex(a, t);
+        if (index < a.worldCount) {
+          const uint4* p = reinterpret_cast<const uint4*>(a.splats + index);
+          const uint4 lo = __ldg(p), hi = __ldg(p + 1);
+          visible = projectSplat<D, kKey16>(cam, lo, hi, index, a.sh, key[r], rec[r]);
+        } else {
+          atomicOr(a.error, SK_DEVERR_BOUNDS);
+        }
+      }
+      rowMask[r] = __ballot_sync(0xffffffffu, visible);
+    }
+    uint32_t warpTotal = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < kItems; ++r) warpTotal += __popc(rowMask[r]);
+    if (lane == 0) warpBase[warp] = warpTotal;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t mine = lane < kThreads / 32 ? warpBase[lane] : 0u;
+      uint32_t inclusive = mine;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t up = __shfl_up_sync(0xffffffffu, inclusive, o);
+        if (lane >= static_cast<uint32_t>(o)) inclusive += up;
+      }
+      const uint32_t aggregate = __shfl_sync(0xffffffffu, inclusive, 31);
+      if (lane < kThreads / 32) warpBase[lane] = inclusive - mine;
+      uint32_t exclusive = 0;
+      if (tile == 0) {
+        if (lane == 0) storeStatus(a.status, makeStatus(a.epoch, kFlagPrefix, aggregate));
+      } else {
+        if (lane == 0) storeStatus(a.status + tile, makeStatus(a.epoch, kFlagAggregate, aggregate));
+        exclusive = warpLookback(a.status, tile, a.epoch, a.error);
+        if (lane == 0)
+          storeStatus(a.status + tile, makeStatus(a.epoch, kFlagPrefix, exclusive + aggregate));
+      }
+      if (lane == 0) {
+        tileBase = exclusive;
+        if (tile == tiles - 1) *a.visibleCount = exclusive + aggregate;
+      }
+    }
+    __syncthreads();
+    uint32_t pos = tileBase + warpBase[warp];
+    const uint32_t below = lanemaskLt();
+#pragma unroll
+    for (uint32_t r = 0; r < kItems; ++r) {
+      if (rowMask[r] & (1u << lane)) {
+        const uint32_t at = pos + __popc(rowMask[r] & below);
+        a.keys[at] = key[r];
+        uint4* o = reinterpret_cast<uint4*>(a.projected + at);
+        o[0] = make_uint4(rec[r][0], rec[r][1], rec[r][2], rec[r][3]);
+        o[1] = make_uint4(rec[r][4], rec[r][5], rec[r][6], rec[r][7]);
+      }
+      pos += __popc(rowMask[r]);
+    }
+  }
+  if (tiles == 0 && tile == 0 && threadIdx.x == 0) *a.visibleCount = 0;
+  finishTile(a.counters);
+}
+
+template <int D, bool kKey16, bool kIndexed>
+void launchOne(const Camera& cam, const VisibilityArgs& a, uint32_t grid, cudaStream_t stream) {
+  visibilityKernel<D, kKey16, kIndexed><<<grid, kThreads, 0, stream>>>(cam, a);
+}
+
+template <int D>
+void launchDegree(const Camera& cam, const VisibilityArgs& a, bool key16, bool indexed,
+                  uint32_t grid, cudaStream_t stream) {
+  if (key16) {
+    if (indexed) launchOne<D, true, true>(cam, a, grid, stream);
+    else launchOne<D, true, false>(cam, a, grid, stream);
+  } else {
+    if (indexed) launchOne<D, false, true>(cam, a, grid, stream);
+    else launchOne<D, false, false>(cam, a, grid, stream);
+  }
+}
+
+}  // namespace
+
+uint32_t visibilityTileSplats() { return kTileSplats; }
+
+cudaError_t launchVisibility(const Camera& cam, const VisibilityArgs& args, int shDegree,
+                             bool key16, bool indexed, cudaStream_t stream) {
+  const uint32_t grid = max(1u, (args.total + kTileSplats - 1) / kTileSplats);
+  switch (shDegree) {
+    case 0: launchDegree<0>(cam, args, key16, indexed, grid, stream); break;
+    case 1: launchDegree<1>(cam, args, key16, indexed, grid, stream); break;
+    case 2: launchDegree<2>(cam, args, key16, indexed, grid, stream); break;
+    default: launchDegree<3>(cam, args, key16, indexed, grid, stream); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace sk

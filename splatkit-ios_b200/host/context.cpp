@@ -1,0 +1,890 @@
+// The C ABI of include/splatkit_b200.h: a headless renderer context that mirrors
+// splatkit::SplatRenderer (packages/splatkit-engine/include/splatkit/rendering/SplatRenderer.h)
+// and the Metal renderer's frame (splatkit-ios/.../metal/MetalSplatRenderer.mm:166-308).
+//
+// A frame is enqueued on the context's stream without a host round trip:
+//   [LOD cut] -> visibility (cull, project, SH, depth key, source-order compaction)
+//   -> depth sort (onesweep radix, 16- or 32-bit keys) -> tile binning -> stable tile sort
+//   -> tile ranges -> composite, then a 64-byte counter block is copied back asynchronously.
+// Every grid is sized by a host-known capacity; live counts stay on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/splatkit_b200.h"
+#include "../csrc/sk_kernels.h"
+#include "context.h"
+#include "world_prep.h"
+
+namespace sk {
+
+// ---- device buffers -----------------------------------------------------------------------
+
+cudaError_t DeviceBuffer::allocate(size_t n) {
+  if (n <= bytes && ptr) return cudaSuccess;
+  void* fresh = nullptr;
+  const cudaError_t e = cudaMalloc(&fresh, std::max<size_t>(n, 256));
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // an allocation failure is not a sticky error
+    return e;
+  }
+  release();
+  ptr = fresh;
+  bytes = std::max<size_t>(n, 256);
+  return cudaSuccess;
+}
+
+void DeviceBuffer::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+namespace {
+
+constexpr uint32_t kMaxRanges = 65536;  // MetalVisibilityPass.h:72
+constexpr float kTransmittanceCutoff = 1e-4f;
+
+int hostThreads() { return std::max(1u, std::min(16u, std::thread::hardware_concurrency())); }
+
+}  // namespace
+
+sk_status Context::fail(sk_status code, const std::string& message) {
+  error = message;
+  return code;
+}
+
+sk_status Context::check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SK_OK;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return fail(SK_E_OOM, std::string(what) + ": out of device memory");
+  }
+  failed.store(true);
+  return fail(SK_E_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+uint32_t Context::nextEpoch(uint32_t n) {
+  const uint32_t e = epoch;
+  epoch += n;
+  if (epoch >= 0x3fff0000u) epoch = 1;  // status words of old epochs never match a new one
+  return e;
+}
+
+// Scratch sized for `sources` splats per frame and `instances` tile instances.
+sk_status Context::reserveFrame(FrameScratch& f, uint32_t sources, uint32_t instances) {
+  sources = std::max(sources, 1u);
+  instances = std::max(instances, 1u);
+  const uint32_t tilesX = (width + kTileSize - 1) / kTileSize;
+  const uint32_t tilesY = (height + kTileSize - 1) / kTileSize;
+  const size_t pixels = size_t{width} * height;
+  const size_t pixelBytes = imageFormat == SK_FORMAT_RGBA32F ? 16 : 4;
+  cudaError_t e = cudaSuccess;
+  auto grab = [&](DeviceBuffer& b, size_t n) {
+    if (e == cudaSuccess) e = b.allocate(n);
+  };
+  const uint32_t visTiles = (sources + visibilityTileSplats() - 1) / visibilityTileSplats();
+  const uint32_t binTiles = visTiles;
+  grab(f.keys, size_t{sources} * 4);
+  grab(f.projected, size_t{sources} * sizeof(Projected));
+  grab(f.order, size_t{sources} * 4);
+  grab(f.sortWorkspace, sortWorkspaceBytes(sources));
+  grab(f.visStatus, size_t{visTiles} * 8);
+  grab(f.binStatus, size_t{binTiles} * 8);
+  grab(f.instKeys, size_t{instances} * 4);
+  grab(f.instValues, size_t{instances} * 4);
+  grab(f.instKeysSorted, size_t{instances} * 4);
+  grab(f.instValuesSorted, size_t{instances} * 4);
+  grab(f.tileSortWorkspace, sortWorkspaceBytes(instances));
+  grab(f.ranges, size_t{tilesX} * tilesY * sizeof(uint2));
+  grab(f.image, pixels * pixelBytes);
+  grab(f.rangeBuffer, size_t{kMaxRanges} * sizeof(Range));
+  grab(f.rangeStarts, size_t{kMaxRanges + 1} * 4);
+  if (!f.counters.ptr) {
+    grab(f.counters, 64 * 4);
+    if (e == cudaSuccess) e = cudaMemsetAsync(f.counters.ptr, 0, 64 * 4, stream);
+    grab(f.frameCounters, sizeof(FrameCounters));
+    if (e == cudaSuccess) e = cudaMemsetAsync(f.frameCounters.ptr, 0, sizeof(FrameCounters), stream);
+  }
+  if (e != cudaSuccess) return check(e, "frame buffers");
+  if (!f.hostCounters) {
+    e = cudaMallocHost(&f.hostCounters, sizeof(FrameCounters));
+    if (e != cudaSuccess) return check(e, "pinned counters");
+    std::memset(f.hostCounters, 0, sizeof(FrameCounters));
+  }
+  // Sort workspaces hold counters that must start at zero.
+  e = cudaMemsetAsync(f.sortWorkspace.ptr, 0, f.sortWorkspace.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.tileSortWorkspace.ptr, 0, f.tileSortWorkspace.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.visStatus.ptr, 0, f.visStatus.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.binStatus.ptr, 0, f.binStatus.bytes, stream);
+  if (e != cudaSuccess) return check(e, "frame buffers");
+  f.sources = sources;
+  f.instanceCapacity = instances;
+  f.tilesX = tilesX;
+  f.tilesY = tilesY;
+  return SK_OK;
+}
+
+sk_status Context::reserveLod(FrameScratch& f, const World& w) {
+  cudaError_t e = cudaSuccess;
+  auto grab = [&](DeviceBuffer& b, size_t n) {
+    if (e == cudaSuccess) e = b.allocate(n);
+  };
+  const uint32_t frontier = std::max(1u, std::min(w.lodCapacity, w.clusterCount));
+  const uint32_t tiles = (frontier + lodTileClusters() - 1) / lodTileClusters();
+  grab(f.lodIndices, size_t{w.lodCapacity} * 4);
+  grab(f.lodFrontier[0], size_t{frontier} * 4);
+  grab(f.lodFrontier[1], size_t{frontier} * 4);
+  grab(f.lodCosts, size_t{frontier} * 8);
+  grab(f.lodOffsets, size_t{frontier} * 16);
+  grab(f.lodPackets, size_t{frontier} * 16);
+  grab(f.lodState, 256);
+  grab(f.lodStatus, size_t{tiles} * 3 * 8);
+  grab(f.lodCounters, 2 * 4);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodStatus.ptr, 0, f.lodStatus.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodCounters.ptr, 0, f.lodCounters.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodState.ptr, 0, f.lodState.bytes, stream);
+  if (e != cudaSuccess) return check(e, "LOD buffers");
+  f.lodFrontierCapacity = frontier;
+  return SK_OK;
+}
+
+Camera Context::cameraFor(const sk_frame& frame) const {
+  Camera c{};
+  std::memcpy(c.view, frame.view, 64);
+  std::memcpy(c.proj, frame.proj, 64);
+  c.screenSize[0] = static_cast<float>(width);
+  c.screenSize[1] = static_cast<float>(height);
+  // MetalFrameCompute.mm:148-151
+  c.focal[0] = (c.screenSize[0] * frame.proj[0]) / 2.0f;
+  c.focal[1] = (c.screenSize[1] * frame.proj[5]) / 2.0f;
+  c.tanHalfFov[0] = 1.0f / frame.proj[0];
+  c.tanHalfFov[1] = 1.0f / frame.proj[5];
+  c.outputLinear = 0;
+  c.minPixelRadius = policy.subpixel_threshold;
+  c.cameraPosition[0] = frame.camera_position[0];
+  c.cameraPosition[1] = frame.camera_position[1];
+  c.cameraPosition[2] = frame.camera_position[2];
+  c.cameraPosition[3] = 1.0f;
+  c.reveal[0] = frame.reveal_level;
+  return c;
+}
+
+// Validates ranges before anything is written (MetalVisibilityPass.mm:150-162).
+sk_status Context::validateRanges(const sk_frame& frame, uint32_t* total) const {
+  if (frame.range_count > kMaxRanges || (frame.range_count > 0 && frame.ranges == nullptr))
+    return SK_E_INVALID;
+  uint32_t sum = 0;
+  const uint32_t capacity = world.count;
+  for (uint32_t i = 0; i < frame.range_count; ++i) {
+    const sk_range& r = frame.ranges[i];
+    if (r.offset > world.count || r.count > world.count - r.offset || r.count > capacity - sum)
+      return SK_E_INVALID;
+    sum += r.count;
+  }
+  *total = sum;
+  return SK_OK;
+}
+
+// Enqueues one frame on `stream` with scratch `f`. `ranges` are already validated.
+sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t total,
+                                cudaStream_t s, bool timed) {
+  const Camera cam = cameraFor(frame);
+  const int degree = std::max(0, std::min(frame.sh_degree, world.shDegree));
+  const bool key16 = policy.sort_depth_bits == 16;
+  uint32_t* counters = static_cast<uint32_t*>(f.counters.ptr);
+  FrameCounters* fc = static_cast<FrameCounters*>(f.frameCounters.ptr);
+  uint32_t* error = &fc->error;
+  cudaError_t e = cudaMemsetAsync(fc, 0, sizeof(FrameCounters), s);
+  if (timed) cudaEventRecord(f.events[0], s);
+
+  const bool lod = world.lod;
+  if (lod && e == cudaSuccess) {
+    LodArgs a{};
+    a.clusters = static_cast<const LodCluster*>(world.clusters.ptr);
+    a.leaves = static_cast<const uint32_t*>(world.leaves.ptr);
+    a.clusterCount = world.clusterCount;
+    a.capacity = world.lodCapacity;
+    a.limit = lodLimit == 0 ? world.lodCapacity : std::min(lodLimit, world.lodCapacity);
+    a.pixelLimit = threshold.pixels();
+    a.colorWeight = 4.0f;
+    a.cull = policy.enable_frustum_culling ? 1u : 0u;
+    a.rounds = world.rounds;
+    a.frontierCapacity = f.lodFrontierCapacity;
+    a.frontier[0] = static_cast<uint32_t*>(f.lodFrontier[0].ptr);
+    a.frontier[1] = static_cast<uint32_t*>(f.lodFrontier[1].ptr);
+    a.costs = static_cast<uint2*>(f.lodCosts.ptr);
+    a.offsets = static_cast<uint4*>(f.lodOffsets.ptr);
+    a.packets = static_cast<uint4*>(f.lodPackets.ptr);
+    a.indices = static_cast<uint32_t*>(f.lodIndices.ptr);
+    a.state = static_cast<LodState*>(f.lodState.ptr);
+    a.status = static_cast<uint64_t*>(f.lodStatus.ptr);
+    a.counters = static_cast<uint32_t*>(f.lodCounters.ptr);
+    a.epoch = nextEpoch(2 * world.rounds + 2);
+    a.error = error;
+    a.report = fc->lod;
+    e = launchLodSelect(cam, a, s);
+  }
+  if (timed) cudaEventRecord(f.events[1], s);
+
+  if (e == cudaSuccess && !lod && frame.range_count > 0) {
+    // Ranges and their starts (SplatVisibility.metal:30-37); pageable copies are staged at once.
+    std::vector<uint32_t> starts(frame.range_count + 1, 0);
+    for (uint32_t i = 0; i < frame.range_count; ++i) starts[i + 1] = starts[i] + frame.ranges[i].count;
+    e = cudaMemcpyAsync(f.rangeBuffer.ptr, frame.ranges, size_t{frame.range_count} * sizeof(Range),
+                        cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(f.rangeStarts.ptr, starts.data(), starts.size() * 4,
+                          cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) {
+    VisibilityArgs v{};
+    v.splats = static_cast<const GpuSplat*>(world.splats.ptr);
+    v.sh = static_cast<const uint32_t*>(world.sh.ptr);
+    v.worldCount = world.count;
+    v.ranges = static_cast<const Range*>(f.rangeBuffer.ptr);
+    v.rangeStarts = static_cast<const uint32_t*>(f.rangeStarts.ptr);
+    v.rangeCount = lod ? 0 : frame.range_count;
+    v.indices = lod ? static_cast<const uint32_t*>(f.lodIndices.ptr) : nullptr;
+    v.indexCount = lod ? &fc->lod[0] : nullptr;
+    v.total = lod ? world.lodCapacity : total;
+    v.keys = static_cast<uint32_t*>(f.keys.ptr);
+    v.projected = static_cast<Projected*>(f.projected.ptr);
+    v.visibleCount = &fc->visible;
+    v.status = static_cast<uint64_t*>(f.visStatus.ptr);
+    v.counters = counters + 0;
+    v.epoch = nextEpoch(1);
+    v.error = error;
+    e = launchVisibility(cam, v, degree, key16, lod, s);
+  }
+  if (timed) cudaEventRecord(f.events[2], s);
+  if (e == cudaSuccess) {
+    SortArgs a{};
+    a.keysIn = static_cast<const uint32_t*>(f.keys.ptr);
+    a.valuesIn = nullptr;
+    a.keysOut = nullptr;
+    a.valuesOut = static_cast<uint32_t*>(f.order.ptr);
+    a.count = &fc->visible;
+    a.capacity = f.sources;
+    a.bits = key16 ? 16 : 32;
+    sortBindWorkspace(a, f.sortWorkspace.ptr, f.sources);
+    a.epoch = nextEpoch(4);
+    a.error = error;
+    e = launchSort(a, s);
+  }
+  if (timed) cudaEventRecord(f.events[3], s);
+  if (e == cudaSuccess) {
+    BinArgs b{};
+    b.projected = static_cast<const Projected*>(f.projected.ptr);
+    b.order = static_cast<const uint32_t*>(f.order.ptr);
+    b.count = &fc->visible;
+    b.capacity = f.sources;
+    b.width = width, b.height = height, b.tilesX = f.tilesX, b.tilesY = f.tilesY;
+    b.instanceKeys = static_cast<uint32_t*>(f.instKeys.ptr);
+    b.instanceValues = static_cast<uint32_t*>(f.instValues.ptr);
+    b.instanceCapacity = f.instanceCapacity;
+    b.instanceCount = &fc->instances;
+    b.overflow = &fc->overflow;
+    b.status = static_cast<uint64_t*>(f.binStatus.ptr);
+    b.counters = counters + 2;
+    b.epoch = nextEpoch(1);
+    b.error = error;
+    e = launchBinning(b, s);
+  }
+  if (e == cudaSuccess) {
+    SortArgs a{};
+    a.keysIn = static_cast<const uint32_t*>(f.instKeys.ptr);
+    a.valuesIn = static_cast<const uint32_t*>(f.instValues.ptr);
+    a.keysOut = static_cast<uint32_t*>(f.instKeysSorted.ptr);
+    a.valuesOut = static_cast<uint32_t*>(f.instValuesSorted.ptr);
+    a.count = &fc->instances;
+    a.capacity = f.instanceCapacity;
+    a.bits = 16;
+    sortBindWorkspace(a, f.tileSortWorkspace.ptr, f.instanceCapacity);
+    a.epoch = nextEpoch(4);
+    a.error = error;
+    e = launchSort(a, s);
+  }
+  if (e == cudaSuccess)
+    e = launchTileRanges(static_cast<const uint32_t*>(f.instKeysSorted.ptr), &fc->instances,
+                         f.instanceCapacity, static_cast<uint2*>(f.ranges.ptr), f.tilesX * f.tilesY, s);
+  if (timed) cudaEventRecord(f.events[4], s);
+  if (e == cudaSuccess) {
+    CompositeArgs c{};
+    c.projected = static_cast<const Projected*>(f.projected.ptr);
+    c.values = static_cast<const uint32_t*>(f.instValuesSorted.ptr);
+    c.ranges = static_cast<const uint2*>(f.ranges.ptr);
+    c.width = width, c.height = height, c.tilesX = f.tilesX, c.tilesY = f.tilesY;
+    for (int j = 0; j < 3; ++j) c.background[j] = static_cast<float>(policy.background[j]);
+    c.opaque = 1;
+    c.cutoff = policy.enable_early_termination ? kTransmittanceCutoff : 0.0f;
+    c.image = f.image.ptr;
+    c.format = imageFormat == SK_FORMAT_RGBA32F ? kRgba32f : kRgba8;
+    c.fragments = &fc->fragments_lo;
+    e = launchComposite(c, s);
+  }
+  if (timed) cudaEventRecord(f.events[5], s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(f.hostCounters, fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaEventRecord(f.done, s);
+  return check(e, "frame");
+}
+
+// Reads the last frame's counters once it completed; grows the instance buffers and redraws
+// when the binning ran out of room.
+sk_status Context::finishFrame(bool wait) {
+  if (!frameInFlight) return SK_OK;
+  if (wait) {
+    const cudaError_t e = cudaEventSynchronize(frame.done);
+    if (e != cudaSuccess) return check(e, "frame wait");
+  } else if (cudaEventQuery(frame.done) != cudaSuccess) {
+    return SK_OK;
+  }
+  frameInFlight = false;
+  ++completed;
+  const FrameCounters c = *frame.hostCounters;
+  if (c.overflow) {
+    // Grow to what the frame needed (plus headroom) and draw it again.
+    const uint32_t need = static_cast<uint32_t>(std::min<uint64_t>(
+        uint64_t{c.instances} + c.instances / 4 + 1024, 0xffffffffu));
+    sk_status st = reserveFrame(frame, frame.sources, need);
+    if (st != SK_OK) return st;
+    st = enqueueFrame(frame, lastFrame, lastTotal, stream, timeStages);
+    if (st != SK_OK) return st;
+    frameInFlight = true;
+    --completed;
+    return finishFrame(true);
+  }
+  lastCounters = c;
+  if (timeStages) {
+    float ms[5] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], frame.events[i], frame.events[i + 1]);
+    float all = 0;
+    cudaEventElapsedTime(&all, frame.events[0], frame.events[5]);
+    stats.select_ms = ms[0], stats.cull_ms = ms[1], stats.sort_ms = ms[2];
+    stats.bin_ms = ms[3], stats.composite_ms = ms[4], stats.gpu_ms = all;
+  }
+  if (world.lod) {
+    threshold.update(c.lod[0], c.lod[4],
+                     lodLimit == 0 ? world.lodCapacity : std::min(lodLimit, world.lodCapacity));
+  }
+  if (c.error) return fail(SK_E_TIMEOUT, "a bounded device wait or bounds check failed in the last frame");
+  return SK_OK;
+}
+
+sk_status Context::uploadCloud(const sk_cloud_view& cloud, int maxSh, World& w) {
+  if (cloud.count > 0 && (!cloud.positions || !cloud.covariances || !cloud.colors || !cloud.alphas))
+    return fail(SK_E_INVALID, "cloud arrays missing");
+  host::CloudRef ref{cloud.positions, cloud.covariances, cloud.colors, cloud.alphas, cloud.sh,
+                     cloud.count, cloud.sh ? std::max(0, std::min(cloud.sh_degree, 3)) : 0};
+  const int degree = std::max(0, std::min({maxSh, ref.shDegree, 3}));
+  const uint32_t stride = shDeviceStride(degree);
+  std::vector<GpuSplat> packed(cloud.count);
+  host::packSplats(ref, 0, cloud.count, packed.data(), hostThreads());
+  std::vector<uint32_t> sh(size_t{cloud.count} * stride);
+  host::packSh(ref, degree, 0, cloud.count, sh.data(), stride, hostThreads());
+  cudaError_t e = w.splats.allocate(std::max<size_t>(packed.size() * sizeof(GpuSplat), 32));
+  if (e == cudaSuccess) e = w.sh.allocate(std::max<size_t>(sh.size() * 4, 16));
+  if (e != cudaSuccess) return check(e, "world upload");
+  if (cloud.count) {
+    e = cudaMemcpy(w.splats.ptr, packed.data(), packed.size() * sizeof(GpuSplat), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !sh.empty())
+      e = cudaMemcpy(w.sh.ptr, sh.data(), sh.size() * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return check(e, "world upload");
+  }
+  w.count = cloud.count;
+  w.shDegree = degree;
+  return SK_OK;
+}
+
+}  // namespace sk
+
+using sk::Context;
+
+extern "C" {
+
+void sk_default_policy(sk_policy* out) {
+  if (!out) return;
+  // RenderPolicy{} (RenderPolicy.h:17-40)
+  out->lod_error_pixels = 1.0f;
+  out->lod_splat_limit = 0;
+  out->alpha_threshold = 1.0f / 255.0f;
+  out->subpixel_threshold = 1.0f;
+  out->enable_frustum_culling = 1;
+  out->enable_early_termination = 1;
+  out->sort_depth_bits = 16;
+  out->background[0] = 0.05, out->background[1] = 0.05, out->background[2] = 0.08;
+}
+
+sk_status sk_create(const sk_config* config, sk_context** out) {
+  if (!config || !out) return SK_E_INVALID;
+  *out = nullptr;
+  if (config->image_format != SK_FORMAT_RGBA8 && config->image_format != SK_FORMAT_RGBA32F)
+    return SK_E_INVALID;
+  if (config->width == 0 || config->height == 0 || config->width > 16384 || config->height > 16384)
+    return SK_E_INVALID;
+  int devices = 0;
+  if (cudaGetDeviceCount(&devices) != cudaSuccess || config->device < 0 || config->device >= devices) {
+    cudaGetLastError();
+    return SK_E_DEVICE;
+  }
+  auto ctx = std::make_unique<Context>();
+  ctx->device = config->device;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return SK_E_DEVICE;
+  ctx->width = config->width;
+  ctx->height = config->height;
+  ctx->imageFormat = config->image_format;
+  ctx->timeStages = config->time_stages != 0;
+  sk_default_policy(&ctx->policy);
+  ctx->threshold.reset(ctx->policy.lod_error_pixels);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SK_E_DEVICE;
+  for (auto& ev : ctx->frame.events)
+    if (cudaEventCreate(&ev) != cudaSuccess) return SK_E_DEVICE;
+  if (cudaEventCreateWithFlags(&ctx->frame.done, cudaEventDisableTiming) != cudaSuccess)
+    return SK_E_DEVICE;
+  if (ctx->reserveFrame(ctx->frame, 1, 1024) != SK_OK) return SK_E_DEVICE;
+  *out = reinterpret_cast<sk_context*>(ctx.release());
+  return SK_OK;
+}
+
+void sk_destroy(sk_context* handle) {
+  auto* ctx = reinterpret_cast<Context*>(handle);
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  delete ctx;
+}
+
+const char* sk_last_error(const sk_context* handle) {
+  const auto* ctx = reinterpret_cast<const Context*>(handle);
+  return ctx ? ctx->error.c_str() : "no context";
+}
+
+#define SK_CTX(handle)                                          \
+  auto* ctx = reinterpret_cast<Context*>(handle);               \
+  if (!ctx) return SK_E_INVALID;                                \
+  if (ctx->failed.load()) return SK_E_DEVICE;                   \
+  cudaSetDevice(ctx->device)
+
+sk_status sk_resize(sk_context* handle, uint32_t width, uint32_t height) {
+  SK_CTX(handle);
+  if (width == 0 || height == 0 || width > 16384 || height > 16384) return SK_E_INVALID;
+  sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK && st != SK_E_TIMEOUT) return st;
+  const uint32_t oldW = ctx->width, oldH = ctx->height;
+  ctx->width = width;
+  ctx->height = height;
+  st = ctx->reserveFrame(ctx->frame, ctx->frame.sources, ctx->frame.instanceCapacity);
+  if (st != SK_OK) {
+    ctx->width = oldW;
+    ctx->height = oldH;
+  }
+  return st;
+}
+
+sk_status sk_device_capabilities(sk_context* handle, sk_capabilities* out) {
+  SK_CTX(handle);
+  if (!out) return SK_E_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  out->max_lod_capacity_splats = sk::kMaxLodBudgetPublic;
+  out->min_residency_capacity_splats = 1;
+  out->max_residency_capacity_splats = 0x7fffffffu;
+  out->supports_subgroups = 1;
+  out->max_texture_dimension = 16384;
+  out->sorts_on_gpu = 1;
+  out->selects_lod_on_gpu = 1;
+  size_t freeBytes = 0, total = 0;
+  if (cudaMemGetInfo(&freeBytes, &total) == cudaSuccess) out->total_memory = total;
+  return SK_OK;
+}
+
+sk_status sk_apply_render_policy(sk_context* handle, const sk_policy* p) {
+  SK_CTX(handle);
+  if (!p) return SK_E_INVALID;
+  // validRenderPolicy (splatkit-engine/src/rendering/RenderPolicy.cpp:29-52)
+  const bool ok = std::isfinite(p->lod_error_pixels) && p->lod_error_pixels > 0.0f &&
+                  std::isfinite(p->alpha_threshold) && p->alpha_threshold >= 0.0f &&
+                  p->alpha_threshold <= 1.0f && std::isfinite(p->subpixel_threshold) &&
+                  p->subpixel_threshold >= 0.0f &&
+                  (p->sort_depth_bits == 16 || p->sort_depth_bits == 32) &&
+                  std::all_of(p->background, p->background + 3,
+                              [](double c) { return std::isfinite(c) && c >= 0 && c <= 1; });
+  if (!ok) return ctx->fail(SK_E_INVALID, "render policy out of range");
+  const bool lodChanged = p->lod_error_pixels != ctx->threshold.policyPixels() ||
+                          p->lod_splat_limit != ctx->lodLimit;
+  ctx->policy = *p;
+  if (lodChanged) {
+    ctx->threshold.reset(p->lod_error_pixels);
+    ctx->lodLimit = p->lod_splat_limit;
+  }
+  return SK_OK;
+}
+
+sk_status sk_available_memory(sk_context* handle, uint64_t* bytes) {
+  SK_CTX(handle);
+  if (!bytes) return SK_E_INVALID;
+  size_t freeBytes = 0, total = 0;
+  if (cudaMemGetInfo(&freeBytes, &total) != cudaSuccess) return ctx->check(cudaGetLastError(), "memory");
+  *bytes = freeBytes;
+  return SK_OK;
+}
+
+int32_t sk_gpu_failed(sk_context* handle) {
+  auto* ctx = reinterpret_cast<Context*>(handle);
+  return ctx && ctx->failed.load() ? 1 : 0;
+}
+
+sk_status sk_upload_world(sk_context* handle, const sk_cloud_view* cloud, int32_t maxSh) {
+  SK_CTX(handle);
+  if (!cloud) return SK_E_INVALID;
+  sk_status st = ctx->finishFrame(true);
+  if (st == SK_E_DEVICE) return st;
+  cudaStreamSynchronize(ctx->stream);
+  // Build the new world aside; the old one stays until everything succeeded.
+  sk::World fresh;
+  st = ctx->uploadCloud(*cloud, maxSh, fresh);
+  if (st != SK_OK) return st;
+  st = ctx->reserveFrame(ctx->frame, cloud->count, std::max(ctx->frame.instanceCapacity,
+                                                             std::max(cloud->count, 1u) * 4));
+  if (st != SK_OK) return st;
+  ctx->world = std::move(fresh);
+  return SK_OK;
+}
+
+sk_status sk_create_slab(sk_context* handle, uint32_t capacity, int32_t shDegree) {
+  SK_CTX(handle);
+  if (shDegree < 0 || shDegree > 3) return SK_E_INVALID;
+  sk_status st = ctx->finishFrame(true);
+  if (st == SK_E_DEVICE) return st;
+  cudaStreamSynchronize(ctx->stream);
+  sk::World fresh;
+  cudaError_t e = fresh.splats.allocate(std::max<size_t>(size_t{capacity} * sizeof(sk::GpuSplat), 32));
+  if (e == cudaSuccess)
+    e = fresh.sh.allocate(std::max<size_t>(size_t{capacity} * sk::shDeviceStride(shDegree) * 4, 16));
+  if (e == cudaSuccess) e = cudaMemset(fresh.splats.ptr, 0, fresh.splats.bytes);
+  if (e == cudaSuccess) e = cudaMemset(fresh.sh.ptr, 0, fresh.sh.bytes);
+  if (e != cudaSuccess) return ctx->check(e, "slab");
+  st = ctx->reserveFrame(ctx->frame, capacity, std::max(ctx->frame.instanceCapacity,
+                                                        std::max(capacity, 1u) * 4));
+  if (st != SK_OK) return st;
+  fresh.count = capacity;
+  fresh.shDegree = shDegree;
+  ctx->world = std::move(fresh);
+  return SK_OK;
+}
+
+sk_status sk_upload_tile(sk_context* handle, uint32_t offset, const sk_cloud_view* cloud) {
+  SK_CTX(handle);
+  if (!cloud || ctx->world.lod) return SK_E_INVALID;
+  if (offset > ctx->world.count || cloud->count > ctx->world.count - offset) return SK_E_INVALID;
+  if (cloud->count == 0) return SK_OK;
+  sk::host::CloudRef ref{cloud->positions, cloud->covariances, cloud->colors, cloud->alphas,
+                         cloud->sh, cloud->count,
+                         cloud->sh ? std::max(0, std::min(cloud->sh_degree, 3)) : 0};
+  if (!ref.positions || !ref.covariances || !ref.colors || !ref.alphas) return SK_E_INVALID;
+  const int degree = std::min(ctx->world.shDegree, ref.shDegree);
+  const uint32_t stride = sk::shDeviceStride(ctx->world.shDegree);
+  std::vector<sk::GpuSplat> packed(cloud->count);
+  sk::host::packSplats(ref, 0, cloud->count, packed.data(), sk::hostThreadsPublic());
+  std::vector<uint32_t> sh(size_t{cloud->count} * stride, 0u);
+  if (degree > 0) sk::host::packSh(ref, degree, 0, cloud->count, sh.data(), stride, sk::hostThreadsPublic());
+  sk_status st = ctx->finishFrame(true);
+  if (st == SK_E_DEVICE) return st;
+  cudaError_t e = cudaMemcpy(static_cast<sk::GpuSplat*>(ctx->world.splats.ptr) + offset, packed.data(),
+                             packed.size() * sizeof(sk::GpuSplat), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && stride > 0)
+    e = cudaMemcpy(static_cast<uint32_t*>(ctx->world.sh.ptr) + size_t{offset} * stride, sh.data(),
+                   sh.size() * 4, cudaMemcpyHostToDevice);
+  return ctx->check(e, "tile upload");
+}
+
+sk_status sk_upload_lod_world(sk_context* handle, const sk_lod_view* tree, int32_t maxSh,
+                              uint32_t budget) {
+  SK_CTX(handle);
+  if (!tree || !tree->layout || tree->node_count == 0 || tree->nodes.count != tree->node_count)
+    return ctx->fail(SK_E_INVALID, "invalid LOD tree view");
+  std::string why;
+  const int64_t depth = sk::host::lodDepth(reinterpret_cast<const sk::LodNode*>(tree->layout),
+                                           tree->node_count, tree->leaf_count, &why);
+  if (depth < 0) return ctx->fail(SK_E_INVALID, "invalid LOD hierarchy: " + why);
+  if (budget == 0) return ctx->fail(SK_E_INVALID, "LOD budget is zero");
+  sk_status st = ctx->finishFrame(true);
+  if (st == SK_E_DEVICE) return st;
+  cudaStreamSynchronize(ctx->stream);
+  // Selection data: the tree's own, else built once here (MetalLodSelection.mm:68-74).
+  std::vector<sk::LodCluster> clusters;
+  std::vector<uint32_t> leaves;
+  if (tree->cluster_count > 0 && tree->clusters && tree->leaves) {
+    clusters.resize(tree->cluster_count);
+    std::memcpy(clusters.data(), tree->clusters, clusters.size() * sizeof(sk::LodCluster));
+    leaves.assign(tree->leaves, tree->leaves + tree->leaf_ref_count);
+  } else {
+    sk::host::CloudRef ref{tree->nodes.positions, tree->nodes.covariances, tree->nodes.colors,
+                           tree->nodes.alphas, tree->nodes.sh, tree->nodes.count,
+                           tree->nodes.sh ? std::max(0, std::min(tree->nodes.sh_degree, 3)) : 0};
+    sk::host::buildSelection(ref, reinterpret_cast<const sk::LodNode*>(tree->layout),
+                             tree->node_count, clusters, leaves);
+  }
+  sk::World fresh;
+  st = ctx->uploadCloud(tree->nodes, maxSh, fresh);
+  if (st != SK_OK) return st;
+  const uint32_t capacity = std::min({budget, sk::kMaxLodBudgetPublic, std::max(tree->leaf_count, 1u)});
+  cudaError_t e = fresh.clusters.allocate(clusters.size() * sizeof(sk::LodCluster));
+  if (e == cudaSuccess) e = fresh.leaves.allocate(std::max<size_t>(leaves.size() * 4, 4));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(fresh.clusters.ptr, clusters.data(), clusters.size() * sizeof(sk::LodCluster),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !leaves.empty())
+    e = cudaMemcpy(fresh.leaves.ptr, leaves.data(), leaves.size() * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return ctx->check(e, "LOD upload");
+  fresh.lod = true;
+  fresh.clusterCount = static_cast<uint32_t>(clusters.size());
+  fresh.leafRefCount = static_cast<uint32_t>(leaves.size());
+  fresh.rounds = static_cast<uint32_t>(depth) + 1;
+  fresh.lodCapacity = capacity;
+  st = ctx->reserveLod(ctx->frame, fresh);
+  if (st != SK_OK) return st;
+  // Projections and sort scratch scale with the cut, not with all resident nodes.
+  st = ctx->reserveFrame(ctx->frame, capacity, std::max(ctx->frame.instanceCapacity, capacity * 4));
+  if (st != SK_OK) return st;
+  ctx->world = std::move(fresh);
+  ctx->threshold.reset(ctx->threshold.policyPixels());
+  return SK_OK;
+}
+
+sk_status sk_world_info(sk_context* handle, uint32_t* count, int32_t* shDegree) {
+  SK_CTX(handle);
+  if (!ctx->world.splats.ptr) return SK_E_NO_WORLD;
+  if (count) *count = ctx->world.count;
+  if (shDegree) *shDegree = ctx->world.shDegree;
+  return SK_OK;
+}
+
+sk_status sk_draw(sk_context* handle, const sk_frame* frame) {
+  SK_CTX(handle);
+  if (!frame) return SK_E_INVALID;
+  uint32_t total = 0;
+  if (!ctx->world.lod && ctx->world.splats.ptr) {
+    if (ctx->validateRanges(*frame, &total) != SK_OK)
+      return ctx->fail(SK_E_INVALID, "invalid visibility ranges");
+  }
+  // One frame in flight on the plain path: the previous one completes first.
+  sk_status st = ctx->finishFrame(true);
+  if (st == SK_E_DEVICE) return st;
+  if (!ctx->world.splats.ptr) total = 0;
+  ctx->lastFrame = *frame;
+  ctx->lastTotal = total;
+  ctx->lastFrame.ranges = nullptr;
+  ctx->lastRanges.assign(frame->ranges, frame->ranges + (frame->ranges ? frame->range_count : 0));
+  ctx->lastFrame.ranges = ctx->lastRanges.data();
+  st = ctx->enqueueFrame(ctx->frame, ctx->lastFrame, total, ctx->stream, ctx->timeStages);
+  if (st != SK_OK) return st;
+  ctx->frameInFlight = true;
+  ++ctx->submitted;
+  return SK_OK;
+}
+
+sk_status sk_wait_idle(sk_context* handle) {
+  SK_CTX(handle);
+  const sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  return ctx->check(cudaStreamSynchronize(ctx->stream), "wait");
+}
+
+sk_status sk_read_image(sk_context* handle, void* host, size_t bytes, int32_t format) {
+  SK_CTX(handle);
+  if (!host) return SK_E_INVALID;
+  sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  const size_t pixels = size_t{ctx->width} * ctx->height;
+  const bool deviceFloat = ctx->imageFormat == SK_FORMAT_RGBA32F;
+  const size_t need = pixels * (format == SK_FORMAT_RGBA32F ? 16 : 4);
+  if (bytes < need) return ctx->fail(SK_E_INVALID, "image buffer too small");
+  if (format == SK_FORMAT_RGBA32F && !deviceFloat)
+    return ctx->fail(SK_E_INVALID, "the context renders 8-bit images");
+  if ((format == SK_FORMAT_RGBA8 && !deviceFloat) || (format == SK_FORMAT_RGBA32F && deviceFloat))
+    return ctx->check(cudaMemcpy(host, ctx->frame.image.ptr, need, cudaMemcpyDeviceToHost), "readback");
+  // Conversions on the host.
+  std::vector<uint8_t> staging(pixels * (deviceFloat ? 16 : 4));
+  cudaError_t e = cudaMemcpy(staging.data(), ctx->frame.image.ptr, staging.size(), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return ctx->check(e, "readback");
+  uint8_t* out = static_cast<uint8_t*>(host);
+  for (size_t i = 0; i < pixels; ++i) {
+    uint8_t rgba[4];
+    if (deviceFloat) {
+      const float* f = reinterpret_cast<const float*>(staging.data()) + i * 4;
+      for (int c = 0; c < 4; ++c)
+        rgba[c] = static_cast<uint8_t>(std::lround(std::min(1.0f, std::max(0.0f, f[c])) * 255.0f));
+    } else {
+      std::memcpy(rgba, staging.data() + i * 4, 4);
+    }
+    if (format == SK_FORMAT_BGRA8) std::swap(rgba[0], rgba[2]);
+    std::memcpy(out + i * 4, rgba, 4);
+  }
+  return SK_OK;
+}
+
+sk_status sk_get_stats(sk_context* handle, sk_stats* out) {
+  SK_CTX(handle);
+  if (!out) return SK_E_INVALID;
+  ctx->finishFrame(false);
+  sk_stats s = ctx->stats;
+  s.submitted_frames = ctx->submitted;
+  s.completed_frames = ctx->completed;
+  const sk::FrameCounters& c = ctx->lastCounters;
+  s.draw_count = c.visible;
+  s.selected_count = ctx->world.lod ? std::min(c.lod[0], ctx->world.lodCapacity) : 0;
+  s.lod_limited = c.lod[4];
+  s.lod_evaluated = c.lod[5];
+  s.instances = c.instances;
+  s.device_error = c.error;
+  s.fragments = uint64_t{c.fragments_lo} | (uint64_t{c.fragments_hi} << 32);
+  s.lod_pixels = ctx->threshold.pixels();
+  *out = s;
+  return SK_OK;
+}
+
+sk_status sk_read_visible(sk_context* handle, uint32_t* keys, void* projected, uint32_t capacity,
+                          uint32_t* count) {
+  SK_CTX(handle);
+  sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  const uint32_t n = ctx->lastCounters.visible;
+  if (count) *count = n;
+  const uint32_t copy = std::min(n, capacity);
+  cudaError_t e = cudaSuccess;
+  if (keys && copy) e = cudaMemcpy(keys, ctx->frame.keys.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && projected && copy)
+    e = cudaMemcpy(projected, ctx->frame.projected.ptr, size_t{copy} * 32, cudaMemcpyDeviceToHost);
+  return ctx->check(e, "readback");
+}
+
+sk_status sk_read_order(sk_context* handle, uint32_t* order, uint32_t capacity, uint32_t* count) {
+  SK_CTX(handle);
+  sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  const uint32_t n = ctx->lastCounters.visible;
+  if (count) *count = n;
+  const uint32_t copy = std::min(n, capacity);
+  if (!order || !copy) return SK_OK;
+  return ctx->check(cudaMemcpy(order, ctx->frame.order.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
+                    "readback");
+}
+
+sk_status sk_read_cut(sk_context* handle, uint32_t* indices, uint32_t capacity, uint32_t* count,
+                      uint32_t* lod6) {
+  SK_CTX(handle);
+  sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  if (!ctx->world.lod) return ctx->fail(SK_E_INVALID, "not a LOD world");
+  const uint32_t n = std::min(ctx->lastCounters.lod[0], ctx->world.lodCapacity);
+  if (count) *count = n;
+  if (lod6) std::memcpy(lod6, ctx->lastCounters.lod, 24);
+  const uint32_t copy = std::min(n, capacity);
+  if (!indices || !copy) return SK_OK;
+  return ctx->check(cudaMemcpy(indices, ctx->frame.lodIndices.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
+                    "readback");
+}
+
+size_t sk_sort_workspace_bytes(uint32_t capacity) { return sk::sortWorkspaceBytes(capacity); }
+
+sk_status sk_radix_argsort_device(const uint32_t* d_keys, const uint32_t* d_count,
+                                  uint32_t capacity, int32_t bits, uint32_t* d_order,
+                                  void* d_workspace, size_t workspaceBytes, uint32_t* d_error,
+                                  void* stream) {
+  if (!d_keys || !d_count || !d_order || !d_workspace || !d_error) return SK_E_INVALID;
+  if (bits != 16 && bits != 32) return SK_E_INVALID;
+  if (workspaceBytes < sk::sortWorkspaceBytes(capacity)) return SK_E_INVALID;
+  static std::atomic<uint32_t> epochs{1};
+  sk::SortArgs a{};
+  a.keysIn = d_keys;
+  a.valuesIn = nullptr;
+  a.keysOut = nullptr;
+  a.valuesOut = d_order;
+  a.count = d_count;
+  a.capacity = capacity;
+  a.bits = bits;
+  sk::sortBindWorkspace(a, d_workspace, capacity);
+  a.epoch = epochs.fetch_add(4) & 0x3fffffffu;
+  a.error = d_error;
+  const auto s = static_cast<cudaStream_t>(stream);
+  // Counters and histogram accumulators start at zero; status words carry the epoch.
+  cudaError_t e = sk::sortResetWorkspace(a, s);
+  if (e == cudaSuccess) e = sk::launchSort(a, s);
+  return e == cudaSuccess ? SK_OK : SK_E_DEVICE;
+}
+
+}  // extern "C"
+
+// ---- host-side world preparation ----------------------------------------------------------
+namespace {
+sk::host::CloudRef cloudRef(const sk_cloud_view& c) {
+  return sk::host::CloudRef{c.positions, c.covariances, c.colors, c.alphas, c.sh, c.count,
+                            c.sh ? std::max(0, std::min(c.sh_degree, 3)) : 0};
+}
+}  // namespace
+
+extern "C" {
+
+uint32_t sk_sh_device_stride(int32_t degree) { return sk::shDeviceStride(degree); }
+
+sk_status sk_pack_splats(const sk_cloud_view* cloud, uint32_t offset, uint32_t count, void* out) {
+  if (!cloud || !out || offset > cloud->count || count > cloud->count - offset) return SK_E_INVALID;
+  const auto ref = cloudRef(*cloud);
+  if (count && (!ref.positions || !ref.covariances || !ref.colors || !ref.alphas)) return SK_E_INVALID;
+  sk::host::packSplats(ref, offset, count, static_cast<sk::GpuSplat*>(out), sk::hostThreadsPublic());
+  return SK_OK;
+}
+
+sk_status sk_pack_sh(const sk_cloud_view* cloud, int32_t degree, uint32_t offset, uint32_t count,
+                     uint32_t* out, uint32_t stride) {
+  if (!cloud || !out || offset > cloud->count || count > cloud->count - offset) return SK_E_INVALID;
+  const auto ref = cloudRef(*cloud);
+  if (degree < 0 || degree > ref.shDegree || stride < sk::shPackedStride(degree)) return SK_E_INVALID;
+  sk::host::packSh(ref, degree, offset, count, out, stride, sk::hostThreadsPublic());
+  return SK_OK;
+}
+
+sk_status sk_build_lod_selection(const sk_lod_view* tree, sk_lod_cluster* clusters,
+                                 uint32_t clusterCapacity, uint32_t* clusterCount,
+                                 uint32_t* leaves, uint32_t leafCapacity, uint32_t* leafCount) {
+  if (!tree || !tree->layout || tree->nodes.count != tree->node_count) return SK_E_INVALID;
+  std::vector<sk::LodCluster> c;
+  std::vector<uint32_t> l;
+  sk::host::buildSelection(cloudRef(tree->nodes), reinterpret_cast<const sk::LodNode*>(tree->layout),
+                           tree->node_count, c, l);
+  if (clusterCount) *clusterCount = static_cast<uint32_t>(c.size());
+  if (leafCount) *leafCount = static_cast<uint32_t>(l.size());
+  if (clusters) std::memcpy(clusters, c.data(), std::min<size_t>(c.size(), clusterCapacity) * 64);
+  if (leaves) std::memcpy(leaves, l.data(), std::min<size_t>(l.size(), leafCapacity) * 4);
+  return SK_OK;
+}
+
+int64_t sk_lod_depth(const sk_lod_node* layout, uint32_t nodeCount, uint32_t leafCount) {
+  if (!layout) return -1;
+  return sk::host::lodDepth(reinterpret_cast<const sk::LodNode*>(layout), nodeCount, leafCount, nullptr);
+}
+
+uint64_t sk_world_bytes(uint64_t records, int32_t shDegree, uint64_t drawCapacity,
+                        uint64_t clusters, uint64_t leafRefs) {
+  return sk::host::worldBytes(records, shDegree, drawCapacity, clusters, leafRefs);
+}
+
+float sk_lod_threshold_update(float* state, uint32_t selected, uint32_t limited, uint32_t limit) {
+  if (!state) return 0.0f;
+  sk::host::LodThreshold t(state[0]);
+  t.restore(state[1]);
+  state[1] = t.update(selected, limited, limit);
+  return state[1];
+}
+
+}  // extern "C"

@@ -1,0 +1,523 @@
+"""splatkit_b200: Python mirror of the B200 splat renderer's C ABI (include/splatkit_b200.h).
+
+The verbs follow the reference's renderer surface, ``splatkit::SplatRenderer``
+(packages/splatkit-engine/include/splatkit/rendering/SplatRenderer.h:36-160): upload a
+world (flat or LOD), apply a render policy, draw a frame, read back the image and the frame
+statistics. Every call goes through ``libsplatkit_b200.so``; there is no other path. If the
+library or a CUDA device is missing, constructing a :class:`Renderer` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import camera  # noqa: F401  (re-exported helpers)
+
+_HERE = Path(__file__).resolve().parent
+LIBRARY_PATH = _HERE.parent / "libsplatkit_b200.so"
+
+# status codes (include/splatkit_b200.h)
+SK_OK = 0
+SK_E_INVALID = 1
+SK_E_OOM = 2
+SK_E_ADMISSION = 3
+SK_E_DEVICE = 4
+SK_E_TIMEOUT = 5
+SK_E_UNSUPPORTED = 6
+SK_E_NO_WORLD = 7
+STATUS_NAMES = {0: "ok", 1: "invalid", 2: "out of memory", 3: "admission", 4: "device",
+                5: "timeout", 6: "unsupported", 7: "no world"}
+
+FORMAT_RGBA8 = 0
+FORMAT_RGBA32F = 1
+FORMAT_BGRA8 = 2
+
+PROJECTED_DTYPE = np.dtype([("center", "<f4", (2,)), ("axis1", "<u4"), ("axis2", "<u4"),
+                            ("color0", "<u4"), ("color1", "<u4"), ("radius", "<f4"),
+                            ("index", "<u4")])
+LOD_NODE_DTYPE = np.dtype([("position", "<f4", (3,)), ("size", "<f4"),
+                           ("child_start", "<u4"), ("child_count", "<u4")])
+LOD_CLUSTER_DTYPE = np.dtype([("center", "<f4", (3,)), ("radius", "<f4"), ("extent", "<f4", (3,)),
+                              ("error", "<f4"), ("color_variance", "<f4"), ("opacity", "<f4"),
+                              ("node", "<u4"), ("child_start", "<u4"), ("child_count", "<u4"),
+                              ("leaf_start", "<u4"), ("leaf_count", "<u4"),
+                              ("subtree_leaves", "<u4")])
+assert PROJECTED_DTYPE.itemsize == 32 and LOD_NODE_DTYPE.itemsize == 24
+assert LOD_CLUSTER_DTYPE.itemsize == 64
+
+
+class SplatError(RuntimeError):
+    """A non-OK status from the C ABI; ``status`` holds the code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+# ---- ctypes mirror of the ABI structs -----------------------------------------------------
+_f32p = ctypes.POINTER(ctypes.c_float)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("image_format", ctypes.c_int32), ("time_stages", ctypes.c_uint32)]
+
+
+class _Cloud(ctypes.Structure):
+    _fields_ = [("positions", _f32p), ("covariances", _f32p), ("colors", _f32p),
+                ("alphas", _f32p), ("sh", _f32p), ("count", ctypes.c_uint32),
+                ("sh_degree", ctypes.c_int32)]
+
+
+class _LodView(ctypes.Structure):
+    _fields_ = [("nodes", _Cloud), ("layout", ctypes.c_void_p), ("node_count", ctypes.c_uint32),
+                ("leaf_count", ctypes.c_uint32), ("clusters", ctypes.c_void_p),
+                ("cluster_count", ctypes.c_uint32), ("leaves", _u32p),
+                ("leaf_ref_count", ctypes.c_uint32)]
+
+
+class _Range(ctypes.Structure):
+    _fields_ = [("offset", ctypes.c_uint32), ("count", ctypes.c_uint32)]
+
+
+class _Frame(ctypes.Structure):
+    _fields_ = [("view", ctypes.c_float * 16), ("proj", ctypes.c_float * 16),
+                ("camera_position", ctypes.c_float * 3), ("reveal_level", ctypes.c_float),
+                ("ranges", ctypes.POINTER(_Range)), ("range_count", ctypes.c_uint32),
+                ("sh_degree", ctypes.c_int32)]
+
+
+class _Policy(ctypes.Structure):
+    _fields_ = [("lod_error_pixels", ctypes.c_float), ("lod_splat_limit", ctypes.c_uint32),
+                ("alpha_threshold", ctypes.c_float), ("subpixel_threshold", ctypes.c_float),
+                ("enable_frustum_culling", ctypes.c_uint32),
+                ("enable_early_termination", ctypes.c_uint32),
+                ("sort_depth_bits", ctypes.c_uint32), ("background", ctypes.c_double * 3)]
+
+
+class _Caps(ctypes.Structure):
+    _fields_ = [("max_lod_capacity_splats", ctypes.c_uint32),
+                ("min_residency_capacity_splats", ctypes.c_uint32),
+                ("max_residency_capacity_splats", ctypes.c_uint32),
+                ("supports_subgroups", ctypes.c_uint32), ("max_texture_dimension", ctypes.c_uint32),
+                ("sorts_on_gpu", ctypes.c_uint32), ("selects_lod_on_gpu", ctypes.c_uint32),
+                ("total_memory", ctypes.c_uint64)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("submitted_frames", ctypes.c_uint64), ("completed_frames", ctypes.c_uint64),
+                ("gpu_ms", ctypes.c_double), ("select_ms", ctypes.c_double),
+                ("cull_ms", ctypes.c_double), ("sort_ms", ctypes.c_double),
+                ("bin_ms", ctypes.c_double), ("composite_ms", ctypes.c_double),
+                ("draw_count", ctypes.c_uint32), ("selected_count", ctypes.c_uint32),
+                ("lod_limited", ctypes.c_uint32), ("lod_evaluated", ctypes.c_uint32),
+                ("instances", ctypes.c_uint32), ("device_error", ctypes.c_uint32),
+                ("fragments", ctypes.c_uint64), ("lod_pixels", ctypes.c_float),
+                ("pad", ctypes.c_uint32)]
+
+
+# Every function the header declares, with its ctypes signature.
+_SIGNATURES = {
+    "sk_create": (ctypes.c_int32, [ctypes.POINTER(_Config), ctypes.POINTER(ctypes.c_void_p)]),
+    "sk_destroy": (None, [ctypes.c_void_p]),
+    "sk_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "sk_resize": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
+    "sk_device_capabilities": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Caps)]),
+    "sk_apply_render_policy": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Policy)]),
+    "sk_default_policy": (None, [ctypes.POINTER(_Policy)]),
+    "sk_available_memory": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "sk_gpu_failed": (ctypes.c_int32, [ctypes.c_void_p]),
+    "sk_upload_world": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Cloud), ctypes.c_int32]),
+    "sk_upload_lod_world": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_LodView),
+                                             ctypes.c_int32, ctypes.c_uint32]),
+    "sk_create_slab": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32]),
+    "sk_upload_tile": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(_Cloud)]),
+    "sk_world_info": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.POINTER(ctypes.c_int32)]),
+    "sk_draw": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Frame)]),
+    "sk_read_image": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                       ctypes.c_int32]),
+    "sk_wait_idle": (ctypes.c_int32, [ctypes.c_void_p]),
+    "sk_get_stats": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Stats)]),
+    "sk_read_visible": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_void_p, ctypes.c_uint32,
+                                         _u32p]),
+    "sk_read_order": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_uint32, _u32p]),
+    "sk_read_cut": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_uint32, _u32p, _u32p]),
+    "sk_sort_workspace_bytes": (ctypes.c_size_t, [ctypes.c_uint32]),
+    "sk_sh_device_stride": (ctypes.c_uint32, [ctypes.c_int32]),
+    "sk_pack_splats": (ctypes.c_int32, [ctypes.POINTER(_Cloud), ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_void_p]),
+    "sk_pack_sh": (ctypes.c_int32, [ctypes.POINTER(_Cloud), ctypes.c_int32, ctypes.c_uint32,
+                                    ctypes.c_uint32, _u32p, ctypes.c_uint32]),
+    "sk_build_lod_selection": (ctypes.c_int32, [ctypes.POINTER(_LodView), ctypes.c_void_p,
+                                                ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32,
+                                                _u32p]),
+    "sk_lod_depth": (ctypes.c_int64, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
+    "sk_world_bytes": (ctypes.c_uint64, [ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint64,
+                                         ctypes.c_uint64, ctypes.c_uint64]),
+    "sk_lod_threshold_update": (ctypes.c_float, [_f32p, ctypes.c_uint32, ctypes.c_uint32,
+                                                 ctypes.c_uint32]),
+    "sk_radix_argsort_device": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                 ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_size_t, ctypes.c_void_p,
+                                                 ctypes.c_void_p]),
+}
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def library() -> ctypes.CDLL:
+    """Loads libsplatkit_b200.so (built in-tree by ``make -C splatkit-ios_b200``)."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            raise SplatError(SK_E_DEVICE, f"{LIBRARY_PATH} is not built")
+        lib = ctypes.CDLL(str(LIBRARY_PATH))
+        for name, (restype, argtypes) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+def exported_symbols() -> Sequence[str]:
+    return tuple(_SIGNATURES)
+
+
+def _ptr(a: Optional[np.ndarray], kind=_f32p):
+    if a is None:
+        return ctypes.cast(None, kind)
+    return a.ctypes.data_as(kind)
+
+
+# ---- world data ---------------------------------------------------------------------------
+def sh_coefficients(degree: int) -> int:
+    return 0 if degree <= 0 else (degree + 1) ** 2 - 1
+
+
+@dataclass
+class Cloud:
+    """A SplatCloud (splat-core/include/splat/formats/SplatCloud.h:30-51), structure of arrays."""
+
+    positions: np.ndarray  # (n, 3) float32
+    covariances: np.ndarray  # (n, 6) float32: xx, xy, xz, yy, yz, zz
+    colors: np.ndarray  # (n, 3) float32 in [0, 1]
+    alphas: np.ndarray  # (n,) float32
+    sh_degree: int = 0
+    sh: Optional[np.ndarray] = None  # (n, 3 * coefficients) float32, channel fastest
+    bounds_min: Optional[np.ndarray] = None
+    bounds_max: Optional[np.ndarray] = None
+
+    def __post_init__(self):
+        self.positions = np.ascontiguousarray(self.positions, np.float32).reshape(-1, 3)
+        self.covariances = np.ascontiguousarray(self.covariances, np.float32).reshape(-1, 6)
+        self.colors = np.ascontiguousarray(self.colors, np.float32).reshape(-1, 3)
+        self.alphas = np.ascontiguousarray(self.alphas, np.float32).reshape(-1)
+        if self.sh is not None:
+            self.sh = np.ascontiguousarray(self.sh, np.float32).reshape(len(self.alphas), -1)
+
+    @property
+    def count(self) -> int:
+        return int(self.alphas.shape[0])
+
+    def view(self) -> _Cloud:
+        return _Cloud(_ptr(self.positions), _ptr(self.covariances), _ptr(self.colors),
+                      _ptr(self.alphas), _ptr(self.sh if self.sh_degree > 0 else None),
+                      self.count, self.sh_degree)
+
+
+@dataclass
+class LodTree:
+    """A LodTree (splat-core/include/splat/lod/LodTree.h:47-55): nodes in layout order."""
+
+    nodes: Cloud
+    layout: np.ndarray  # LOD_NODE_DTYPE
+    leaf_count: int
+    clusters: Optional[np.ndarray] = None  # LOD_CLUSTER_DTYPE
+    leaves: Optional[np.ndarray] = None  # uint32 leaf references
+
+    def view(self) -> _LodView:
+        layout = np.ascontiguousarray(self.layout)
+        self._keep = [layout]
+        clusters = None if self.clusters is None else np.ascontiguousarray(self.clusters)
+        leaves = None if self.leaves is None else np.ascontiguousarray(self.leaves, np.uint32)
+        self._keep += [clusters, leaves]
+        return _LodView(self.nodes.view(), layout.ctypes.data, len(layout), self.leaf_count,
+                        None if clusters is None else clusters.ctypes.data,
+                        0 if clusters is None else len(clusters),
+                        _ptr(leaves, _u32p), 0 if leaves is None else len(leaves))
+
+
+@dataclass
+class Policy:
+    """RenderPolicy (splatkit-engine/include/splatkit/rendering/RenderPolicy.h:17-40)."""
+
+    lod_error_pixels: float = 1.0
+    lod_splat_limit: int = 0
+    alpha_threshold: float = 1.0 / 255.0
+    subpixel_threshold: float = 1.0
+    enable_frustum_culling: bool = True
+    enable_early_termination: bool = True
+    sort_depth_bits: int = 16
+    background: tuple = (0.05, 0.05, 0.08)
+
+    def native(self) -> _Policy:
+        p = _Policy()
+        p.lod_error_pixels = self.lod_error_pixels
+        p.lod_splat_limit = self.lod_splat_limit
+        p.alpha_threshold = self.alpha_threshold
+        p.subpixel_threshold = self.subpixel_threshold
+        p.enable_frustum_culling = int(self.enable_frustum_culling)
+        p.enable_early_termination = int(self.enable_early_termination)
+        p.sort_depth_bits = self.sort_depth_bits
+        for i in range(3):
+            p.background[i] = float(self.background[i])
+        return p
+
+
+@dataclass
+class Frame:
+    """SplatRenderer::Frame (SplatRenderer.h:111-131) for the GPU order source."""
+
+    view: np.ndarray  # (16,) column major
+    proj: np.ndarray  # (16,) column major
+    camera_position: np.ndarray  # (3,)
+    ranges: Sequence[tuple] = ()
+    sh_degree: int = 0
+    reveal_level: float = float("inf")
+
+    def native(self):
+        f = _Frame()
+        view = np.asarray(self.view, np.float32).reshape(16)
+        proj = np.asarray(self.proj, np.float32).reshape(16)
+        for i in range(16):
+            f.view[i] = float(view[i])
+            f.proj[i] = float(proj[i])
+        pos = np.asarray(self.camera_position, np.float32).reshape(3)
+        for i in range(3):
+            f.camera_position[i] = float(pos[i])
+        f.reveal_level = self.reveal_level
+        ranges = (_Range * max(1, len(self.ranges)))(*[_Range(int(o), int(c)) for o, c in self.ranges])
+        f.ranges = ctypes.cast(ranges, ctypes.POINTER(_Range)) if len(self.ranges) else None
+        f.range_count = len(self.ranges)
+        f.sh_degree = self.sh_degree
+        return f, ranges
+
+
+# ---- the renderer -------------------------------------------------------------------------
+class Renderer:
+    """A headless splat renderer on one CUDA device (``CudaSplatRenderer``'s Python mirror)."""
+
+    def __init__(self, width: int, height: int, device: int = 0, image_format: int = FORMAT_RGBA8,
+                 time_stages: bool = True):
+        self._lib = library()
+        cfg = _Config(device, width, height, image_format, 1 if time_stages else 0)
+        handle = ctypes.c_void_p()
+        st = self._lib.sk_create(ctypes.byref(cfg), ctypes.byref(handle))
+        if st != SK_OK:
+            raise SplatError(st, "sk_create failed (is a CUDA device visible?)")
+        self._h = handle
+        self.width, self.height, self.image_format = width, height, image_format
+
+    # lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sk_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st != SK_OK:
+            msg = self._lib.sk_last_error(self._h)
+            raise SplatError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    # SplatRenderer verbs
+    def resize(self, width: int, height: int):
+        self._check(self._lib.sk_resize(self._h, width, height), "resize")
+        self.width, self.height = width, height
+
+    def device_capabilities(self) -> dict:
+        caps = _Caps()
+        self._check(self._lib.sk_device_capabilities(self._h, ctypes.byref(caps)), "capabilities")
+        return {name: getattr(caps, name) for name, _ in _Caps._fields_}
+
+    def apply_render_policy(self, policy: Policy):
+        p = policy.native()
+        self._check(self._lib.sk_apply_render_policy(self._h, ctypes.byref(p)), "policy")
+
+    def available_memory(self) -> int:
+        v = ctypes.c_uint64()
+        self._check(self._lib.sk_available_memory(self._h, ctypes.byref(v)), "memory")
+        return v.value
+
+    def gpu_failed(self) -> bool:
+        return bool(self._lib.sk_gpu_failed(self._h))
+
+    def upload_world(self, cloud: Cloud, max_sh_degree: int = 3):
+        v = cloud.view()
+        self._check(self._lib.sk_upload_world(self._h, ctypes.byref(v), max_sh_degree), "upload")
+
+    def upload_lod_world(self, tree: LodTree, max_sh_degree: int, budget: int):
+        v = tree.view()
+        self._check(self._lib.sk_upload_lod_world(self._h, ctypes.byref(v), max_sh_degree, budget),
+                    "LOD upload")
+
+    def create_slab(self, capacity: int, sh_degree: int):
+        self._check(self._lib.sk_create_slab(self._h, capacity, sh_degree), "slab")
+
+    def upload_tile(self, offset: int, cloud: Cloud):
+        v = cloud.view()
+        self._check(self._lib.sk_upload_tile(self._h, offset, ctypes.byref(v)), "tile")
+
+    def world(self):
+        n = ctypes.c_uint32()
+        d = ctypes.c_int32()
+        st = self._lib.sk_world_info(self._h, ctypes.byref(n), ctypes.byref(d))
+        if st == SK_E_NO_WORLD:
+            return None
+        self._check(st, "world")
+        return n.value, d.value
+
+    def draw(self, frame: Frame):
+        f, keep = frame.native()
+        self._check(self._lib.sk_draw(self._h, ctypes.byref(f)), "draw")
+        del keep
+
+    def wait_idle(self):
+        self._check(self._lib.sk_wait_idle(self._h), "wait")
+
+    def read_image(self, fmt: int = None, out: Optional[np.ndarray] = None) -> np.ndarray:
+        fmt = self.image_format if fmt is None else fmt
+        if out is None:
+            if fmt == FORMAT_RGBA32F:
+                out = np.empty((self.height, self.width, 4), np.float32)
+            else:
+                out = np.empty((self.height, self.width, 4), np.uint8)
+        self._check(self._lib.sk_read_image(self._h, out.ctypes.data, out.nbytes, fmt), "read image")
+        return out
+
+    def stats(self) -> dict:
+        s = _Stats()
+        self._check(self._lib.sk_get_stats(self._h, ctypes.byref(s)), "stats")
+        return {name: getattr(s, name) for name, _ in _Stats._fields_ if name != "pad"}
+
+    def read_visible(self):
+        n = ctypes.c_uint32()
+        self._check(self._lib.sk_read_visible(self._h, None, None, 0, ctypes.byref(n)), "visible")
+        keys = np.empty(n.value, np.uint32)
+        proj = np.empty(n.value, PROJECTED_DTYPE)
+        self._check(self._lib.sk_read_visible(self._h, _ptr(keys, _u32p), proj.ctypes.data,
+                                              n.value, ctypes.byref(n)), "visible")
+        return keys, proj
+
+    def read_order(self) -> np.ndarray:
+        n = ctypes.c_uint32()
+        self._check(self._lib.sk_read_order(self._h, None, 0, ctypes.byref(n)), "order")
+        order = np.empty(n.value, np.uint32)
+        self._check(self._lib.sk_read_order(self._h, _ptr(order, _u32p), n.value,
+                                            ctypes.byref(n)), "order")
+        return order
+
+    def read_cut(self):
+        n = ctypes.c_uint32()
+        stats = np.zeros(6, np.uint32)
+        self._check(self._lib.sk_read_cut(self._h, None, 0, ctypes.byref(n), _ptr(stats, _u32p)),
+                    "cut")
+        cut = np.empty(n.value, np.uint32)
+        self._check(self._lib.sk_read_cut(self._h, _ptr(cut, _u32p), n.value, ctypes.byref(n),
+                                          _ptr(stats, _u32p)), "cut")
+        return cut, stats
+
+
+def radix_argsort_device(keys_ptr: int, count_ptr: int, capacity: int, bits: int, order_ptr: int,
+                         workspace_ptr: int, workspace_bytes: int, error_ptr: int, stream: int = 0):
+    """The standalone sort operator over caller device memory (MetalRadixSort's contract)."""
+    st = library().sk_radix_argsort_device(keys_ptr, count_ptr, capacity, bits, order_ptr,
+                                           workspace_ptr, workspace_bytes, error_ptr, stream)
+    if st != SK_OK:
+        raise SplatError(st, "sk_radix_argsort_device")
+
+
+def sort_workspace_bytes(capacity: int) -> int:
+    return int(library().sk_sort_workspace_bytes(capacity))
+
+
+# ---- host-side world preparation (no device needed) -----------------------------------------
+SPLAT_DTYPE = np.dtype([("position", "<f4", (3,)), ("rgba8", "<u4"), ("cov", "<u4", (3,)),
+                        ("lodAlpha", "<u4")])
+
+
+def sh_device_stride(degree: int) -> int:
+    return int(library().sk_sh_device_stride(degree))
+
+
+def pack_splats(cloud: Cloud) -> np.ndarray:
+    """The 32-byte GPU records of a cloud (GpuLayout.cpp:122-137)."""
+    out = np.empty(cloud.count, SPLAT_DTYPE)
+    v = cloud.view()
+    st = library().sk_pack_splats(ctypes.byref(v), 0, cloud.count, out.ctypes.data)
+    if st != SK_OK:
+        raise SplatError(st, "sk_pack_splats")
+    return out
+
+
+def pack_sh(cloud: Cloud, degree: int, stride: Optional[int] = None) -> np.ndarray:
+    """Harmonics halves, channel fastest, `stride` words per splat (GpuLayout.cpp:92-113)."""
+    stride = sh_device_stride(degree) if stride is None else stride
+    out = np.zeros((cloud.count, max(stride, 1)), np.uint32)
+    v = cloud.view()
+    st = library().sk_pack_sh(ctypes.byref(v), degree, 0, cloud.count, _ptr(out, _u32p), stride)
+    if st != SK_OK:
+        raise SplatError(st, "sk_pack_sh")
+    return out[:, :stride]
+
+
+def build_lod_selection(tree: LodTree):
+    """The interior clusters and leaf references of a tree (LodSelection.cpp:47-133)."""
+    v = tree.view()
+    nc, nl = ctypes.c_uint32(), ctypes.c_uint32()
+    lib = library()
+    st = lib.sk_build_lod_selection(ctypes.byref(v), None, 0, ctypes.byref(nc), None, 0,
+                                    ctypes.byref(nl))
+    if st != SK_OK:
+        raise SplatError(st, "sk_build_lod_selection")
+    clusters = np.empty(nc.value, LOD_CLUSTER_DTYPE)
+    leaves = np.empty(nl.value, np.uint32)
+    st = lib.sk_build_lod_selection(ctypes.byref(v), clusters.ctypes.data, nc.value,
+                                    ctypes.byref(nc), _ptr(leaves, _u32p), nl.value,
+                                    ctypes.byref(nl))
+    if st != SK_OK:
+        raise SplatError(st, "sk_build_lod_selection")
+    return clusters, leaves
+
+
+def lod_depth(layout: np.ndarray, leaf_count: int) -> int:
+    layout = np.ascontiguousarray(layout, LOD_NODE_DTYPE)
+    return int(library().sk_lod_depth(layout.ctypes.data, len(layout), leaf_count))
+
+
+def world_bytes(records: int, sh_degree: int, draw_capacity: int, clusters: int = 0,
+                leaf_refs: int = 0) -> int:
+    return int(library().sk_world_bytes(records, sh_degree, draw_capacity, clusters, leaf_refs))
+
+
+def lod_threshold_update(state: np.ndarray, selected: int, limited: int, limit: int) -> float:
+    """state: float32[2] = (policy pixels, current pixels), updated in place."""
+    return float(library().sk_lod_threshold_update(_ptr(state), selected, limited, limit))
