@@ -156,7 +156,10 @@ __global__ void __launch_bounds__(kThreads)
                       const uint32_t* __restrict__ frontier, uint32_t epoch) {
   LodState* st = a.state;
   const uint32_t tile = takeTile(a.counters);
-  const uint32_t active = st->active;
+  // The guard keeps the frontier within the capacity; clamp anyway so no index leaves the
+  // buffers (and say so).
+  const uint32_t active = min(st->active, a.frontierCapacity);
+  if (tile == 0 && threadIdx.x == 0 && st->active > a.frontierCapacity) atomicOr(a.error, SK_DEVERR_BOUNDS);
   const uint32_t tiles = (active + kTileClusters - 1) / kTileClusters;
   if (tile < tiles) {
     uint32_t extra[1][kItems], word[kItems];
@@ -246,7 +249,7 @@ __global__ void __launch_bounds__(kThreads)
                      RoundSums* sums, uint32_t epoch) {
   LodState* st = a.state;
   const uint32_t tile = takeTile(a.counters);
-  const uint32_t active = st->active;
+  const uint32_t active = min(st->active, a.frontierCapacity);
   const uint32_t accepted = st->accepted;
   const uint32_t tiles = (active + kTileClusters - 1) / kTileClusters;
   if (tile < tiles) {
@@ -310,7 +313,7 @@ __global__ void __launch_bounds__(kThreads)
     lodScatterKernel(const __grid_constant__ LodArgs a, const uint32_t* __restrict__ frontier,
                      uint32_t* __restrict__ next) {
   const LodState* st = a.state;
-  const uint32_t active = st->scatterActive;
+  const uint32_t active = min(st->scatterActive, a.frontierCapacity);
   const uint32_t countBase = st->scatterCount, packetBase = st->scatterPackets;
   for (uint32_t t = blockIdx.x * kThreads + threadIdx.x; t < active; t += gridDim.x * kThreads) {
     const uint4 local = a.offsets[t];
@@ -327,7 +330,10 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t count = split ? node.leafCount : 1;
     const uint32_t destination = countBase + local.y;
     if (count > 32) {
-      a.packets[packetBase + local.z] = make_uint4(node.leafStart, count, destination, 1);
+      if (packetBase + local.z < a.frontierCapacity)
+        a.packets[packetBase + local.z] = make_uint4(node.leafStart, count, destination, 1);
+      else
+        atomicOr(a.error, SK_DEVERR_BOUNDS);
     } else if (destination + count > a.capacity) {
       atomicOr(a.error, SK_DEVERR_BOUNDS);
     } else if (!split) {
@@ -339,7 +345,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void __launch_bounds__(kThreads) lodEmitKernel(const __grid_constant__ LodArgs a) {
-  const uint32_t packets = a.state->packets;
+  const uint32_t packets = min(a.state->packets, a.frontierCapacity);
   for (uint32_t p = blockIdx.x; p < packets; p += gridDim.x) {
     const uint4 packet = a.packets[p];
     if (packet.z + packet.y > a.capacity) {

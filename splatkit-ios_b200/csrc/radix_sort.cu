@@ -190,11 +190,18 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (uint32_t r = 0; r < kPerThread; ++r) {
       const uint32_t i = threadIdx.x + r * kThreads;
+      dst[r] = 0xffffffffu;
       if (i < inTile) {
         const uint32_t k = s.stage[i];
         const uint32_t dd = (k >> shift) & 0xffu;
-        dst[r] = s.globalBase[dd] + (i - s.localOffset[dd]);
-        if (kWriteKeys) keysOut[dst[r]] = k;
+        const uint32_t at = s.globalBase[dd] + (i - s.localOffset[dd]);
+        // Only a look-back that gave up can put `at` past the end; never write there.
+        if (at < n) {
+          dst[r] = at;
+          if (kWriteKeys) keysOut[at] = k;
+        } else {
+          atomicOr(error, SK_DEVERR_BOUNDS);
+        }
       }
     }
     __syncthreads();
@@ -207,7 +214,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (uint32_t r = 0; r < kPerThread; ++r) {
       const uint32_t i = threadIdx.x + r * kThreads;
-      if (i < inTile) valuesOut[dst[r]] = s.stage[i];
+      if (i < inTile && dst[r] != 0xffffffffu) valuesOut[dst[r]] = s.stage[i];
     }
   }
   finishTile(counters);

@@ -14,7 +14,8 @@ namespace sk {
 // ---- visibility (visibility.cu) --------------------------------------------------------
 struct VisibilityArgs {
   const GpuSplat* splats;
-  const uint32_t* sh;  // device stride shDeviceStride(degree) words per splat
+  const uint32_t* sh;  // shStride words per splat
+  uint32_t shStride;   // shDeviceStride(world degree); the frame may use fewer bands
   uint32_t worldCount;
   const Range* ranges;  // ranges mode
   const uint32_t* rangeStarts;

@@ -41,9 +41,9 @@ template <int D>
 struct ShWords {
   static constexpr uint32_t kWords = shDeviceStride(D);
   uint32_t w[kWords > 0 ? kWords : 1];
-  __device__ __forceinline__ void load(const uint32_t* sh, uint32_t index) {
+  __device__ __forceinline__ void load(const uint32_t* sh, uint32_t index, uint32_t stride) {
     if constexpr (kWords > 0) {
-      const uint4* p = reinterpret_cast<const uint4*>(sh + static_cast<size_t>(index) * kWords);
+      const uint4* p = reinterpret_cast<const uint4*>(sh + static_cast<size_t>(index) * stride);
 #pragma unroll
       for (uint32_t i = 0; i < kWords / 4; ++i) {
         const uint4 v = __ldg(p + i);
@@ -107,7 +107,7 @@ __device__ __forceinline__ void shColor(const ShWords<D>& s, float x, float y, f
 // Projected record and the depth key; returns whether the splat survives.
 template <int D, bool kKey16>
 __device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, const uint4 hi,
-                                             uint32_t index, const uint32_t* sh,
+                                             uint32_t index, const uint32_t* sh, uint32_t shStride,
                                              uint32_t& key, uint32_t* out) {
   const float px = asF(lo.x), py = asF(lo.y), pz = asF(lo.z);
   const uint32_t rgba8 = lo.w;
@@ -205,7 +205,7 @@ __device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, 
                   static_cast<float>((rgba8 >> 16) & 0xffu) / 255.0f};
   if constexpr (D >= 1) {
     ShWords<D> words;
-    words.load(sh, index);
+    words.load(sh, index, shStride);
     const float dx = px - cam.cameraPosition[0];
     const float dy = py - cam.cameraPosition[1];
     const float dz = pz - cam.cameraPosition[2];
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kThreads)
         if (index < a.worldCount) {
           const uint4* p = reinterpret_cast<const uint4*>(a.splats + index);
           const uint4 lo = __ldg(p), hi = __ldg(p + 1);
-          visible = projectSplat<D, kKey16>(cam, lo, hi, index, a.sh, key[r], rec[r]);
+          visible = projectSplat<D, kKey16>(cam, lo, hi, index, a.sh, a.shStride, key[r], rec[r]);
         } else {
           atomicOr(a.error, SK_DEVERR_BOUNDS);
         }

@@ -250,6 +250,7 @@ sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t
     VisibilityArgs v{};
     v.splats = static_cast<const GpuSplat*>(world.splats.ptr);
     v.sh = static_cast<const uint32_t*>(world.sh.ptr);
+    v.shStride = shDeviceStride(world.shDegree);
     v.worldCount = world.count;
     v.ranges = static_cast<const Range*>(f.rangeBuffer.ptr);
     v.rangeStarts = static_cast<const uint32_t*>(f.rangeStarts.ptr);
