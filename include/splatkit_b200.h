@@ -148,7 +148,7 @@ typedef struct {
   uint32_t device_error;   /* SK_DEVERR bits of the last frame */
   uint64_t fragments;      /* blended pixel x splat pairs */
   float lod_pixels;        /* the adapted LOD threshold in use */
-  uint32_t pad;
+  uint32_t instances_read; /* tile-list records the composite read before termination */
 } sk_stats;
 
 /* ---- context (SplatRenderer lifetime, deviceCapabilities, applyRenderPolicy) ---------- */
@@ -186,6 +186,11 @@ sk_status sk_read_visible(sk_context* ctx, uint32_t* keys, void* projected, uint
 sk_status sk_read_order(sk_context* ctx, uint32_t* order, uint32_t capacity, uint32_t* count);
 sk_status sk_read_cut(sk_context* ctx, uint32_t* indices, uint32_t capacity, uint32_t* count,
                       uint32_t* lod_counters6);
+/* The last frame's tile lists: ranges[2 * t], ranges[2 * t + 1] = [start, end) of 16x16 tile
+ * t (row major) in `values`, which holds projected-record indices front to back per tile.
+ * ranges needs 2 * tiles words; *count receives the number of list entries. */
+sk_status sk_read_tile_lists(sk_context* ctx, uint32_t* ranges, uint32_t* values,
+                             uint32_t capacity, uint32_t* count);
 
 /* ---- component operators over caller device memory ----------------------------------- */
 /* MetalRadixSort (splatkit-ios/.../metal/sort/MetalRadixSort.h:13-54): stable ascending argsort

@@ -11,9 +11,10 @@
 //
 // Each block walks its tile's list in batches of 256 records. Thread i fetches record i of the
 // batch (two 128-bit loads), turns it into the coverage form (pixel centre, inverse axes,
-// radius, log cutoff, colour) in shared memory, then every thread sweeps the batch. The
-// coverage decision uses explicit round-to-nearest intrinsics in a fixed order, so it is
-// bit-identical to the host oracle's FP32 formula.
+// radius, log cutoff, colour, pixel box) in shared memory, then every warp sweeps the batch
+// over its 8x4 pixels, skipping at once the splats whose box misses them. The coverage decision
+// uses explicit round-to-nearest intrinsics in a fixed order, so it is bit-identical to the
+// host oracle's FP32 formula.
 #include <cuda_runtime.h>
 
 #include "sk_device.cuh"
@@ -23,11 +24,15 @@ namespace sk {
 namespace {
 
 constexpr uint32_t kThreads = kTileSize * kTileSize;  // 256
+constexpr uint32_t kWarpCols = 8, kWarpRows = 4;      // a warp's pixels
 
-struct Splat2D {
-  float cx, cy, m00, m01, m10, m11, radius, lcut;
+struct alignas(16) Splat2D {
+  float cx, cy, m00, m01;
+  float m10, m11, radius, lcut;
   float alpha, r, g, b;
+  float x0, x1, y0, y1;  // box (y up) outside which no pixel centre is covered
 };
+static_assert(sizeof(Splat2D) == 64, "Splat2D is four 16-byte words");
 
 __device__ __forceinline__ Splat2D coverageForm(const uint4 lo, const uint4 hi, float halfW,
                                                 float halfH) {
@@ -50,6 +55,12 @@ __device__ __forceinline__ Splat2D coverageForm(const uint4 lo, const uint4 hi, 
   s.r = lowHalf(hi.x);
   s.g = highHalf(hi.x);
   s.b = lowHalf(hi.y);
+  // |s|,|t| <= radius bounds the offset by radius * (|a1| + |a2|) per axis; half a pixel of
+  // slack keeps the box conservative against the rounding of the inverse.
+  const float ex = s.radius * (fabsf(a1x) + fabsf(a2x)) + 0.5f;
+  const float ey = s.radius * (fabsf(a1y) + fabsf(a2y)) + 0.5f;
+  s.x0 = s.cx - ex, s.x1 = s.cx + ex, s.y0 = s.cy - ey, s.y1 = s.cy + ey;
+  if (!any) s.x0 = 1.0f, s.x1 = -1.0f;
   return s;
 }
 
@@ -58,46 +69,57 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   __shared__ Splat2D batch[kThreads];
   const uint32_t tile = blockIdx.x;
   const uint32_t tx = tile % a.tilesX, ty = tile / a.tilesX;
-  const uint32_t col = tx * kTileSize + (threadIdx.x % kTileSize);
-  const uint32_t row = ty * kTileSize + (threadIdx.x / kTileSize);
+  const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+  const uint32_t wx = warp & 1u, wy = warp >> 1;
+  const uint32_t col0 = tx * kTileSize + wx * kWarpCols;
+  const uint32_t row0 = ty * kTileSize + wy * kWarpRows;
+  const uint32_t col = col0 + (lane % kWarpCols);
+  const uint32_t row = row0 + (lane / kWarpCols);
   const bool inside = col < a.width && row < a.height;
+  const float height = static_cast<float>(a.height);
   const float px = static_cast<float>(col) + 0.5f;
   const float py = static_cast<float>(a.height - row) - 0.5f;  // y up, as NDC
+  // the warp's pixel centres, y up
+  const float wx0 = static_cast<float>(col0) + 0.5f, wx1 = wx0 + (kWarpCols - 1);
+  const float wy1 = height - (static_cast<float>(row0) + 0.5f), wy0 = wy1 - (kWarpRows - 1);
   const float halfW = 0.5f * static_cast<float>(a.width);
-  const float halfH = 0.5f * static_cast<float>(a.height);
+  const float halfH = 0.5f * height;
   const uint2 range = a.ranges[tile];
   float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
   bool done = !inside;
-  uint32_t blended = 0;
+  uint32_t blended = 0, loaded = 0;
   for (uint32_t start = range.x; start < range.y; start += kThreads) {
-    const uint32_t i = start + threadIdx.x;
-    if (i < range.y) {
-      const uint32_t v = a.values[i];
+    const uint32_t inBatch = min(kThreads, range.y - start);
+    loaded += inBatch;
+    if (threadIdx.x < inBatch) {
+      const uint32_t v = a.values[start + threadIdx.x];
       const uint4* p = reinterpret_cast<const uint4*>(a.projected + v);
       batch[threadIdx.x] = coverageForm(__ldg(p), __ldg(p + 1), halfW, halfH);
     }
     __syncthreads();
-    const uint32_t inBatch = min(kThreads, range.y - start);
-    if (!done) {
+    if (!__all_sync(0xffffffffu, done)) {
       for (uint32_t j = 0; j < inBatch; ++j) {
-        const Splat2D& s = batch[j];
-        const float dx = __fsub_rn(px, s.cx), dy = __fsub_rn(py, s.cy);
-        const float u = __fadd_rn(__fmul_rn(s.m00, dx), __fmul_rn(s.m01, dy));
-        const float w = __fadd_rn(__fmul_rn(s.m10, dx), __fmul_rn(s.m11, dy));
-        if (!(fabsf(u) <= s.radius && fabsf(w) <= s.radius)) continue;
-        const float q = __fmul_rn(0.5f, __fadd_rn(__fmul_rn(u, u), __fmul_rn(w, w)));
-        if (!(q <= s.lcut)) continue;
-        const float alpha = fminf(s.alpha * __expf(-q), 1.0f);
+        const float4 box = reinterpret_cast<const float4*>(&batch[j])[3];
+        // warp-uniform: the splat's box misses all 32 pixel centres of this warp
+        if (box.y < wx0 || box.x > wx1 || box.w < wy0 || box.z > wy1) continue;
+        if (done) continue;
+        const float4 w0 = reinterpret_cast<const float4*>(&batch[j])[0];
+        const float4 w1 = reinterpret_cast<const float4*>(&batch[j])[1];
+        const float dx = __fsub_rn(px, w0.x), dy = __fsub_rn(py, w0.y);
+        const float u = __fadd_rn(__fmul_rn(w0.z, dx), __fmul_rn(w0.w, dy));
+        const float v = __fadd_rn(__fmul_rn(w1.x, dx), __fmul_rn(w1.y, dy));
+        if (!(fabsf(u) <= w1.z && fabsf(v) <= w1.z)) continue;
+        const float q = __fmul_rn(0.5f, __fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)));
+        if (!(q <= w1.w)) continue;
+        const float4 c = reinterpret_cast<const float4*>(&batch[j])[2];
+        const float alpha = fminf(c.x * __expf(-q), 1.0f);
         const float weight = T * alpha;
-        cr += weight * s.r;
-        cg += weight * s.g;
-        cb += weight * s.b;
+        cr += weight * c.y;
+        cg += weight * c.z;
+        cb += weight * c.w;
         T *= 1.0f - alpha;
         ++blended;
-        if (T < a.cutoff) {
-          done = true;
-          break;
-        }
+        if (T < a.cutoff) done = true;
       }
     }
     if (__syncthreads_count(done ? 0 : 1) == 0) break;
@@ -108,10 +130,11 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   __syncthreads();
   uint32_t warpSum = blended;
   for (int o = 16; o > 0; o >>= 1) warpSum += __shfl_xor_sync(0xffffffffu, warpSum, o);
-  if (laneId() == 0 && warpSum) atomicAdd(&blockFragments, static_cast<unsigned long long>(warpSum));
+  if (lane == 0 && warpSum) atomicAdd(&blockFragments, static_cast<unsigned long long>(warpSum));
   __syncthreads();
   if (threadIdx.x == 0 && blockFragments)
     atomicAdd(reinterpret_cast<unsigned long long*>(a.fragments), blockFragments);
+  if (threadIdx.x == 0 && loaded) atomicAdd(a.loaded, loaded);
   if (!inside) return;
   float outR, outG, outB, outA;
   if (a.opaque) {

@@ -17,9 +17,10 @@ struct VisibilityArgs {
   const uint32_t* sh;  // shStride words per splat
   uint32_t shStride;   // shDeviceStride(world degree); the frame may use fewer bands
   uint32_t worldCount;
-  const Range* ranges;  // ranges mode
+  const Range* ranges;  // ranges mode (device), used when rangeCount > 1
   const uint32_t* rangeStarts;
   uint32_t rangeCount;
+  Range single;  // the range itself when rangeCount == 1 (no device copy needed)
   const uint32_t* indices;     // indexed (LOD) mode
   const uint32_t* indexCount;  // indexed mode: entries in indices (device)
   uint32_t total;              // ranges mode: sum of counts; indexed mode: capacity bound
@@ -103,6 +104,7 @@ struct CompositeArgs {
   void* image;   // row 0 on top
   int format;
   uint32_t* fragments;  // FrameCounters.fragments_lo/hi (64-bit add)
+  uint32_t* loaded;     // FrameCounters.loaded
 };
 cudaError_t launchComposite(const CompositeArgs& args, cudaStream_t stream);
 

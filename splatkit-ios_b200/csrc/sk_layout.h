@@ -87,7 +87,8 @@ struct FrameCounters {
   uint32_t lod[6];        // LOD counters of this frame
   uint32_t fragments_lo;  // blended fragments (pixel x splat), when counted
   uint32_t fragments_hi;
-  uint32_t pad[4];
+  uint32_t loaded;  // tile-list records the composite read before its tiles terminated
+  uint32_t pad[3];
 };
 static_assert(sizeof(FrameCounters) == 64, "FrameCounters is 64 bytes");
 

@@ -235,7 +235,7 @@ __device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, 
 }
 
 __device__ __forceinline__ uint32_t sourceIndex(const VisibilityArgs& a, uint32_t t) {
-  if (a.rangeCount == 1) return a.ranges[0].offset + t;
+  if (a.rangeCount == 1) return a.single.offset + t;
   // SplatVisibility.metal:30-37: the range whose start is the last one <= t.
   uint32_t lo = 0, hi = a.rangeCount;
   while (hi - lo > 1) {
@@ -245,42 +245,77 @@ __device__ __forceinline__ uint32_t sourceIndex(const VisibilityArgs& a, uint32_
   return a.ranges[lo].offset + (t - a.rangeStarts[lo]);
 }
 
+// Shared memory of one tile: survivors staged at their source slot, then compacted.
+struct VisibilitySmem {
+  uint4 rec[kTileSplats * 2];     // projected records by source slot
+  uint32_t key[kTileSplats];      // depth keys by source slot
+  uint16_t slotOf[kTileSplats];   // survivor k of the tile -> its source slot
+  uint32_t rowMask[kThreads / 32][kItems];
+  uint32_t warpBase[kThreads / 32];
+  uint32_t tileBase, tileCount;
+};
+
 template <int D, bool kKey16, bool kIndexed>
 __global__ void __launch_bounds__(kThreads)
     visibilityKernel(const __grid_constant__ Camera cam, const __grid_constant__ VisibilityArgs a) {
-  __shared__ uint32_t warpBase[kThreads / 32];
-  __shared__ uint32_t tileBase;
+  __shared__ VisibilitySmem s;
   const uint32_t tile = takeTile(a.counters);
   const uint32_t total = kIndexed ? min(*a.indexCount, a.total) : a.total;
   const uint32_t tiles = (total + kTileSplats - 1) / kTileSplats;
   if (tile < tiles) {
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
-    uint32_t key[kItems];
-    uint32_t rec[kItems][8];
-    uint32_t rowMask[kItems];
-#pragma unroll
+    const uint32_t first = tile * kTileSplats + warp * (32 * kItems) + lane;
+    // One splat per row of the warp, not unrolled (the projection is large); the next row's
+    // record is fetched while this one is projected.
+    auto indexOf = [&](uint32_t t) -> uint32_t {
+      if (t >= total) return 0xffffffffu;
+      const uint32_t index = kIndexed ? a.indices[t] : sourceIndex(a, t);
+      if (index >= a.worldCount) {
+        atomicOr(a.error, SK_DEVERR_BOUNDS);
+        return 0xffffffffu;
+      }
+      return index;
+    };
+    uint32_t index = indexOf(first);
+    uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
+    if (index != 0xffffffffu) {
+      const uint4* p = reinterpret_cast<const uint4*>(a.splats + index);
+      lo = __ldg(p), hi = __ldg(p + 1);
+    }
+#pragma unroll 1
     for (uint32_t r = 0; r < kItems; ++r) {
-      const uint32_t t = tile * kTileSplats + warp * (32 * kItems) + r * 32 + lane;
-      bool visible = false;
-      if (t < total) {
-        const uint32_t index = kIndexed ? a.indices[t] : sourceIndex(a, t);
-        if (index < a.worldCount) {
-          const uint4* p = reinterpret_cast<const uint4*>(a.splats + index);
-          const uint4 lo = __ldg(p), hi = __ldg(p + 1);
-          visible = projectSplat<D, kKey16>(cam, lo, hi, index, a.sh, a.shStride, key[r], rec[r]);
-        } else {
-          atomicOr(a.error, SK_DEVERR_BOUNDS);
+      uint32_t nextIndex = 0xffffffffu;
+      uint4 nextLo = make_uint4(0, 0, 0, 0), nextHi = nextLo;
+      if (r + 1 < kItems) {
+        nextIndex = indexOf(first + (r + 1) * 32);
+        if (nextIndex != 0xffffffffu) {
+          const uint4* p = reinterpret_cast<const uint4*>(a.splats + nextIndex);
+          nextLo = __ldg(p), nextHi = __ldg(p + 1);
         }
       }
-      rowMask[r] = __ballot_sync(0xffffffffu, visible);
+      bool visible = false;
+      const uint32_t slot = warp * (32 * kItems) + r * 32 + lane;
+      if (index != 0xffffffffu) {
+        uint32_t key, rec[8];
+        visible = projectSplat<D, kKey16>(cam, lo, hi, index, a.sh, a.shStride, key, rec);
+        if (visible) {
+          s.key[slot] = key;
+          s.rec[2 * slot] = make_uint4(rec[0], rec[1], rec[2], rec[3]);
+          s.rec[2 * slot + 1] = make_uint4(rec[4], rec[5], rec[6], rec[7]);
+        }
+      }
+      const uint32_t mask = __ballot_sync(0xffffffffu, visible);
+      if (lane == 0) s.rowMask[warp][r] = mask;
+      index = nextIndex, lo = nextLo, hi = nextHi;
     }
+    __syncwarp();
     uint32_t warpTotal = 0;
 #pragma unroll
-    for (uint32_t r = 0; r < kItems; ++r) warpTotal += __popc(rowMask[r]);
-    if (lane == 0) warpBase[warp] = warpTotal;
+    for (uint32_t r = 0; r < kItems; ++r) warpTotal += __popc(s.rowMask[warp][r]);
+    if (lane == 0) s.warpBase[warp] = warpTotal;
     __syncthreads();
     if (warp == 0) {
-      const uint32_t mine = lane < kThreads / 32 ? warpBase[lane] : 0u;
+      const uint32_t mine = lane < kThreads / 32 ? s.warpBase[lane] : 0u;
       uint32_t inclusive = mine;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -288,7 +323,7 @@ __global__ void __launch_bounds__(kThreads)
         if (lane >= static_cast<uint32_t>(o)) inclusive += up;
       }
       const uint32_t aggregate = __shfl_sync(0xffffffffu, inclusive, 31);
-      if (lane < kThreads / 32) warpBase[lane] = inclusive - mine;
+      if (lane < kThreads / 32) s.warpBase[lane] = inclusive - mine;
       uint32_t exclusive = 0;
       if (tile == 0) {
         if (lane == 0) storeStatus(a.status, makeStatus(a.epoch, kFlagPrefix, aggregate));
@@ -299,28 +334,38 @@ __global__ void __launch_bounds__(kThreads)
           storeStatus(a.status + tile, makeStatus(a.epoch, kFlagPrefix, exclusive + aggregate));
       }
       if (lane == 0) {
-        tileBase = exclusive;
+        s.tileBase = exclusive;
+        s.tileCount = aggregate;
         if (tile == tiles - 1) *a.visibleCount = exclusive + aggregate;
       }
     }
     __syncthreads();
-    uint32_t pos = tileBase + warpBase[warp];
-    const uint32_t below = lanemaskLt();
+    // survivor k of the tile <- its source slot, in source order
+    {
+      uint32_t pos = s.warpBase[warp];
+      const uint32_t below = lanemaskLt();
 #pragma unroll
-    for (uint32_t r = 0; r < kItems; ++r) {
-      if (rowMask[r] & (1u << lane)) {
-        const uint32_t at = pos + __popc(rowMask[r] & below);
-        a.keys[at] = key[r];
-        uint4* o = reinterpret_cast<uint4*>(a.projected + at);
-        o[0] = make_uint4(rec[r][0], rec[r][1], rec[r][2], rec[r][3]);
-        o[1] = make_uint4(rec[r][4], rec[r][5], rec[r][6], rec[r][7]);
+      for (uint32_t r = 0; r < kItems; ++r) {
+        const uint32_t mask = s.rowMask[warp][r];
+        if (mask & (1u << lane)) s.slotOf[pos + __popc(mask & below)] = warp * (32 * kItems) + r * 32 + lane;
+        pos += __popc(mask);
       }
-      pos += __popc(rowMask[r]);
+    }
+    __syncthreads();
+    // coalesced copy-out: consecutive threads write consecutive survivors
+    const uint32_t count = s.tileCount, base = s.tileBase;
+    for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
+      const uint32_t slot = s.slotOf[k];
+      a.keys[base + k] = s.key[slot];
+      uint4* o = reinterpret_cast<uint4*>(a.projected + base + k);
+      o[0] = s.rec[2 * slot];
+      o[1] = s.rec[2 * slot + 1];
     }
   }
   if (tiles == 0 && tile == 0 && threadIdx.x == 0) *a.visibleCount = 0;
   finishTile(a.counters);
 }
+
 
 template <int D, bool kKey16, bool kIndexed>
 void launchOne(const Camera& cam, const VisibilityArgs& a, uint32_t grid, cudaStream_t stream) {

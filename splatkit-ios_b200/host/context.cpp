@@ -236,8 +236,9 @@ sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t
   }
   if (timed) cudaEventRecord(f.events[1], s);
 
-  if (e == cudaSuccess && !lod && frame.range_count > 0) {
+  if (e == cudaSuccess && !lod && frame.range_count > 1) {
     // Ranges and their starts (SplatVisibility.metal:30-37); pageable copies are staged at once.
+    // A single range travels in the kernel parameters instead.
     std::vector<uint32_t> starts(frame.range_count + 1, 0);
     for (uint32_t i = 0; i < frame.range_count; ++i) starts[i + 1] = starts[i] + frame.ranges[i].count;
     e = cudaMemcpyAsync(f.rangeBuffer.ptr, frame.ranges, size_t{frame.range_count} * sizeof(Range),
@@ -255,6 +256,7 @@ sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t
     v.ranges = static_cast<const Range*>(f.rangeBuffer.ptr);
     v.rangeStarts = static_cast<const uint32_t*>(f.rangeStarts.ptr);
     v.rangeCount = lod ? 0 : frame.range_count;
+    if (!lod && frame.range_count == 1) v.single = Range{frame.ranges[0].offset, frame.ranges[0].count};
     v.indices = lod ? static_cast<const uint32_t*>(f.lodIndices.ptr) : nullptr;
     v.indexCount = lod ? &fc->lod[0] : nullptr;
     v.total = lod ? world.lodCapacity : total;
@@ -331,6 +333,7 @@ sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t
     c.image = f.image.ptr;
     c.format = imageFormat == SK_FORMAT_RGBA32F ? kRgba32f : kRgba8;
     c.fragments = &fc->fragments_lo;
+    c.loaded = &fc->loaded;
     e = launchComposite(c, s);
   }
   if (timed) cudaEventRecord(f.events[5], s);
@@ -750,6 +753,7 @@ sk_status sk_get_stats(sk_context* handle, sk_stats* out) {
   s.device_error = c.error;
   s.fragments = uint64_t{c.fragments_lo} | (uint64_t{c.fragments_hi} << 32);
   s.lod_pixels = ctx->threshold.pixels();
+  s.instances_read = c.loaded;
   *out = s;
   return SK_OK;
 }
@@ -889,3 +893,19 @@ float sk_lod_threshold_update(float* state, uint32_t selected, uint32_t limited,
 }
 
 }  // extern "C"
+
+extern "C" sk_status sk_read_tile_lists(sk_context* handle, uint32_t* ranges, uint32_t* values,
+                                        uint32_t capacity, uint32_t* count) {
+  SK_CTX(handle);
+  sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  const uint32_t n = std::min(ctx->lastCounters.instances, ctx->frame.instanceCapacity);
+  if (count) *count = n;
+  cudaError_t e = cudaSuccess;
+  const size_t tiles = size_t{ctx->frame.tilesX} * ctx->frame.tilesY;
+  if (ranges) e = cudaMemcpy(ranges, ctx->frame.ranges.ptr, tiles * 8, cudaMemcpyDeviceToHost);
+  const uint32_t copy = std::min(n, capacity);
+  if (e == cudaSuccess && values && copy)
+    e = cudaMemcpy(values, ctx->frame.instValuesSorted.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
+  return ctx->check(e, "readback");
+}

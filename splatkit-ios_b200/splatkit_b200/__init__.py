@@ -119,7 +119,7 @@ class _Stats(ctypes.Structure):
                 ("lod_limited", ctypes.c_uint32), ("lod_evaluated", ctypes.c_uint32),
                 ("instances", ctypes.c_uint32), ("device_error", ctypes.c_uint32),
                 ("fragments", ctypes.c_uint64), ("lod_pixels", ctypes.c_float),
-                ("pad", ctypes.c_uint32)]
+                ("instances_read", ctypes.c_uint32)]
 
 
 # Every function the header declares, with its ctypes signature.
@@ -148,6 +148,7 @@ _SIGNATURES = {
                                          _u32p]),
     "sk_read_order": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_uint32, _u32p]),
     "sk_read_cut": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_uint32, _u32p, _u32p]),
+    "sk_read_tile_lists": (ctypes.c_int32, [ctypes.c_void_p, _u32p, _u32p, ctypes.c_uint32, _u32p]),
     "sk_sort_workspace_bytes": (ctypes.c_size_t, [ctypes.c_uint32]),
     "sk_sh_device_stride": (ctypes.c_uint32, [ctypes.c_int32]),
     "sk_pack_splats": (ctypes.c_int32, [ctypes.POINTER(_Cloud), ctypes.c_uint32, ctypes.c_uint32,
@@ -416,7 +417,7 @@ class Renderer:
     def stats(self) -> dict:
         s = _Stats()
         self._check(self._lib.sk_get_stats(self._h, ctypes.byref(s)), "stats")
-        return {name: getattr(s, name) for name, _ in _Stats._fields_ if name != "pad"}
+        return {name: getattr(s, name) for name, _ in _Stats._fields_}
 
     def read_visible(self):
         n = ctypes.c_uint32()
@@ -434,6 +435,18 @@ class Renderer:
         self._check(self._lib.sk_read_order(self._h, _ptr(order, _u32p), n.value,
                                             ctypes.byref(n)), "order")
         return order
+
+    def read_tile_lists(self):
+        """(ranges (tiles, 2), values): each 16x16 tile's front-to-back projected indices."""
+        tiles = ((self.width + 15) // 16) * ((self.height + 15) // 16)
+        ranges = np.zeros((tiles, 2), np.uint32)
+        n = ctypes.c_uint32()
+        self._check(self._lib.sk_read_tile_lists(self._h, _ptr(ranges, _u32p), None, 0,
+                                                 ctypes.byref(n)), "tile lists")
+        values = np.empty(n.value, np.uint32)
+        self._check(self._lib.sk_read_tile_lists(self._h, _ptr(ranges, _u32p), _ptr(values, _u32p),
+                                                 n.value, ctypes.byref(n)), "tile lists")
+        return ranges, values
 
     def read_cut(self):
         n = ctypes.c_uint32()
