@@ -310,7 +310,8 @@ def run_ours(args):
                       "composite": "composite"}[dominant]
         traffic = traffic_from_profiles(kernel_tag)
         passes = 2 if args.bits == 16 else 4
-        launches_per_frame = 1 + (1 + passes) + 1 + 3 + 1 + 1
+        # visibility, depth sort (histogram + passes), bin count + emit, tile sort, ranges, composite
+        launches_per_frame = 1 + (1 + passes) + 2 + 3 + 1 + 1
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,

@@ -423,12 +423,13 @@ Support supportOf(const sko_projected& p, float width, float height) {
 }
 
 // The kernel's coverage test for pixel centre (px, py), y up. Writes q = (s^2 + t^2) / 2.
+// Each fma rounds once; every other product and sum rounds on its own.
 inline bool covers(const Support& s, float px, float py, float* q) {
   const float dx = px - s.cx, dy = py - s.cy;
-  const float u = s.m00 * dx + s.m01 * dy;
-  const float v = s.m10 * dx + s.m11 * dy;
+  const float u = std::fma(s.m00, dx, s.m01 * dy);
+  const float v = std::fma(s.m10, dx, s.m11 * dy);
   if (!(std::fabs(u) <= s.radius && std::fabs(v) <= s.radius)) return false;
-  const float qq = 0.5f * (u * u + v * v);
+  const float qq = 0.5f * std::fma(u, u, v * v);
   if (!(qq <= s.lcut)) return false;
   *q = qq;
   return true;

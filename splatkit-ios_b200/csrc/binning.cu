@@ -3,21 +3,18 @@
 // .../metal/cull/PrepareIndirect.metalh:4-21); this build composites 16x16 pixel tiles, so each
 // survivor is listed once per tile its quad touches.
 //
-// A splat's quad is the parallelogram c + s a1 + t a2, |s|, |t| <= radius, in pixel units (the
-// same half-rounded axes the compositor inverts). Its tiles are those of its pixel box whose
-// square it overlaps by the separating-axis test (x, y and the normals of a1 and a2); the tile
-// square is the pixel area, half a pixel beyond every pixel centre, so the test can only keep
-// too many tiles, never drop one the compositor would cover.
-//
-// One kernel walks the depth-sorted list, counts each splat's tiles, takes its output offset
-// by decoupled look-back, and writes (tile id, projected index) pairs. Offsets grow with depth
-// rank and the tile sort that follows is stable, so every tile's list stays front to back. A
-// count beyond the reserved capacity is recorded and nothing past it is written; the host
-// grows the buffers and draws again.
+// The visibility pass already decided each survivor's tiles (a span, sk_tiles.cuh). Binning walks
+// the depth-sorted list in blocks of 1024 ranks: one pass sums each block's tile count, the next
+// adds up the sums of the blocks before its own (no block waits on another) and writes
+// (tile id, projected index) pairs at its offsets. Offsets grow with depth rank and the tile sort
+// that follows is stable, so every tile's list stays front to back. A count beyond the reserved
+// capacity is recorded and nothing past it is written; the host grows the buffers and draws
+// again.
 #include <cuda_runtime.h>
 
 #include "sk_device.cuh"
 #include "sk_kernels.h"
+#include "sk_tiles.cuh"
 
 namespace sk {
 namespace {
@@ -26,80 +23,61 @@ constexpr uint32_t kThreads = 256;
 constexpr uint32_t kItems = 4;
 constexpr uint32_t kTileSplats = kThreads * kItems;
 
-// The quad in y-up pixel coordinates.
-struct Quad {
-  float cx, cy, a1x, a1y, a2x, a2y, r;
-};
-
-__device__ __forceinline__ Quad quadOf(const uint4 lo, const uint4 hi, float halfW, float halfH) {
-  Quad q;
-  q.cx = (asF(lo.x) + 1.0f) * halfW;
-  q.cy = (asF(lo.y) + 1.0f) * halfH;
-  q.a1x = lowHalf(lo.z), q.a1y = highHalf(lo.z);
-  q.a2x = lowHalf(lo.w), q.a2y = highHalf(lo.w);
-  q.r = asF(hi.z);
-  return q;
+// Pass 1: instances per block of 1024 depth ranks (no waiting on other blocks).
+__global__ void __launch_bounds__(kThreads) binCountKernel(const __grid_constant__ BinArgs a) {
+  __shared__ uint32_t warpSum[kThreads / 32];
+  const uint32_t n = min(*a.count, a.capacity);
+  const uint32_t block = blockIdx.x;
+  if (block * kTileSplats >= n) return;
+  uint32_t sum = 0;
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r) {
+    const uint32_t i = block * kTileSplats + r * kThreads + threadIdx.x;
+    if (i < n) sum += spanCount(__ldg(a.spans + __ldg(a.order + i)));
+  }
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (laneId() == 0) warpSum[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t total = 0;
+    for (uint32_t w = 0; w < kThreads / 32; ++w) total += warpSum[w];
+    a.blockSums[block] = total;
+  }
 }
 
-struct TileRect {
-  uint32_t x0, y0, x1, y1;  // inclusive tile bounds; empty when x0 > x1
-};
-
-// Tiles of the quad's pixel box (plus one pixel).
-__device__ __forceinline__ TileRect tileRect(const Quad& q, float width, float height,
-                                             uint32_t tilesX, uint32_t tilesY) {
-  TileRect t{1, 1, 0, 0};
-  const float ex = q.r * (fabsf(q.a1x) + fabsf(q.a2x)) + 1.0f;
-  const float ey = q.r * (fabsf(q.a1y) + fabsf(q.a2y)) + 1.0f;
-  if (!(isfinite(q.cx) && isfinite(q.cy) && isfinite(ex) && isfinite(ey) && q.r >= 0.0f)) return t;
-  const float xa = floorf(q.cx - ex), xb = ceilf(q.cx + ex);
-  const float ya = floorf(q.cy - ey), yb = ceilf(q.cy + ey);
-  if (xb < 0.0f || xa >= width || yb < 0.0f || ya >= height) return t;
-  // columns [c0, c1]; rows from the y-up box: row = H - y_up - 0.5
-  const uint32_t c0 = static_cast<uint32_t>(fmaxf(xa, 0.0f));
-  const uint32_t c1 = static_cast<uint32_t>(fminf(xb, width - 1.0f));
-  const uint32_t r0 = static_cast<uint32_t>(fmaxf(height - yb - 1.0f, 0.0f));
-  const uint32_t r1 = static_cast<uint32_t>(fminf(fmaxf(height - ya, 0.0f), height - 1.0f));
-  t.x0 = c0 / kTileSize;
-  t.x1 = min(c1 / kTileSize, tilesX - 1);
-  t.y0 = r0 / kTileSize;
-  t.y1 = min(r1 / kTileSize, tilesY - 1);
-  return t;
-}
-
-// Separating-axis test of the quad against tile (tx, ty)'s pixel square (y up).
-__device__ __forceinline__ bool touches(const Quad& q, uint32_t tx, uint32_t ty, float height) {
-  const float half = 0.5f * static_cast<float>(kTileSize);
-  const float rx = static_cast<float>(tx * kTileSize) + half;
-  const float ry = height - (static_cast<float>(ty * kTileSize) + half);
-  const float dx = rx - q.cx, dy = ry - q.cy;
-  if (fabsf(dx) > q.r * (fabsf(q.a1x) + fabsf(q.a2x)) + half) return false;
-  if (fabsf(dy) > q.r * (fabsf(q.a1y) + fabsf(q.a2y)) + half) return false;
-  // normal of a1: the quad's extent along it comes from t a2 only
-  const float n1x = -q.a1y, n1y = q.a1x;
-  if (fabsf(dx * n1x + dy * n1y) >
-      q.r * fabsf(q.a2x * n1x + q.a2y * n1y) + half * (fabsf(n1x) + fabsf(n1y)))
-    return false;
-  const float n2x = -q.a2y, n2y = q.a2x;
-  if (fabsf(dx * n2x + dy * n2y) >
-      q.r * fabsf(q.a1x * n2x + q.a1y * n2y) + half * (fabsf(n2x) + fabsf(n2y)))
-    return false;
-  return true;
-}
-
-__global__ void __launch_bounds__(kThreads) binKernel(const __grid_constant__ BinArgs a) {
+// Pass 2: each block sums the totals of the blocks before it, then writes its instances.
+__global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant__ BinArgs a) {
   __shared__ uint32_t warpBase[kThreads / 32];
   __shared__ uint32_t tileBase;
-  const uint32_t tile = takeTile(a.counters);
   const uint32_t n = min(*a.count, a.capacity);
   const uint32_t tiles = (n + kTileSplats - 1) / kTileSplats;
-  const float width = static_cast<float>(a.width), height = static_cast<float>(a.height);
-  const float halfW = 0.5f * width, halfH = 0.5f * height;
+  const uint32_t tile = blockIdx.x;
+  if (tile == 0 && threadIdx.x == 0 && tiles == 0) {
+    *a.instanceCount = 0;
+    *a.overflow = 0;
+  }
   if (tile < tiles) {
+    {
+      uint32_t before = 0;
+      for (uint32_t b = threadIdx.x; b < tile; b += kThreads) before += __ldcg(a.blockSums + b);
+      for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
+      if (laneId() == 0) warpBase[threadIdx.x >> 5] = before;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint32_t s = 0;
+        for (uint32_t w = 0; w < kThreads / 32; ++w) s += warpBase[w];
+        tileBase = s;
+        if (tile == tiles - 1) {
+          const uint32_t total = s + __ldcg(a.blockSums + tile);
+          *a.instanceCount = total;
+          *a.overflow = total > a.instanceCapacity ? 1u : 0u;
+        }
+      }
+      __syncthreads();
+    }
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
-    uint32_t value[kItems];
-    uint4 lo[kItems], hi[kItems];
-    // all loads first: the order entries, then the records they name
+    uint32_t value[kItems], cnt[kItems];
+    uint4 span[kItems];
 #pragma unroll
     for (uint32_t r = 0; r < kItems; ++r) {
       const uint32_t i = tile * kTileSplats + warp * (32 * kItems) + r * 32 + lane;
@@ -107,37 +85,8 @@ __global__ void __launch_bounds__(kThreads) binKernel(const __grid_constant__ Bi
     }
 #pragma unroll
     for (uint32_t r = 0; r < kItems; ++r) {
-      if (value[r] != 0xffffffffu) {
-        const uint4* p = reinterpret_cast<const uint4*>(a.projected + value[r]);
-        lo[r] = __ldg(p);
-        hi[r] = __ldg(p + 1);
-      }
-    }
-    // Each splat's tiles are decided once: a bit per tile of its box (row major), for boxes of
-    // up to 64 tiles; a larger box keeps all its tiles. The count and the emission both read
-    // this mask, so they cannot disagree.
-    uint32_t rx0[kItems], ry0[kItems], rw[kItems], area[kItems], cnt[kItems];
-    uint64_t mask[kItems];
-#pragma unroll
-    for (uint32_t r = 0; r < kItems; ++r) {
-      cnt[r] = 0, mask[r] = 0, area[r] = 0, rx0[r] = 0, ry0[r] = 0, rw[r] = 1;
-      if (value[r] == 0xffffffffu) continue;
-      const Quad q = quadOf(lo[r], hi[r], halfW, halfH);
-      const TileRect t = tileRect(q, width, height, a.tilesX, a.tilesY);
-      if (t.x0 > t.x1 || t.y0 > t.y1) continue;
-      rx0[r] = t.x0, ry0[r] = t.y0, rw[r] = t.x1 - t.x0 + 1;
-      area[r] = rw[r] * (t.y1 - t.y0 + 1);
-      if (area[r] > 64) {
-        cnt[r] = area[r];
-        continue;
-      }
-      uint64_t m = 0;
-      for (uint32_t k = 0; k < area[r]; ++k) {
-        const uint32_t tx = t.x0 + k % rw[r], ty = t.y0 + k / rw[r];
-        if (touches(q, tx, ty, height)) m |= 1ull << k;
-      }
-      mask[r] = m;
-      cnt[r] = static_cast<uint32_t>(__popcll(m));
+      span[r] = value[r] != 0xffffffffu ? __ldg(a.spans + value[r]) : make_uint4(0, 0, 0, 0);
+      cnt[r] = spanCount(span[r]);
     }
     // Offsets in (warp, row, lane) order = depth order.
     uint32_t rowExclusive[kItems];
@@ -161,25 +110,7 @@ __global__ void __launch_bounds__(kThreads) binKernel(const __grid_constant__ Bi
         const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
         if (lane >= static_cast<uint32_t>(o)) inc += up;
       }
-      const uint32_t aggregate = __shfl_sync(0xffffffffu, inc, 31);
       if (lane < kThreads / 32) warpBase[lane] = inc - w;
-      uint32_t exclusive = 0;
-      if (tile == 0) {
-        if (lane == 0) storeStatus(a.status, makeStatus(a.epoch, kFlagPrefix, aggregate));
-      } else {
-        if (lane == 0) storeStatus(a.status + tile, makeStatus(a.epoch, kFlagAggregate, aggregate));
-        exclusive = warpLookback(a.status, tile, a.epoch, a.error);
-        if (lane == 0)
-          storeStatus(a.status + tile, makeStatus(a.epoch, kFlagPrefix, exclusive + aggregate));
-      }
-      if (lane == 0) {
-        tileBase = exclusive;
-        if (tile == tiles - 1) {
-          const uint32_t total = exclusive + aggregate;
-          *a.instanceCount = total;
-          *a.overflow = total > a.instanceCapacity ? 1u : 0u;
-        }
-      }
     }
     __syncthreads();
     const uint32_t base = tileBase + warpBase[warp];
@@ -187,23 +118,33 @@ __global__ void __launch_bounds__(kThreads) binKernel(const __grid_constant__ Bi
     for (uint32_t r = 0; r < kItems; ++r) {
       if (cnt[r] == 0) continue;
       uint32_t at = base + rowExclusive[r];
-      const bool all = area[r] > 64;
-      uint64_t m = mask[r];
-      for (uint32_t k = 0; k < area[r]; ++k) {
-        if (!all && !((m >> k) & 1ull)) continue;
-        if (at < a.instanceCapacity) {
-          a.instanceKeys[at] = (ry0[r] + k / rw[r]) * a.tilesX + rx0[r] + k % rw[r];
-          a.instanceValues[at] = value[r];
+      const uint32_t x0 = span[r].x & 0xffffu, y0 = span[r].x >> 16;
+      const uint32_t w = span[r].y & 0xffffu, area = span[r].y >> 16;
+      if (area > 64) {
+        for (uint32_t k = 0; k < area; ++k, ++at) {
+          if (at < a.instanceCapacity) {
+            a.instanceKeys[at] = (y0 + k / w) * a.tilesX + x0 + k % w;
+            a.instanceValues[at] = value[r];
+          }
         }
-        ++at;
+      } else {
+        // row by row through the mask: no division
+        const uint64_t m = (static_cast<uint64_t>(span[r].w) << 32) | span[r].z;
+        const uint64_t rowBits = (w >= 64) ? ~0ull : ((1ull << w) - 1);
+        const uint32_t rows = area / w;  // area = w * rows <= 64, so row * w stays below 64
+        uint32_t rowTile = y0 * a.tilesX + x0;
+        for (uint32_t row = 0; row < rows; ++row, rowTile += a.tilesX) {
+          for (uint64_t bits = (m >> (row * w)) & rowBits; bits; bits &= bits - 1, ++at) {
+            const uint32_t x = static_cast<uint32_t>(__ffsll(static_cast<long long>(bits)) - 1);
+            if (at < a.instanceCapacity) {
+              a.instanceKeys[at] = rowTile + x;
+              a.instanceValues[at] = value[r];
+            }
+          }
+        }
       }
     }
   }
-  if (tiles == 0 && tile == 0 && threadIdx.x == 0) {
-    *a.instanceCount = 0;
-    *a.overflow = 0;
-  }
-  finishTile(a.counters);
 }
 
 __global__ void rangesKernel(const uint32_t* __restrict__ keys, const uint32_t* count,
@@ -219,9 +160,12 @@ __global__ void rangesKernel(const uint32_t* __restrict__ keys, const uint32_t* 
 
 }  // namespace
 
+uint32_t binBlocks(uint32_t capacity) { return max(1u, (capacity + kTileSplats - 1) / kTileSplats); }
+
 cudaError_t launchBinning(const BinArgs& a, cudaStream_t stream) {
-  const uint32_t grid = max(1u, (a.capacity + kTileSplats - 1) / kTileSplats);
-  binKernel<<<grid, kThreads, 0, stream>>>(a);
+  const uint32_t grid = binBlocks(a.capacity);
+  binCountKernel<<<grid, kThreads, 0, stream>>>(a);
+  binEmitKernel<<<grid, kThreads, 0, stream>>>(a);
   return cudaGetLastError();
 }
 

@@ -1,4 +1,4 @@
-// Front-to-back compositing of 16x16 pixel tiles, one thread per pixel.
+// Front-to-back compositing of 16x16 pixel tiles.
 //
 // The equations are the reference's raster stage (splatkit-ios/.../metal/raster/
 // SplatRaster.metal:27-44, .../metal/layout/SplatProjection.metalh:155-175, blend state
@@ -9,12 +9,14 @@
 // mask between four draw batches are replaced by FP32 accumulation and per-pixel early
 // termination when the remaining transmittance drops below `cutoff`.
 //
-// Each block walks its tile's list in batches of 256 records. Thread i fetches record i of the
-// batch (two 128-bit loads), turns it into the coverage form (pixel centre, inverse axes,
-// radius, log cutoff, colour, pixel box) in shared memory, then every warp sweeps the batch
-// over its 8x4 pixels, skipping at once the splats whose box misses them. The coverage decision
-// uses explicit round-to-nearest intrinsics in a fixed order, so it is bit-identical to the
-// host oracle's FP32 formula.
+// A block of 128 threads owns a tile; each thread owns two horizontally adjacent pixels and each
+// warp a 16x4-pixel strip. The block walks the tile's list in batches of 128 records: thread i
+// fetches record i (two 128-bit loads), turns it into the coverage form (pixel centre, inverse
+// axes, radius, log cutoff, colour) in shared memory and marks which of the four strips its
+// quad's box reaches. Each warp compacts, by ballot, the batch entries that reach it and sweeps
+// only those, both of its pixels per entry. The coverage decision (quad bound and 1/255 cutoff)
+// is a fixed sequence of correctly rounded operations, bit-identical to the host oracle's FP32
+// formula.
 #include <cuda_runtime.h>
 
 #include "sk_device.cuh"
@@ -23,20 +25,27 @@
 namespace sk {
 namespace {
 
-constexpr uint32_t kThreads = kTileSize * kTileSize;  // 256
-constexpr uint32_t kWarpCols = 8, kWarpRows = 4;      // a warp's pixels
+constexpr uint32_t kThreads = kTileSize * kTileSize / 2;  // 128: two pixels per thread
+constexpr uint32_t kWarps = kThreads / 32;
+constexpr uint32_t kStripRows = kTileSize / kWarps;  // 4 rows of 16 pixels per warp
 
 struct alignas(16) Splat2D {
   float cx, cy, m00, m01;
   float m10, m11, radius, lcut;
   float alpha, r, g, b;
-  float x0, x1, y0, y1;  // box (y up) outside which no pixel centre is covered
 };
-static_assert(sizeof(Splat2D) == 64, "Splat2D is four 16-byte words");
+static_assert(sizeof(Splat2D) == 48, "Splat2D is three 16-byte words");
 
-__device__ __forceinline__ Splat2D coverageForm(const uint4 lo, const uint4 hi, float halfW,
-                                                float halfH) {
-  Splat2D s;
+struct CompositeSmem {
+  Splat2D splat[kThreads];
+  uint8_t list[kWarps][kThreads];  // per warp: batch entries whose box reaches its strip
+  uint8_t reach[kThreads];         // per entry: bit w set when it reaches strip w
+};
+
+// Fills the coverage form; returns the bitmask of warp strips its box reaches.
+__device__ __forceinline__ uint32_t coverageForm(const uint4 lo, const uint4 hi, float halfW,
+                                                 float halfH, float tileX, float tileTop,
+                                                 Splat2D& s) {
   s.cx = __fmul_rn(__fadd_rn(asF(lo.x), 1.0f), halfW);
   s.cy = __fmul_rn(__fadd_rn(asF(lo.y), 1.0f), halfH);
   const float a1x = lowHalf(lo.z), a1y = highHalf(lo.z);
@@ -50,100 +59,69 @@ __device__ __forceinline__ Splat2D coverageForm(const uint4 lo, const uint4 hi, 
   s.alpha = highHalf(hi.y);
   s.lcut = lnF32(__fmul_rn(255.0f, s.alpha));
   s.radius = asF(hi.z);
-  const bool any = det != 0.0f && isfinite(inv) && isfinite(s.cx) && isfinite(s.cy);
-  if (!any) s.radius = -1.0f;
   s.r = lowHalf(hi.x);
   s.g = highHalf(hi.x);
   s.b = lowHalf(hi.y);
+  const bool any = det != 0.0f && isfinite(inv) && isfinite(s.cx) && isfinite(s.cy);
+  if (!any) {
+    s.radius = -1.0f;
+    return 0u;
+  }
   // |s|,|t| <= radius bounds the offset by radius * (|a1| + |a2|) per axis; half a pixel of
   // slack keeps the box conservative against the rounding of the inverse.
   const float ex = s.radius * (fabsf(a1x) + fabsf(a2x)) + 0.5f;
   const float ey = s.radius * (fabsf(a1y) + fabsf(a2y)) + 0.5f;
-  s.x0 = s.cx - ex, s.x1 = s.cx + ex, s.y0 = s.cy - ey, s.y1 = s.cy + ey;
-  if (!any) s.x0 = 1.0f, s.x1 = -1.0f;
-  return s;
+  if (s.cx + ex < tileX + 0.5f || s.cx - ex > tileX + (kTileSize - 0.5f)) return 0u;
+  const float y0 = s.cy - ey, y1 = s.cy + ey;
+  uint32_t reach = 0;
+#pragma unroll
+  for (uint32_t w = 0; w < kWarps; ++w) {
+    // strip w's pixel centres, y up: from tileTop - 4w - 0.5 down by three rows
+    const float top = tileTop - static_cast<float>(w * kStripRows) - 0.5f;
+    const bool hit = !(y1 < top - (kStripRows - 1) || y0 > top);
+    reach |= hit ? (1u << w) : 0u;
+  }
+  return reach;
+}
+
+struct Pixel {
+  float T = 1.0f, r = 0.0f, g = 0.0f, b = 0.0f;
+  bool done;
+};
+
+// One pixel against one splat; dyTerms = (m01 * dy, m11 * dy), shared by the row.
+__device__ __forceinline__ void blend(Pixel& p, const float4 w0, const float4 w1, const float4 c,
+                                      float px, float m01dy, float m11dy, float cutoff,
+                                      uint32_t& blended) {
+  if (p.done) return;
+  const float dx = __fsub_rn(px, w0.x);
+  const float u = __fmaf_rn(w0.z, dx, m01dy);
+  const float v = __fmaf_rn(w1.x, dx, m11dy);
+  if (!(fabsf(u) <= w1.z && fabsf(v) <= w1.z)) return;
+  const float q = __fmul_rn(0.5f, __fmaf_rn(u, u, __fmul_rn(v, v)));
+  if (!(q <= w1.w)) return;
+  const float alpha = fminf(c.x * __expf(-q), 1.0f);
+  const float weight = p.T * alpha;
+  p.r += weight * c.y;
+  p.g += weight * c.z;
+  p.b += weight * c.w;
+  p.T *= 1.0f - alpha;
+  ++blended;
+  if (p.T < cutoff) p.done = true;
 }
 
 template <int kFormat>
-__global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constant__ CompositeArgs a) {
-  __shared__ Splat2D batch[kThreads];
-  const uint32_t tile = blockIdx.x;
-  const uint32_t tx = tile % a.tilesX, ty = tile / a.tilesX;
-  const uint32_t warp = threadIdx.x >> 5, lane = laneId();
-  const uint32_t wx = warp & 1u, wy = warp >> 1;
-  const uint32_t col0 = tx * kTileSize + wx * kWarpCols;
-  const uint32_t row0 = ty * kTileSize + wy * kWarpRows;
-  const uint32_t col = col0 + (lane % kWarpCols);
-  const uint32_t row = row0 + (lane / kWarpCols);
-  const bool inside = col < a.width && row < a.height;
-  const float height = static_cast<float>(a.height);
-  const float px = static_cast<float>(col) + 0.5f;
-  const float py = static_cast<float>(a.height - row) - 0.5f;  // y up, as NDC
-  // the warp's pixel centres, y up
-  const float wx0 = static_cast<float>(col0) + 0.5f, wx1 = wx0 + (kWarpCols - 1);
-  const float wy1 = height - (static_cast<float>(row0) + 0.5f), wy0 = wy1 - (kWarpRows - 1);
-  const float halfW = 0.5f * static_cast<float>(a.width);
-  const float halfH = 0.5f * height;
-  const uint2 range = a.ranges[tile];
-  float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
-  bool done = !inside;
-  uint32_t blended = 0, loaded = 0;
-  for (uint32_t start = range.x; start < range.y; start += kThreads) {
-    const uint32_t inBatch = min(kThreads, range.y - start);
-    loaded += inBatch;
-    if (threadIdx.x < inBatch) {
-      const uint32_t v = a.values[start + threadIdx.x];
-      const uint4* p = reinterpret_cast<const uint4*>(a.projected + v);
-      batch[threadIdx.x] = coverageForm(__ldg(p), __ldg(p + 1), halfW, halfH);
-    }
-    __syncthreads();
-    if (!__all_sync(0xffffffffu, done)) {
-      for (uint32_t j = 0; j < inBatch; ++j) {
-        const float4 box = reinterpret_cast<const float4*>(&batch[j])[3];
-        // warp-uniform: the splat's box misses all 32 pixel centres of this warp
-        if (box.y < wx0 || box.x > wx1 || box.w < wy0 || box.z > wy1) continue;
-        if (done) continue;
-        const float4 w0 = reinterpret_cast<const float4*>(&batch[j])[0];
-        const float4 w1 = reinterpret_cast<const float4*>(&batch[j])[1];
-        const float dx = __fsub_rn(px, w0.x), dy = __fsub_rn(py, w0.y);
-        const float u = __fadd_rn(__fmul_rn(w0.z, dx), __fmul_rn(w0.w, dy));
-        const float v = __fadd_rn(__fmul_rn(w1.x, dx), __fmul_rn(w1.y, dy));
-        if (!(fabsf(u) <= w1.z && fabsf(v) <= w1.z)) continue;
-        const float q = __fmul_rn(0.5f, __fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)));
-        if (!(q <= w1.w)) continue;
-        const float4 c = reinterpret_cast<const float4*>(&batch[j])[2];
-        const float alpha = fminf(c.x * __expf(-q), 1.0f);
-        const float weight = T * alpha;
-        cr += weight * c.y;
-        cg += weight * c.z;
-        cb += weight * c.w;
-        T *= 1.0f - alpha;
-        ++blended;
-        if (T < a.cutoff) done = true;
-      }
-    }
-    if (__syncthreads_count(done ? 0 : 1) == 0) break;
-  }
-  // blended fragments: one 64-bit add per block
-  __shared__ unsigned long long blockFragments;
-  if (threadIdx.x == 0) blockFragments = 0;
-  __syncthreads();
-  uint32_t warpSum = blended;
-  for (int o = 16; o > 0; o >>= 1) warpSum += __shfl_xor_sync(0xffffffffu, warpSum, o);
-  if (lane == 0 && warpSum) atomicAdd(&blockFragments, static_cast<unsigned long long>(warpSum));
-  __syncthreads();
-  if (threadIdx.x == 0 && blockFragments)
-    atomicAdd(reinterpret_cast<unsigned long long*>(a.fragments), blockFragments);
-  if (threadIdx.x == 0 && loaded) atomicAdd(a.loaded, loaded);
-  if (!inside) return;
+__device__ __forceinline__ void writePixel(const CompositeArgs& a, const Pixel& p, uint32_t col,
+                                           uint32_t row) {
+  if (col >= a.width || row >= a.height) return;
   float outR, outG, outB, outA;
   if (a.opaque) {
-    outR = cr + T * a.background[0];
-    outG = cg + T * a.background[1];
-    outB = cb + T * a.background[2];
+    outR = p.r + p.T * a.background[0];
+    outG = p.g + p.T * a.background[1];
+    outB = p.b + p.T * a.background[2];
     outA = 1.0f;
   } else {
-    outR = cr, outG = cg, outB = cb, outA = 1.0f - T;
+    outR = p.r, outG = p.g, outB = p.b, outA = 1.0f - p.T;
   }
   outR = fminf(fmaxf(outR, 0.0f), 1.0f);
   outG = fminf(fmaxf(outG, 0.0f), 1.0f);
@@ -157,6 +135,82 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
     const uint32_t b8 = __float2uint_rn(outB * 255.0f), a8 = __float2uint_rn(outA * 255.0f);
     reinterpret_cast<uint32_t*>(a.image)[at] = r8 | (g8 << 8) | (b8 << 16) | (a8 << 24);
   }
+}
+
+template <int kFormat>
+__global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constant__ CompositeArgs a) {
+  __shared__ CompositeSmem sm;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t tx = tile % a.tilesX, ty = tile / a.tilesX;
+  const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+  const uint32_t col = tx * kTileSize + (lane % 8u) * 2u;  // and col + 1
+  const uint32_t row = ty * kTileSize + warp * kStripRows + lane / 8u;
+  const float height = static_cast<float>(a.height);
+  const float px0 = static_cast<float>(col) + 0.5f, px1 = px0 + 1.0f;
+  const float py = static_cast<float>(a.height - row) - 0.5f;  // y up, as NDC
+  const float tileX = static_cast<float>(tx * kTileSize);
+  const float tileTop = height - static_cast<float>(ty * kTileSize);
+  const float halfW = 0.5f * static_cast<float>(a.width);
+  const float halfH = 0.5f * height;
+  const uint2 range = a.ranges[tile];
+  const uint32_t below = lanemaskLt();
+  Pixel p0, p1;
+  p0.done = !(col < a.width && row < a.height);
+  p1.done = !(col + 1 < a.width && row < a.height);
+  uint32_t blended = 0, loaded = 0;
+  for (uint32_t start = range.x; start < range.y; start += kThreads) {
+    const uint32_t inBatch = min(kThreads, range.y - start);
+    loaded += inBatch;
+    if (threadIdx.x < inBatch) {
+      const uint32_t v = a.values[start + threadIdx.x];
+      const uint4* p = reinterpret_cast<const uint4*>(a.projected + v);
+      Splat2D s;
+      sm.reach[threadIdx.x] =
+          static_cast<uint8_t>(coverageForm(__ldg(p), __ldg(p + 1), halfW, halfH, tileX, tileTop, s));
+      sm.splat[threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (!__all_sync(0xffffffffu, p0.done && p1.done)) {
+      // this warp's entries, in batch (= depth) order
+      uint32_t count = 0;
+      for (uint32_t c = 0; c < inBatch; c += 32) {
+        const uint32_t j = c + lane;
+        const bool mine = j < inBatch && ((sm.reach[j] >> warp) & 1u);
+        const uint32_t m = __ballot_sync(0xffffffffu, mine);
+        if (mine) sm.list[warp][count + __popc(m & below)] = static_cast<uint8_t>(j);
+        count += __popc(m);
+      }
+      __syncwarp();
+      for (uint32_t k0 = 0; k0 < count; k0 += 16) {
+        if (__all_sync(0xffffffffu, p0.done && p1.done)) break;
+        const uint32_t k1 = min(count, k0 + 16);
+        for (uint32_t k = k0; k < k1; ++k) {
+          const Splat2D& s = sm.splat[sm.list[warp][k]];
+          const float4 w0 = reinterpret_cast<const float4*>(&s)[0];
+          const float4 w1 = reinterpret_cast<const float4*>(&s)[1];
+          const float4 c = reinterpret_cast<const float4*>(&s)[2];
+          const float dy = __fsub_rn(py, w0.y);
+          const float m01dy = __fmul_rn(w0.w, dy), m11dy = __fmul_rn(w1.y, dy);
+          blend(p0, w0, w1, c, px0, m01dy, m11dy, a.cutoff, blended);
+          blend(p1, w0, w1, c, px1, m01dy, m11dy, a.cutoff, blended);
+        }
+      }
+    }
+    if (__syncthreads_count((p0.done && p1.done) ? 0 : 1) == 0) break;
+  }
+  // blended fragments: one 64-bit add per block
+  __shared__ unsigned long long blockFragments;
+  if (threadIdx.x == 0) blockFragments = 0;
+  __syncthreads();
+  uint32_t warpSum = blended;
+  for (int o = 16; o > 0; o >>= 1) warpSum += __shfl_xor_sync(0xffffffffu, warpSum, o);
+  if (lane == 0 && warpSum) atomicAdd(&blockFragments, static_cast<unsigned long long>(warpSum));
+  __syncthreads();
+  if (threadIdx.x == 0 && blockFragments)
+    atomicAdd(reinterpret_cast<unsigned long long*>(a.fragments), blockFragments);
+  if (threadIdx.x == 0 && loaded) atomicAdd(a.loaded, loaded);
+  writePixel<kFormat>(a, p0, col, row);
+  writePixel<kFormat>(a, p1, col + 1, row);
 }
 
 }  // namespace

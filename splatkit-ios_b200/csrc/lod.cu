@@ -152,10 +152,12 @@ __global__ void lodInitKernel(uint32_t* frontier, LodState* state) {
 }
 
 __global__ void __launch_bounds__(kThreads)
-    lodEvaluateKernel(const __grid_constant__ Camera cam, const __grid_constant__ LodArgs a,
+    lodEvaluateKernel(const Camera* __restrict__ camera, const __grid_constant__ LodArgs a,
                       const uint32_t* __restrict__ frontier, uint32_t epoch) {
+  __shared__ Camera cam;
+  loadCamera(camera, &cam);
   LodState* st = a.state;
-  const uint32_t tile = takeTile(a.counters);
+  const uint32_t tile = takeTile(a.counters);  // its barrier also publishes the camera
   // The guard keeps the frontier within the capacity; clamp anyway so no index leaves the
   // buffers (and say so).
   const uint32_t active = min(st->active, a.frontierCapacity);
@@ -365,7 +367,7 @@ __global__ void lodReportKernel(const LodState* state, uint32_t* report) {
 
 uint32_t lodTileClusters() { return kTileClusters; }
 
-cudaError_t launchLodSelect(const Camera& cam, const LodArgs& a, cudaStream_t stream) {
+cudaError_t launchLodSelect(const Camera* cam, const LodArgs& a, cudaStream_t stream) {
   const uint32_t grid = max(1u, (a.frontierCapacity + kTileClusters - 1) / kTileClusters);
   RoundSums* sums = reinterpret_cast<RoundSums*>(reinterpret_cast<char*>(a.state) + sizeof(LodState));
   lodInitKernel<<<1, 1, 0, stream>>>(a.frontier[0], a.state);

@@ -8,6 +8,8 @@
 // product and sum rounds on its own. The composite kernel does its coverage decision with
 // explicit __fmul_rn/__fadd_rn intrinsics for the same reason.
 #pragma once
+#include <cuda_fp16.h>
+
 #include <cstdint>
 
 #include "sk_layout.h"
@@ -28,37 +30,19 @@ __device__ __forceinline__ uint32_t lanemaskLt() {
 // ---- binary16, round to nearest even, saturating to 65504, NaN kept -----------------
 // The reference's float -> half packing rule (splat-core/include/splat/math/Half.h:12-38),
 // written from the IEEE encodings.
+// The hardware conversion rounds to nearest even (subnormals included); clamping to the largest
+// finite half first turns its overflow to infinity into the saturation Half.h specifies, and
+// a NaN keeps its sign with the quiet-NaN payload 0x7e00.
 __device__ __forceinline__ uint32_t floatToHalf(float v) {
-  const uint32_t x = asU(v);
-  const uint32_t sign = (x >> 16) & 0x8000u;
-  const uint32_t ax = x & 0x7fffffffu;
-  const uint32_t e = ax >> 23;
-  const uint32_t mant = ax & 0x7fffffu;
-  if (e == 0xffu) return sign | (mant ? 0x7e00u : 0x7bffu);
-  if (e < 113u) {
-    const uint32_t shift = 126u - e;
-    if (shift > 24u) return sign;
-    const uint32_t full = mant | 0x800000u;
-    const uint32_t h = full >> shift;
-    const uint32_t rem = full & ((1u << shift) - 1u);
-    const uint32_t mid = 1u << (shift - 1u);
-    const uint32_t up = (rem > mid || (rem == mid && (h & 1u))) ? 1u : 0u;
-    return sign | (h + up);
-  }
-  uint32_t h = ((e - 112u) << 10) | (mant >> 13);
-  const uint32_t rem = mant & 0x1fffu;
-  if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) ++h;
-  if (h >= 0x7c00u) h = 0x7bffu;
-  return sign | h;
+  if (v != v) return ((asU(v) >> 16) & 0x8000u) | 0x7e00u;
+  const float c = fminf(fmaxf(v, -65504.0f), 65504.0f);
+  return static_cast<uint32_t>(__half_as_ushort(__float2half_rn(c)));
 }
 
+// binary16 -> binary32 is exact, so the hardware conversion gives the same bits as any correct
+// conversion (the host side decodes the IEEE fields by hand).
 __device__ __forceinline__ float halfToFloat(uint32_t h) {
-  const uint32_t sign = (h & 0x8000u) << 16;
-  const uint32_t e = (h >> 10) & 0x1fu;
-  const uint32_t m = h & 0x3ffu;
-  if (e == 0) return asF(asU(__fmul_rn(static_cast<float>(m), 5.9604644775390625e-08f)) | sign);
-  if (e == 31) return asF(sign | 0x7f800000u | (m << 13));
-  return asF(sign | ((e + 112u) << 23) | (m << 13));
+  return __half2float(__ushort_as_half(static_cast<unsigned short>(h & 0xffffu)));
 }
 
 __device__ __forceinline__ float lowHalf(uint32_t w) { return halfToFloat(w & 0xffffu); }
@@ -106,6 +90,13 @@ __device__ __forceinline__ float lnF32(float x) {
   const float fe = static_cast<float>(e);
   return __fadd_rn(__fmul_rn(fe, 0.693145751953125f),
                    __fadd_rn(lnm, __fmul_rn(fe, 1.428606820309417e-06f)));
+}
+
+// Copies the 208-byte camera from device memory into shared memory (the caller syncs).
+__device__ __forceinline__ void loadCamera(const Camera* __restrict__ src, Camera* dst) {
+  constexpr uint32_t kWords = sizeof(Camera) / 4;
+  if (threadIdx.x < kWords)
+    reinterpret_cast<uint32_t*>(dst)[threadIdx.x] = __ldg(reinterpret_cast<const uint32_t*>(src) + threadIdx.x);
 }
 
 // ---- decoupled look-back ----------------------------------------------------------------

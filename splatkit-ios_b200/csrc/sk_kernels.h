@@ -26,6 +26,8 @@ struct VisibilityArgs {
   uint32_t total;              // ranges mode: sum of counts; indexed mode: capacity bound
   uint32_t* keys;
   Projected* projected;
+  uint4* spans;  // per survivor: the 16x16 tiles its quad touches (sk_tiles.cuh)
+  uint32_t tilesX, tilesY;
   uint32_t* visibleCount;
   uint64_t* status;    // one word per 1024-splat tile
   uint32_t* counters;  // two words
@@ -33,7 +35,9 @@ struct VisibilityArgs {
   uint32_t* error;
 };
 uint32_t visibilityTileSplats();
-cudaError_t launchVisibility(const Camera& cam, const VisibilityArgs& args, int shDegree,
+// `cam` is a device pointer: the kernels stage it in shared memory, so a captured graph can be
+// replayed with new cameras written into the same buffer.
+cudaError_t launchVisibility(const Camera* cam, const VisibilityArgs& args, int shDegree,
                              bool key16, bool indexed, cudaStream_t stream);
 
 // ---- radix sort (radix_sort.cu) --------------------------------------------------------
@@ -68,7 +72,7 @@ cudaError_t sortResetWorkspace(const SortArgs& args, cudaStream_t stream);
 
 // ---- tile binning (binning.cu) ---------------------------------------------------------
 struct BinArgs {
-  const Projected* projected;
+  const uint4* spans;     // per survivor tile spans, indexed like the projected records
   const uint32_t* order;  // depth order (indices into projected)
   const uint32_t* count;  // survivors (device)
   uint32_t capacity;      // bound on count
@@ -78,11 +82,9 @@ struct BinArgs {
   uint32_t instanceCapacity;
   uint32_t* instanceCount;  // FrameCounters.instances
   uint32_t* overflow;       // FrameCounters.overflow
-  uint64_t* status;
-  uint32_t* counters;
-  uint32_t epoch;
-  uint32_t* error;
+  uint32_t* blockSums;      // binBlocks(capacity) words of scratch
 };
+uint32_t binBlocks(uint32_t capacity);
 cudaError_t launchBinning(const BinArgs& args, cudaStream_t stream);
 
 // Tile [start, end) ranges from the tile-sorted instance keys. ranges: tilesX * tilesY uint2,
@@ -133,6 +135,6 @@ struct LodArgs {
   uint32_t* report;  // six words copied from the state at the end (FrameCounters.lod)
 };
 uint32_t lodTileClusters();
-cudaError_t launchLodSelect(const Camera& cam, const LodArgs& args, cudaStream_t stream);
+cudaError_t launchLodSelect(const Camera* cam, const LodArgs& args, cudaStream_t stream);
 
 }  // namespace sk

@@ -1,0 +1,89 @@
+// Which 16x16 tiles a projected splat's quad touches.
+//
+// The quad is the parallelogram c + s a1 + t a2, |s|, |t| <= radius, in pixel units (y up), with
+// the half-rounded axes the compositor inverts. Its tiles are those of its pixel box whose
+// square it overlaps by the separating-axis test (x, y and the normals of a1 and a2). The tile
+// square is the pixel area, half a pixel beyond every pixel centre, so the test can only keep
+// too many tiles, never drop one the compositor would cover.
+//
+// A span packs the result in 16 bytes: (x0 | y0 << 16, width | area << 16, mask lo, mask hi),
+// bit k of the mask standing for box tile (x0 + k % width, y0 + k / width). A box of more than
+// 64 tiles keeps all of them (its mask is unused); area 0 means no tile.
+#pragma once
+#include "sk_device.cuh"
+
+namespace sk {
+
+struct Quad {
+  float cx, cy, a1x, a1y, a2x, a2y, r;
+};
+
+__device__ __forceinline__ Quad quadOf(const uint4 lo, const uint4 hi, float halfW, float halfH) {
+  Quad q;
+  q.cx = (asF(lo.x) + 1.0f) * halfW;
+  q.cy = (asF(lo.y) + 1.0f) * halfH;
+  q.a1x = lowHalf(lo.z), q.a1y = highHalf(lo.z);
+  q.a2x = lowHalf(lo.w), q.a2y = highHalf(lo.w);
+  q.r = asF(hi.z);
+  return q;
+}
+
+// Separating-axis test of the quad against tile (tx, ty)'s pixel square (y up).
+__device__ __forceinline__ bool quadTouchesTile(const Quad& q, uint32_t tx, uint32_t ty,
+                                                float height) {
+  const float half = 0.5f * static_cast<float>(kTileSize);
+  const float rx = static_cast<float>(tx * kTileSize) + half;
+  const float ry = height - (static_cast<float>(ty * kTileSize) + half);
+  const float dx = rx - q.cx, dy = ry - q.cy;
+  if (fabsf(dx) > q.r * (fabsf(q.a1x) + fabsf(q.a2x)) + half) return false;
+  if (fabsf(dy) > q.r * (fabsf(q.a1y) + fabsf(q.a2y)) + half) return false;
+  // normal of a1: the quad's extent along it comes from t a2 only
+  const float n1x = -q.a1y, n1y = q.a1x;
+  if (fabsf(dx * n1x + dy * n1y) >
+      q.r * fabsf(q.a2x * n1x + q.a2y * n1y) + half * (fabsf(n1x) + fabsf(n1y)))
+    return false;
+  const float n2x = -q.a2y, n2y = q.a2x;
+  if (fabsf(dx * n2x + dy * n2y) >
+      q.r * fabsf(q.a1x * n2x + q.a1y * n2y) + half * (fabsf(n2x) + fabsf(n2y)))
+    return false;
+  return true;
+}
+
+// The span of one projected record (two uint4 words) on a width x height target.
+__device__ __forceinline__ uint4 tileSpan(const uint4 lo, const uint4 hi, float width, float height,
+                                          uint32_t tilesX, uint32_t tilesY) {
+  const Quad q = quadOf(lo, hi, 0.5f * width, 0.5f * height);
+  const float ex = q.r * (fabsf(q.a1x) + fabsf(q.a2x)) + 1.0f;
+  const float ey = q.r * (fabsf(q.a1y) + fabsf(q.a2y)) + 1.0f;
+  if (!(isfinite(q.cx) && isfinite(q.cy) && isfinite(ex) && isfinite(ey) && q.r >= 0.0f))
+    return make_uint4(0, 0, 0, 0);
+  const float xa = floorf(q.cx - ex), xb = ceilf(q.cx + ex);
+  const float ya = floorf(q.cy - ey), yb = ceilf(q.cy + ey);
+  if (xb < 0.0f || xa >= width || yb < 0.0f || ya >= height) return make_uint4(0, 0, 0, 0);
+  // columns [c0, c1]; rows from the y-up box: row = H - y_up - 0.5
+  const uint32_t c0 = static_cast<uint32_t>(fmaxf(xa, 0.0f));
+  const uint32_t c1 = static_cast<uint32_t>(fminf(xb, width - 1.0f));
+  const uint32_t r0 = static_cast<uint32_t>(fmaxf(height - yb - 1.0f, 0.0f));
+  const uint32_t r1 = static_cast<uint32_t>(fminf(fmaxf(height - ya, 0.0f), height - 1.0f));
+  const uint32_t x0 = c0 / kTileSize, x1 = min(c1 / kTileSize, tilesX - 1);
+  const uint32_t y0 = r0 / kTileSize, y1 = min(r1 / kTileSize, tilesY - 1);
+  if (x0 > x1 || y0 > y1) return make_uint4(0, 0, 0, 0);
+  const uint32_t w = x1 - x0 + 1, area = w * (y1 - y0 + 1);
+  uint64_t mask = 0;
+  if (area <= 64) {
+    for (uint32_t k = 0; k < area; ++k)
+      if (quadTouchesTile(q, x0 + k % w, y0 + k / w, height)) mask |= 1ull << k;
+    if (mask == 0) return make_uint4(0, 0, 0, 0);
+  }
+  return make_uint4(x0 | (y0 << 16), w | (area << 16), static_cast<uint32_t>(mask),
+                    static_cast<uint32_t>(mask >> 32));
+}
+
+// Tiles a span lists.
+__device__ __forceinline__ uint32_t spanCount(const uint4 s) {
+  const uint32_t area = s.y >> 16;
+  if (area > 64) return area;
+  return static_cast<uint32_t>(__popc(s.z) + __popc(s.w));
+}
+
+}  // namespace sk

@@ -14,6 +14,7 @@
 
 #include "sk_device.cuh"
 #include "sk_kernels.h"
+#include "sk_tiles.cuh"
 
 namespace sk {
 namespace {
@@ -257,9 +258,11 @@ struct VisibilitySmem {
 
 template <int D, bool kKey16, bool kIndexed>
 __global__ void __launch_bounds__(kThreads)
-    visibilityKernel(const __grid_constant__ Camera cam, const __grid_constant__ VisibilityArgs a) {
+    visibilityKernel(const Camera* __restrict__ camera, const __grid_constant__ VisibilityArgs a) {
   __shared__ VisibilitySmem s;
-  const uint32_t tile = takeTile(a.counters);
+  __shared__ Camera cam;
+  loadCamera(camera, &cam);
+  const uint32_t tile = takeTile(a.counters);  // its barrier also publishes the camera
   const uint32_t total = kIndexed ? min(*a.indexCount, a.total) : a.total;
   const uint32_t tiles = (total + kTileSplats - 1) / kTileSplats;
   if (tile < tiles) {
@@ -352,14 +355,17 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
     __syncthreads();
-    // coalesced copy-out: consecutive threads write consecutive survivors
+    // coalesced copy-out: consecutive threads write consecutive survivors, with the tiles
+    // each survivor's quad touches
     const uint32_t count = s.tileCount, base = s.tileBase;
     for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
       const uint32_t slot = s.slotOf[k];
       a.keys[base + k] = s.key[slot];
+      const uint4 lo = s.rec[2 * slot], hi = s.rec[2 * slot + 1];
       uint4* o = reinterpret_cast<uint4*>(a.projected + base + k);
-      o[0] = s.rec[2 * slot];
-      o[1] = s.rec[2 * slot + 1];
+      o[0] = lo;
+      o[1] = hi;
+      a.spans[base + k] = tileSpan(lo, hi, cam.screenSize[0], cam.screenSize[1], a.tilesX, a.tilesY);
     }
   }
   if (tiles == 0 && tile == 0 && threadIdx.x == 0) *a.visibleCount = 0;
@@ -368,12 +374,12 @@ __global__ void __launch_bounds__(kThreads)
 
 
 template <int D, bool kKey16, bool kIndexed>
-void launchOne(const Camera& cam, const VisibilityArgs& a, uint32_t grid, cudaStream_t stream) {
+void launchOne(const Camera* cam, const VisibilityArgs& a, uint32_t grid, cudaStream_t stream) {
   visibilityKernel<D, kKey16, kIndexed><<<grid, kThreads, 0, stream>>>(cam, a);
 }
 
 template <int D>
-void launchDegree(const Camera& cam, const VisibilityArgs& a, bool key16, bool indexed,
+void launchDegree(const Camera* cam, const VisibilityArgs& a, bool key16, bool indexed,
                   uint32_t grid, cudaStream_t stream) {
   if (key16) {
     if (indexed) launchOne<D, true, true>(cam, a, grid, stream);
@@ -388,7 +394,7 @@ void launchDegree(const Camera& cam, const VisibilityArgs& a, bool key16, bool i
 
 uint32_t visibilityTileSplats() { return kTileSplats; }
 
-cudaError_t launchVisibility(const Camera& cam, const VisibilityArgs& args, int shDegree,
+cudaError_t launchVisibility(const Camera* cam, const VisibilityArgs& args, int shDegree,
                              bool key16, bool indexed, cudaStream_t stream) {
   const uint32_t grid = max(1u, (args.total + kTileSplats - 1) / kTileSplats);
   switch (shDegree) {

@@ -3,43 +3,40 @@
 // and the Metal renderer's frame (splatkit-ios/.../metal/MetalSplatRenderer.mm:166-308).
 //
 // A frame is enqueued on the context's stream without a host round trip:
-//   [LOD cut] -> visibility (cull, project, SH, depth key, source-order compaction)
+//   [LOD cut] -> visibility (cull, project, SH, depth key, tile span, source-order compaction)
 //   -> depth sort (onesweep radix, 16- or 32-bit keys) -> tile binning -> stable tile sort
 //   -> tile ranges -> composite, then a 64-byte counter block is copied back asynchronously.
 // Every grid is sized by a host-known capacity; live counts stay on the device.
+#include "context.h"
+
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
-#include <limits>
 #include <memory>
-#include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
-#include "../../include/splatkit_b200.h"
-#include "../csrc/sk_kernels.h"
-#include "context.h"
 #include "world_prep.h"
 
 namespace sk {
 
-// ---- device buffers -----------------------------------------------------------------------
+// ---- buffers ------------------------------------------------------------------------------
 
 cudaError_t DeviceBuffer::allocate(size_t n) {
+  n = std::max<size_t>(n, 256);
   if (n <= bytes && ptr) return cudaSuccess;
   void* fresh = nullptr;
-  const cudaError_t e = cudaMalloc(&fresh, std::max<size_t>(n, 256));
+  const cudaError_t e = cudaMalloc(&fresh, n);
   if (e != cudaSuccess) {
     cudaGetLastError();  // an allocation failure is not a sticky error
     return e;
   }
   release();
   ptr = fresh;
-  bytes = std::max<size_t>(n, 256);
+  bytes = n;
   return cudaSuccess;
 }
 
@@ -49,14 +46,34 @@ void DeviceBuffer::release() {
   bytes = 0;
 }
 
-namespace {
+cudaError_t PinnedBuffer::allocate(size_t n) {
+  n = std::max<size_t>(n, 64);
+  if (n <= bytes && ptr) return cudaSuccess;
+  void* fresh = nullptr;
+  const cudaError_t e = cudaMallocHost(&fresh, n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e;
+  }
+  release();
+  ptr = fresh;
+  bytes = n;
+  std::memset(ptr, 0, n);
+  return cudaSuccess;
+}
 
-constexpr uint32_t kMaxRanges = 65536;  // MetalVisibilityPass.h:72
-constexpr float kTransmittanceCutoff = 1e-4f;
+void PinnedBuffer::release() {
+  if (ptr) cudaFreeHost(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
 
-int hostThreads() { return std::max(1u, std::min(16u, std::thread::hardware_concurrency())); }
+// ---- context ------------------------------------------------------------------------------
 
-}  // namespace
+Context::~Context() {
+  if (done) cudaEventDestroy(done);
+  if (stream) cudaStreamDestroy(stream);
+}
 
 sk_status Context::fail(sk_status code, const std::string& message) {
   error = message;
@@ -80,61 +97,53 @@ uint32_t Context::nextEpoch(uint32_t n) {
   return e;
 }
 
-// Scratch sized for `sources` splats per frame and `instances` tile instances.
-sk_status Context::reserveFrame(FrameScratch& f, uint32_t sources, uint32_t instances) {
+uint32_t Context::instanceGuess(uint32_t sources) const {
+  return static_cast<uint32_t>(std::min<uint64_t>(uint64_t{std::max(sources, 1u)} * 8, 0x7fffffffu));
+}
+
+sk_status Context::reserveScratch(FrameScratch& f, uint32_t sources, uint32_t instances,
+                                  uint32_t maxTiles, cudaStream_t s) {
   sources = std::max(sources, 1u);
   instances = std::max(instances, 1u);
-  const uint32_t tilesX = (width + kTileSize - 1) / kTileSize;
-  const uint32_t tilesY = (height + kTileSize - 1) / kTileSize;
-  const size_t pixels = size_t{width} * height;
-  const size_t pixelBytes = imageFormat == SK_FORMAT_RGBA32F ? 16 : 4;
+  maxTiles = std::max(maxTiles, 1u);
   cudaError_t e = cudaSuccess;
   auto grab = [&](DeviceBuffer& b, size_t n) {
     if (e == cudaSuccess) e = b.allocate(n);
   };
   const uint32_t visTiles = (sources + visibilityTileSplats() - 1) / visibilityTileSplats();
-  const uint32_t binTiles = visTiles;
   grab(f.keys, size_t{sources} * 4);
   grab(f.projected, size_t{sources} * sizeof(Projected));
+  grab(f.spans, size_t{sources} * 16);
   grab(f.order, size_t{sources} * 4);
   grab(f.sortWorkspace, sortWorkspaceBytes(sources));
   grab(f.visStatus, size_t{visTiles} * 8);
-  grab(f.binStatus, size_t{binTiles} * 8);
+  grab(f.binSums, size_t{binBlocks(sources)} * 4);
   grab(f.instKeys, size_t{instances} * 4);
   grab(f.instValues, size_t{instances} * 4);
   grab(f.instKeysSorted, size_t{instances} * 4);
   grab(f.instValuesSorted, size_t{instances} * 4);
   grab(f.tileSortWorkspace, sortWorkspaceBytes(instances));
-  grab(f.ranges, size_t{tilesX} * tilesY * sizeof(uint2));
-  grab(f.image, pixels * pixelBytes);
+  grab(f.ranges, size_t{maxTiles} * sizeof(uint2));
   grab(f.rangeBuffer, size_t{kMaxRanges} * sizeof(Range));
   grab(f.rangeStarts, size_t{kMaxRanges + 1} * 4);
-  if (!f.counters.ptr) {
-    grab(f.counters, 64 * 4);
-    if (e == cudaSuccess) e = cudaMemsetAsync(f.counters.ptr, 0, 64 * 4, stream);
-    grab(f.frameCounters, sizeof(FrameCounters));
-    if (e == cudaSuccess) e = cudaMemsetAsync(f.frameCounters.ptr, 0, sizeof(FrameCounters), stream);
-  }
-  if (e != cudaSuccess) return check(e, "frame buffers");
-  if (!f.hostCounters) {
-    e = cudaMallocHost(&f.hostCounters, sizeof(FrameCounters));
-    if (e != cudaSuccess) return check(e, "pinned counters");
-    std::memset(f.hostCounters, 0, sizeof(FrameCounters));
-  }
-  // Sort workspaces hold counters that must start at zero.
-  e = cudaMemsetAsync(f.sortWorkspace.ptr, 0, f.sortWorkspace.bytes, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(f.tileSortWorkspace.ptr, 0, f.tileSortWorkspace.bytes, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(f.visStatus.ptr, 0, f.visStatus.bytes, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(f.binStatus.ptr, 0, f.binStatus.bytes, stream);
+  const bool fresh = f.counters.ptr == nullptr;
+  grab(f.counters, 64 * 4);
+  if (e == cudaSuccess && fresh) e = cudaMemsetAsync(f.counters.ptr, 0, 64 * 4, s);
+  // Sort workspaces hold counters that must start at zero; status words carry epochs.
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.sortWorkspace.ptr, 0, f.sortWorkspace.bytes, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.tileSortWorkspace.ptr, 0, f.tileSortWorkspace.bytes, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.visStatus.ptr, 0, f.visStatus.bytes, s);
+  if (e == cudaSuccess && !f.events[0])
+    for (auto& ev : f.events)
+      if (e == cudaSuccess) e = cudaEventCreate(&ev);
   if (e != cudaSuccess) return check(e, "frame buffers");
   f.sources = sources;
   f.instanceCapacity = instances;
-  f.tilesX = tilesX;
-  f.tilesY = tilesY;
+  f.maxTiles = std::max(f.maxTiles, maxTiles);
   return SK_OK;
 }
 
-sk_status Context::reserveLod(FrameScratch& f, const World& w) {
+sk_status Context::reserveLod(FrameScratch& f, const World& w, cudaStream_t s) {
   cudaError_t e = cudaSuccess;
   auto grab = [&](DeviceBuffer& b, size_t n) {
     if (e == cudaSuccess) e = b.allocate(n);
@@ -150,20 +159,30 @@ sk_status Context::reserveLod(FrameScratch& f, const World& w) {
   grab(f.lodState, 256);
   grab(f.lodStatus, size_t{tiles} * 3 * 8);
   grab(f.lodCounters, 2 * 4);
-  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodStatus.ptr, 0, f.lodStatus.bytes, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodCounters.ptr, 0, f.lodCounters.bytes, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodState.ptr, 0, f.lodState.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodStatus.ptr, 0, f.lodStatus.bytes, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodCounters.ptr, 0, f.lodCounters.bytes, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.lodState.ptr, 0, f.lodState.bytes, s);
   if (e != cudaSuccess) return check(e, "LOD buffers");
   f.lodFrontierCapacity = frontier;
   return SK_OK;
 }
 
-Camera Context::cameraFor(const sk_frame& frame) const {
+sk_status Context::reserveView(uint32_t w, uint32_t h) {
+  const size_t pixelBytes = imageFormat == SK_FORMAT_RGBA32F ? 16 : 4;
+  cudaError_t e = image.allocate(size_t{w} * h * pixelBytes);
+  if (e == cudaSuccess) e = frameCounters.allocate(sizeof(FrameCounters));
+  if (e == cudaSuccess) e = camera.allocate(sizeof(Camera));
+  if (e == cudaSuccess) e = hostCounters.allocate(sizeof(FrameCounters));
+  if (e == cudaSuccess) e = hostCamera.allocate(sizeof(Camera));
+  return check(e, "view buffers");
+}
+
+Camera Context::cameraFor(const sk_frame& frame, uint32_t w, uint32_t h) const {
   Camera c{};
   std::memcpy(c.view, frame.view, 64);
   std::memcpy(c.proj, frame.proj, 64);
-  c.screenSize[0] = static_cast<float>(width);
-  c.screenSize[1] = static_cast<float>(height);
+  c.screenSize[0] = static_cast<float>(w);
+  c.screenSize[1] = static_cast<float>(h);
   // MetalFrameCompute.mm:148-151
   c.focal[0] = (c.screenSize[0] * frame.proj[0]) / 2.0f;
   c.focal[1] = (c.screenSize[1] * frame.proj[5]) / 2.0f;
@@ -195,14 +214,13 @@ sk_status Context::validateRanges(const sk_frame& frame, uint32_t* total) const 
   return SK_OK;
 }
 
-// Enqueues one frame on `stream` with scratch `f`. `ranges` are already validated.
-sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t total,
-                                cudaStream_t s, bool timed) {
-  const Camera cam = cameraFor(frame);
+sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, const sk_frame& frame,
+                                   uint32_t total, cudaStream_t s, bool timed) {
   const int degree = std::max(0, std::min(frame.sh_degree, world.shDegree));
   const bool key16 = policy.sort_depth_bits == 16;
+  const uint32_t tilesX = view.tilesX(), tilesY = view.tilesY();
   uint32_t* counters = static_cast<uint32_t*>(f.counters.ptr);
-  FrameCounters* fc = static_cast<FrameCounters*>(f.frameCounters.ptr);
+  FrameCounters* fc = view.counters;
   uint32_t* error = &fc->error;
   cudaError_t e = cudaMemsetAsync(fc, 0, sizeof(FrameCounters), s);
   if (timed) cudaEventRecord(f.events[0], s);
@@ -232,7 +250,7 @@ sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t
     a.epoch = nextEpoch(2 * world.rounds + 2);
     a.error = error;
     a.report = fc->lod;
-    e = launchLodSelect(cam, a, s);
+    e = launchLodSelect(view.camera, a, s);
   }
   if (timed) cudaEventRecord(f.events[1], s);
 
@@ -262,12 +280,15 @@ sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t
     v.total = lod ? world.lodCapacity : total;
     v.keys = static_cast<uint32_t*>(f.keys.ptr);
     v.projected = static_cast<Projected*>(f.projected.ptr);
+    v.spans = static_cast<uint4*>(f.spans.ptr);
+    v.tilesX = tilesX;
+    v.tilesY = tilesY;
     v.visibleCount = &fc->visible;
     v.status = static_cast<uint64_t*>(f.visStatus.ptr);
     v.counters = counters + 0;
     v.epoch = nextEpoch(1);
     v.error = error;
-    e = launchVisibility(cam, v, degree, key16, lod, s);
+    e = launchVisibility(view.camera, v, degree, key16, lod, s);
   }
   if (timed) cudaEventRecord(f.events[2], s);
   if (e == cudaSuccess) {
@@ -287,20 +308,17 @@ sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t
   if (timed) cudaEventRecord(f.events[3], s);
   if (e == cudaSuccess) {
     BinArgs b{};
-    b.projected = static_cast<const Projected*>(f.projected.ptr);
+    b.spans = static_cast<const uint4*>(f.spans.ptr);
     b.order = static_cast<const uint32_t*>(f.order.ptr);
     b.count = &fc->visible;
     b.capacity = f.sources;
-    b.width = width, b.height = height, b.tilesX = f.tilesX, b.tilesY = f.tilesY;
+    b.width = view.width, b.height = view.height, b.tilesX = tilesX, b.tilesY = tilesY;
     b.instanceKeys = static_cast<uint32_t*>(f.instKeys.ptr);
     b.instanceValues = static_cast<uint32_t*>(f.instValues.ptr);
     b.instanceCapacity = f.instanceCapacity;
     b.instanceCount = &fc->instances;
     b.overflow = &fc->overflow;
-    b.status = static_cast<uint64_t*>(f.binStatus.ptr);
-    b.counters = counters + 2;
-    b.epoch = nextEpoch(1);
-    b.error = error;
+    b.blockSums = static_cast<uint32_t*>(f.binSums.ptr);
     e = launchBinning(b, s);
   }
   if (e == cudaSuccess) {
@@ -319,50 +337,70 @@ sk_status Context::enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t
   }
   if (e == cudaSuccess)
     e = launchTileRanges(static_cast<const uint32_t*>(f.instKeysSorted.ptr), &fc->instances,
-                         f.instanceCapacity, static_cast<uint2*>(f.ranges.ptr), f.tilesX * f.tilesY, s);
+                         f.instanceCapacity, static_cast<uint2*>(f.ranges.ptr), tilesX * tilesY, s);
   if (timed) cudaEventRecord(f.events[4], s);
   if (e == cudaSuccess) {
     CompositeArgs c{};
     c.projected = static_cast<const Projected*>(f.projected.ptr);
     c.values = static_cast<const uint32_t*>(f.instValuesSorted.ptr);
     c.ranges = static_cast<const uint2*>(f.ranges.ptr);
-    c.width = width, c.height = height, c.tilesX = f.tilesX, c.tilesY = f.tilesY;
+    c.width = view.width, c.height = view.height, c.tilesX = tilesX, c.tilesY = tilesY;
     for (int j = 0; j < 3; ++j) c.background[j] = static_cast<float>(policy.background[j]);
     c.opaque = 1;
     c.cutoff = policy.enable_early_termination ? kTransmittanceCutoff : 0.0f;
-    c.image = f.image.ptr;
+    c.image = view.image;
     c.format = imageFormat == SK_FORMAT_RGBA32F ? kRgba32f : kRgba8;
     c.fragments = &fc->fragments_lo;
     c.loaded = &fc->loaded;
     e = launchComposite(c, s);
   }
   if (timed) cudaEventRecord(f.events[5], s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(f.hostCounters, fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaEventRecord(f.done, s);
+  if (e == cudaSuccess && view.hostCounters)
+    e = cudaMemcpyAsync(view.hostCounters, fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s);
   return check(e, "frame");
 }
 
-// Reads the last frame's counters once it completed; grows the instance buffers and redraws
-// when the binning ran out of room.
+ViewTarget Context::plainView() {
+  ViewTarget v;
+  v.width = width;
+  v.height = height;
+  v.image = image.ptr;
+  v.counters = static_cast<FrameCounters*>(frameCounters.ptr);
+  v.hostCounters = static_cast<FrameCounters*>(hostCounters.ptr);
+  v.camera = static_cast<const Camera*>(camera.ptr);
+  return v;
+}
+
+sk_status Context::enqueuePlainFrame(const sk_frame& frame, uint32_t total) {
+  // The previous frame has completed, so the pinned camera can be rewritten.
+  *static_cast<Camera*>(hostCamera.ptr) = cameraFor(frame, width, height);
+  cudaError_t e = cudaMemcpyAsync(camera.ptr, hostCamera.ptr, sizeof(Camera),
+                                  cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return check(e, "camera upload");
+  sk_status st = enqueuePipeline(scratch, plainView(), frame, total, stream, timeStages);
+  if (st != SK_OK) return st;
+  return check(cudaEventRecord(done, stream), "frame");
+}
+
+// Reads the last frame's counters once it completed; grows the instance buffers and draws
+// again when the binning ran out of room.
 sk_status Context::finishFrame(bool wait) {
   if (!frameInFlight) return SK_OK;
   if (wait) {
-    const cudaError_t e = cudaEventSynchronize(frame.done);
+    const cudaError_t e = cudaEventSynchronize(done);
     if (e != cudaSuccess) return check(e, "frame wait");
-  } else if (cudaEventQuery(frame.done) != cudaSuccess) {
+  } else if (cudaEventQuery(done) != cudaSuccess) {
     return SK_OK;
   }
   frameInFlight = false;
   ++completed;
-  const FrameCounters c = *frame.hostCounters;
+  const FrameCounters c = *static_cast<const FrameCounters*>(hostCounters.ptr);
   if (c.overflow) {
-    // Grow to what the frame needed (plus headroom) and draw it again.
     const uint32_t need = static_cast<uint32_t>(std::min<uint64_t>(
-        uint64_t{c.instances} + c.instances / 4 + 1024, 0xffffffffu));
-    sk_status st = reserveFrame(frame, frame.sources, need);
+        uint64_t{c.instances} + c.instances / 4 + 1024, 0x7fffffffu));
+    sk_status st = reserveScratch(scratch, scratch.sources, need, scratch.maxTiles, stream);
     if (st != SK_OK) return st;
-    st = enqueueFrame(frame, lastFrame, lastTotal, stream, timeStages);
+    st = enqueuePlainFrame(lastFrame, lastTotal);
     if (st != SK_OK) return st;
     frameInFlight = true;
     --completed;
@@ -371,9 +409,9 @@ sk_status Context::finishFrame(bool wait) {
   lastCounters = c;
   if (timeStages) {
     float ms[5] = {0, 0, 0, 0, 0};
-    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], frame.events[i], frame.events[i + 1]);
+    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], scratch.events[i], scratch.events[i + 1]);
     float all = 0;
-    cudaEventElapsedTime(&all, frame.events[0], frame.events[5]);
+    cudaEventElapsedTime(&all, scratch.events[0], scratch.events[5]);
     stats.select_ms = ms[0], stats.cull_ms = ms[1], stats.sort_ms = ms[2];
     stats.bin_ms = ms[3], stats.composite_ms = ms[4], stats.gpu_ms = all;
   }
@@ -393,11 +431,11 @@ sk_status Context::uploadCloud(const sk_cloud_view& cloud, int maxSh, World& w) 
   const int degree = std::max(0, std::min({maxSh, ref.shDegree, 3}));
   const uint32_t stride = shDeviceStride(degree);
   std::vector<GpuSplat> packed(cloud.count);
-  host::packSplats(ref, 0, cloud.count, packed.data(), hostThreads());
+  host::packSplats(ref, 0, cloud.count, packed.data(), hostThreadsPublic());
   std::vector<uint32_t> sh(size_t{cloud.count} * stride);
-  host::packSh(ref, degree, 0, cloud.count, sh.data(), stride, hostThreads());
-  cudaError_t e = w.splats.allocate(std::max<size_t>(packed.size() * sizeof(GpuSplat), 32));
-  if (e == cudaSuccess) e = w.sh.allocate(std::max<size_t>(sh.size() * 4, 16));
+  host::packSh(ref, degree, 0, cloud.count, sh.data(), stride, hostThreadsPublic());
+  cudaError_t e = w.splats.allocate(packed.size() * sizeof(GpuSplat));
+  if (e == cudaSuccess) e = w.sh.allocate(sh.size() * 4);
   if (e != cudaSuccess) return check(e, "world upload");
   if (cloud.count) {
     e = cudaMemcpy(w.splats.ptr, packed.data(), packed.size() * sizeof(GpuSplat), cudaMemcpyHostToDevice);
@@ -451,11 +489,10 @@ sk_status sk_create(const sk_config* config, sk_context** out) {
   sk_default_policy(&ctx->policy);
   ctx->threshold.reset(ctx->policy.lod_error_pixels);
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SK_E_DEVICE;
-  for (auto& ev : ctx->frame.events)
-    if (cudaEventCreate(&ev) != cudaSuccess) return SK_E_DEVICE;
-  if (cudaEventCreateWithFlags(&ctx->frame.done, cudaEventDisableTiming) != cudaSuccess)
-    return SK_E_DEVICE;
-  if (ctx->reserveFrame(ctx->frame, 1, 1024) != SK_OK) return SK_E_DEVICE;
+  if (cudaEventCreateWithFlags(&ctx->done, cudaEventDisableTiming) != cudaSuccess) return SK_E_DEVICE;
+  if (ctx->reserveView(ctx->width, ctx->height) != SK_OK) return SK_E_DEVICE;
+  const uint32_t tiles = ((ctx->width + 15) / 16) * ((ctx->height + 15) / 16);
+  if (ctx->reserveScratch(ctx->scratch, 1, 1024, tiles, ctx->stream) != SK_OK) return SK_E_DEVICE;
   *out = reinterpret_cast<sk_context*>(ctx.release());
   return SK_OK;
 }
@@ -484,15 +521,15 @@ sk_status sk_resize(sk_context* handle, uint32_t width, uint32_t height) {
   if (width == 0 || height == 0 || width > 16384 || height > 16384) return SK_E_INVALID;
   sk_status st = ctx->finishFrame(true);
   if (st != SK_OK && st != SK_E_TIMEOUT) return st;
-  const uint32_t oldW = ctx->width, oldH = ctx->height;
+  st = ctx->reserveView(width, height);
+  if (st != SK_OK) return st;
+  const uint32_t tiles = ((width + 15) / 16) * ((height + 15) / 16);
+  st = ctx->reserveScratch(ctx->scratch, ctx->scratch.sources, ctx->scratch.instanceCapacity, tiles,
+                           ctx->stream);
+  if (st != SK_OK) return st;
   ctx->width = width;
   ctx->height = height;
-  st = ctx->reserveFrame(ctx->frame, ctx->frame.sources, ctx->frame.instanceCapacity);
-  if (st != SK_OK) {
-    ctx->width = oldW;
-    ctx->height = oldH;
-  }
-  return st;
+  return SK_OK;
 }
 
 sk_status sk_device_capabilities(sk_context* handle, sk_capabilities* out) {
@@ -557,8 +594,9 @@ sk_status sk_upload_world(sk_context* handle, const sk_cloud_view* cloud, int32_
   sk::World fresh;
   st = ctx->uploadCloud(*cloud, maxSh, fresh);
   if (st != SK_OK) return st;
-  st = ctx->reserveFrame(ctx->frame, cloud->count, std::max(ctx->frame.instanceCapacity,
-                                                             std::max(cloud->count, 1u) * 4));
+  st = ctx->reserveScratch(ctx->scratch, cloud->count,
+                           std::max(ctx->scratch.instanceCapacity, ctx->instanceGuess(cloud->count)),
+                           ctx->scratch.maxTiles, ctx->stream);
   if (st != SK_OK) return st;
   ctx->world = std::move(fresh);
   return SK_OK;
@@ -571,14 +609,14 @@ sk_status sk_create_slab(sk_context* handle, uint32_t capacity, int32_t shDegree
   if (st == SK_E_DEVICE) return st;
   cudaStreamSynchronize(ctx->stream);
   sk::World fresh;
-  cudaError_t e = fresh.splats.allocate(std::max<size_t>(size_t{capacity} * sizeof(sk::GpuSplat), 32));
-  if (e == cudaSuccess)
-    e = fresh.sh.allocate(std::max<size_t>(size_t{capacity} * sk::shDeviceStride(shDegree) * 4, 16));
+  cudaError_t e = fresh.splats.allocate(size_t{capacity} * sizeof(sk::GpuSplat));
+  if (e == cudaSuccess) e = fresh.sh.allocate(size_t{capacity} * sk::shDeviceStride(shDegree) * 4);
   if (e == cudaSuccess) e = cudaMemset(fresh.splats.ptr, 0, fresh.splats.bytes);
   if (e == cudaSuccess) e = cudaMemset(fresh.sh.ptr, 0, fresh.sh.bytes);
   if (e != cudaSuccess) return ctx->check(e, "slab");
-  st = ctx->reserveFrame(ctx->frame, capacity, std::max(ctx->frame.instanceCapacity,
-                                                        std::max(capacity, 1u) * 4));
+  st = ctx->reserveScratch(ctx->scratch, capacity,
+                           std::max(ctx->scratch.instanceCapacity, ctx->instanceGuess(capacity)),
+                           ctx->scratch.maxTiles, ctx->stream);
   if (st != SK_OK) return st;
   fresh.count = capacity;
   fresh.shDegree = shDegree;
@@ -643,7 +681,7 @@ sk_status sk_upload_lod_world(sk_context* handle, const sk_lod_view* tree, int32
   if (st != SK_OK) return st;
   const uint32_t capacity = std::min({budget, sk::kMaxLodBudgetPublic, std::max(tree->leaf_count, 1u)});
   cudaError_t e = fresh.clusters.allocate(clusters.size() * sizeof(sk::LodCluster));
-  if (e == cudaSuccess) e = fresh.leaves.allocate(std::max<size_t>(leaves.size() * 4, 4));
+  if (e == cudaSuccess) e = fresh.leaves.allocate(leaves.size() * 4);
   if (e == cudaSuccess)
     e = cudaMemcpy(fresh.clusters.ptr, clusters.data(), clusters.size() * sizeof(sk::LodCluster),
                    cudaMemcpyHostToDevice);
@@ -655,10 +693,12 @@ sk_status sk_upload_lod_world(sk_context* handle, const sk_lod_view* tree, int32
   fresh.leafRefCount = static_cast<uint32_t>(leaves.size());
   fresh.rounds = static_cast<uint32_t>(depth) + 1;
   fresh.lodCapacity = capacity;
-  st = ctx->reserveLod(ctx->frame, fresh);
+  st = ctx->reserveLod(ctx->scratch, fresh, ctx->stream);
   if (st != SK_OK) return st;
   // Projections and sort scratch scale with the cut, not with all resident nodes.
-  st = ctx->reserveFrame(ctx->frame, capacity, std::max(ctx->frame.instanceCapacity, capacity * 4));
+  st = ctx->reserveScratch(ctx->scratch, capacity,
+                           std::max(ctx->scratch.instanceCapacity, ctx->instanceGuess(capacity)),
+                           ctx->scratch.maxTiles, ctx->stream);
   if (st != SK_OK) return st;
   ctx->world = std::move(fresh);
   ctx->threshold.reset(ctx->threshold.policyPixels());
@@ -687,10 +727,9 @@ sk_status sk_draw(sk_context* handle, const sk_frame* frame) {
   if (!ctx->world.splats.ptr) total = 0;
   ctx->lastFrame = *frame;
   ctx->lastTotal = total;
-  ctx->lastFrame.ranges = nullptr;
   ctx->lastRanges.assign(frame->ranges, frame->ranges + (frame->ranges ? frame->range_count : 0));
   ctx->lastFrame.ranges = ctx->lastRanges.data();
-  st = ctx->enqueueFrame(ctx->frame, ctx->lastFrame, total, ctx->stream, ctx->timeStages);
+  st = ctx->enqueuePlainFrame(ctx->lastFrame, total);
   if (st != SK_OK) return st;
   ctx->frameInFlight = true;
   ++ctx->submitted;
@@ -716,10 +755,10 @@ sk_status sk_read_image(sk_context* handle, void* host, size_t bytes, int32_t fo
   if (format == SK_FORMAT_RGBA32F && !deviceFloat)
     return ctx->fail(SK_E_INVALID, "the context renders 8-bit images");
   if ((format == SK_FORMAT_RGBA8 && !deviceFloat) || (format == SK_FORMAT_RGBA32F && deviceFloat))
-    return ctx->check(cudaMemcpy(host, ctx->frame.image.ptr, need, cudaMemcpyDeviceToHost), "readback");
+    return ctx->check(cudaMemcpy(host, ctx->image.ptr, need, cudaMemcpyDeviceToHost), "readback");
   // Conversions on the host.
   std::vector<uint8_t> staging(pixels * (deviceFloat ? 16 : 4));
-  cudaError_t e = cudaMemcpy(staging.data(), ctx->frame.image.ptr, staging.size(), cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpy(staging.data(), ctx->image.ptr, staging.size(), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return ctx->check(e, "readback");
   uint8_t* out = static_cast<uint8_t*>(host);
   for (size_t i = 0; i < pixels; ++i) {
@@ -767,9 +806,9 @@ sk_status sk_read_visible(sk_context* handle, uint32_t* keys, void* projected, u
   if (count) *count = n;
   const uint32_t copy = std::min(n, capacity);
   cudaError_t e = cudaSuccess;
-  if (keys && copy) e = cudaMemcpy(keys, ctx->frame.keys.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
+  if (keys && copy) e = cudaMemcpy(keys, ctx->scratch.keys.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && projected && copy)
-    e = cudaMemcpy(projected, ctx->frame.projected.ptr, size_t{copy} * 32, cudaMemcpyDeviceToHost);
+    e = cudaMemcpy(projected, ctx->scratch.projected.ptr, size_t{copy} * 32, cudaMemcpyDeviceToHost);
   return ctx->check(e, "readback");
 }
 
@@ -781,7 +820,7 @@ sk_status sk_read_order(sk_context* handle, uint32_t* order, uint32_t capacity, 
   if (count) *count = n;
   const uint32_t copy = std::min(n, capacity);
   if (!order || !copy) return SK_OK;
-  return ctx->check(cudaMemcpy(order, ctx->frame.order.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
+  return ctx->check(cudaMemcpy(order, ctx->scratch.order.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
                     "readback");
 }
 
@@ -796,8 +835,24 @@ sk_status sk_read_cut(sk_context* handle, uint32_t* indices, uint32_t capacity, 
   if (lod6) std::memcpy(lod6, ctx->lastCounters.lod, 24);
   const uint32_t copy = std::min(n, capacity);
   if (!indices || !copy) return SK_OK;
-  return ctx->check(cudaMemcpy(indices, ctx->frame.lodIndices.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
+  return ctx->check(cudaMemcpy(indices, ctx->scratch.lodIndices.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
                     "readback");
+}
+
+sk_status sk_read_tile_lists(sk_context* handle, uint32_t* ranges, uint32_t* values,
+                             uint32_t capacity, uint32_t* count) {
+  SK_CTX(handle);
+  sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  const uint32_t n = std::min(ctx->lastCounters.instances, ctx->scratch.instanceCapacity);
+  if (count) *count = n;
+  cudaError_t e = cudaSuccess;
+  const size_t tiles = size_t{(ctx->width + 15) / 16} * ((ctx->height + 15) / 16);
+  if (ranges) e = cudaMemcpy(ranges, ctx->scratch.ranges.ptr, tiles * 8, cudaMemcpyDeviceToHost);
+  const uint32_t copy = std::min(n, capacity);
+  if (e == cudaSuccess && values && copy)
+    e = cudaMemcpy(values, ctx->scratch.instValuesSorted.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
+  return ctx->check(e, "readback");
 }
 
 size_t sk_sort_workspace_bytes(uint32_t capacity) { return sk::sortWorkspaceBytes(capacity); }
@@ -829,83 +884,3 @@ sk_status sk_radix_argsort_device(const uint32_t* d_keys, const uint32_t* d_coun
 }
 
 }  // extern "C"
-
-// ---- host-side world preparation ----------------------------------------------------------
-namespace {
-sk::host::CloudRef cloudRef(const sk_cloud_view& c) {
-  return sk::host::CloudRef{c.positions, c.covariances, c.colors, c.alphas, c.sh, c.count,
-                            c.sh ? std::max(0, std::min(c.sh_degree, 3)) : 0};
-}
-}  // namespace
-
-extern "C" {
-
-uint32_t sk_sh_device_stride(int32_t degree) { return sk::shDeviceStride(degree); }
-
-sk_status sk_pack_splats(const sk_cloud_view* cloud, uint32_t offset, uint32_t count, void* out) {
-  if (!cloud || !out || offset > cloud->count || count > cloud->count - offset) return SK_E_INVALID;
-  const auto ref = cloudRef(*cloud);
-  if (count && (!ref.positions || !ref.covariances || !ref.colors || !ref.alphas)) return SK_E_INVALID;
-  sk::host::packSplats(ref, offset, count, static_cast<sk::GpuSplat*>(out), sk::hostThreadsPublic());
-  return SK_OK;
-}
-
-sk_status sk_pack_sh(const sk_cloud_view* cloud, int32_t degree, uint32_t offset, uint32_t count,
-                     uint32_t* out, uint32_t stride) {
-  if (!cloud || !out || offset > cloud->count || count > cloud->count - offset) return SK_E_INVALID;
-  const auto ref = cloudRef(*cloud);
-  if (degree < 0 || degree > ref.shDegree || stride < sk::shPackedStride(degree)) return SK_E_INVALID;
-  sk::host::packSh(ref, degree, offset, count, out, stride, sk::hostThreadsPublic());
-  return SK_OK;
-}
-
-sk_status sk_build_lod_selection(const sk_lod_view* tree, sk_lod_cluster* clusters,
-                                 uint32_t clusterCapacity, uint32_t* clusterCount,
-                                 uint32_t* leaves, uint32_t leafCapacity, uint32_t* leafCount) {
-  if (!tree || !tree->layout || tree->nodes.count != tree->node_count) return SK_E_INVALID;
-  std::vector<sk::LodCluster> c;
-  std::vector<uint32_t> l;
-  sk::host::buildSelection(cloudRef(tree->nodes), reinterpret_cast<const sk::LodNode*>(tree->layout),
-                           tree->node_count, c, l);
-  if (clusterCount) *clusterCount = static_cast<uint32_t>(c.size());
-  if (leafCount) *leafCount = static_cast<uint32_t>(l.size());
-  if (clusters) std::memcpy(clusters, c.data(), std::min<size_t>(c.size(), clusterCapacity) * 64);
-  if (leaves) std::memcpy(leaves, l.data(), std::min<size_t>(l.size(), leafCapacity) * 4);
-  return SK_OK;
-}
-
-int64_t sk_lod_depth(const sk_lod_node* layout, uint32_t nodeCount, uint32_t leafCount) {
-  if (!layout) return -1;
-  return sk::host::lodDepth(reinterpret_cast<const sk::LodNode*>(layout), nodeCount, leafCount, nullptr);
-}
-
-uint64_t sk_world_bytes(uint64_t records, int32_t shDegree, uint64_t drawCapacity,
-                        uint64_t clusters, uint64_t leafRefs) {
-  return sk::host::worldBytes(records, shDegree, drawCapacity, clusters, leafRefs);
-}
-
-float sk_lod_threshold_update(float* state, uint32_t selected, uint32_t limited, uint32_t limit) {
-  if (!state) return 0.0f;
-  sk::host::LodThreshold t(state[0]);
-  t.restore(state[1]);
-  state[1] = t.update(selected, limited, limit);
-  return state[1];
-}
-
-}  // extern "C"
-
-extern "C" sk_status sk_read_tile_lists(sk_context* handle, uint32_t* ranges, uint32_t* values,
-                                        uint32_t capacity, uint32_t* count) {
-  SK_CTX(handle);
-  sk_status st = ctx->finishFrame(true);
-  if (st != SK_OK) return st;
-  const uint32_t n = std::min(ctx->lastCounters.instances, ctx->frame.instanceCapacity);
-  if (count) *count = n;
-  cudaError_t e = cudaSuccess;
-  const size_t tiles = size_t{ctx->frame.tilesX} * ctx->frame.tilesY;
-  if (ranges) e = cudaMemcpy(ranges, ctx->frame.ranges.ptr, tiles * 8, cudaMemcpyDeviceToHost);
-  const uint32_t copy = std::min(n, capacity);
-  if (e == cudaSuccess && values && copy)
-    e = cudaMemcpy(values, ctx->frame.instValuesSorted.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
-  return ctx->check(e, "readback");
-}

@@ -1,5 +1,6 @@
-// The renderer context behind the C ABI: device buffers of the resident world and of one
-// frame's scratch, the policy, the adaptive LOD threshold and the frame statistics.
+// The renderer context behind the C ABI: device buffers of the resident world, the reusable
+// scratch of one frame pipeline, the per-view outputs, the policy, the adaptive LOD threshold
+// and the frame statistics.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -17,6 +18,8 @@
 namespace sk {
 
 inline constexpr uint32_t kMaxLodBudgetPublic = 4000000;  // MetalLodSelection.h:18
+inline constexpr uint32_t kMaxRanges = 65536;             // MetalVisibilityPass.h:72
+inline constexpr float kTransmittanceCutoff = 1e-4f;
 inline int hostThreadsPublic() {
   return static_cast<int>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
 }
@@ -47,6 +50,18 @@ struct DeviceBuffer {
   void release();
 };
 
+// Owning pinned host allocation.
+struct PinnedBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  PinnedBuffer() = default;
+  PinnedBuffer(const PinnedBuffer&) = delete;
+  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+  ~PinnedBuffer() { release(); }
+  cudaError_t allocate(size_t n);
+  void release();
+};
+
 // A resident world: packed records, harmonics at the device stride, and for a hierarchy its
 // selection data.
 struct World {
@@ -58,27 +73,35 @@ struct World {
   uint32_t clusterCount = 0, leafRefCount = 0, rounds = 0, lodCapacity = 0;
 };
 
-// Everything one frame writes. One per stream that renders concurrently.
+// Everything one pipeline run writes besides its outputs; reused frame after frame on one
+// stream. One per stream that renders concurrently.
 struct FrameScratch {
-  uint32_t sources = 0, instanceCapacity = 0, tilesX = 0, tilesY = 0;
-  DeviceBuffer keys, projected, order, sortWorkspace, visStatus, binStatus;
+  uint32_t sources = 0, instanceCapacity = 0, maxTiles = 0;
+  DeviceBuffer keys, projected, spans, order, sortWorkspace, visStatus, binSums;
   DeviceBuffer instKeys, instValues, instKeysSorted, instValuesSorted, tileSortWorkspace;
-  DeviceBuffer ranges, image, rangeBuffer, rangeStarts, counters, frameCounters;
+  DeviceBuffer ranges, rangeBuffer, rangeStarts, counters;
   DeviceBuffer lodIndices, lodFrontier[2], lodCosts, lodOffsets, lodPackets, lodState, lodStatus,
       lodCounters;
   uint32_t lodFrontierCapacity = 0;
-  FrameCounters* hostCounters = nullptr;  // pinned
   cudaEvent_t events[6] = {};
-  cudaEvent_t done = nullptr;
   FrameScratch() = default;
   FrameScratch(const FrameScratch&) = delete;
   FrameScratch& operator=(const FrameScratch&) = delete;
   ~FrameScratch() {
-    if (hostCounters) cudaFreeHost(hostCounters);
     for (auto& e : events)
       if (e) cudaEventDestroy(e);
-    if (done) cudaEventDestroy(done);
   }
+};
+
+// Where one view's results go.
+struct ViewTarget {
+  uint32_t width = 0, height = 0;
+  void* image = nullptr;                   // device, the context's pixel format
+  FrameCounters* counters = nullptr;       // device
+  FrameCounters* hostCounters = nullptr;   // pinned; null: no readback
+  const Camera* camera = nullptr;          // device, written before the pipeline runs
+  uint32_t tilesX() const { return (width + kTileSize - 1) / kTileSize; }
+  uint32_t tilesY() const { return (height + kTileSize - 1) / kTileSize; }
 };
 
 struct Context {
@@ -91,7 +114,11 @@ struct Context {
   uint32_t lodLimit = 0;
   host::LodThreshold threshold;
   World world;
-  FrameScratch frame;
+  FrameScratch scratch;
+  // the plain renderer's own view: image, counters, camera
+  DeviceBuffer image, frameCounters, camera;
+  PinnedBuffer hostCounters, hostCamera;
+  cudaEvent_t done = nullptr;
   bool frameInFlight = false;
   sk_frame lastFrame{};
   std::vector<sk_range> lastRanges;
@@ -103,21 +130,26 @@ struct Context {
   std::atomic<bool> failed{false};
   std::string error;
 
-  ~Context() {
-    if (stream) cudaStreamDestroy(stream);
-  }
+  ~Context();
 
   sk_status fail(sk_status code, const std::string& message);
   sk_status check(cudaError_t e, const char* what);
   uint32_t nextEpoch(uint32_t n);
-  sk_status reserveFrame(FrameScratch& f, uint32_t sources, uint32_t instances);
-  sk_status reserveLod(FrameScratch& f, const World& w);
-  Camera cameraFor(const sk_frame& frame) const;
+  // Scratch for `sources` splats, `instances` tile instances and targets up to maxTiles tiles.
+  sk_status reserveScratch(FrameScratch& f, uint32_t sources, uint32_t instances, uint32_t maxTiles,
+                           cudaStream_t s);
+  sk_status reserveLod(FrameScratch& f, const World& w, cudaStream_t s);
+  sk_status reserveView(uint32_t width, uint32_t height);
+  Camera cameraFor(const sk_frame& frame, uint32_t width, uint32_t height) const;
   sk_status validateRanges(const sk_frame& frame, uint32_t* total) const;
-  sk_status enqueueFrame(FrameScratch& f, const sk_frame& frame, uint32_t total, cudaStream_t s,
-                         bool timed);
+  // The whole frame pipeline for one view on stream s; nothing waits on the host.
+  sk_status enqueuePipeline(FrameScratch& f, const ViewTarget& v, const sk_frame& frame,
+                            uint32_t total, cudaStream_t s, bool timed);
+  ViewTarget plainView();
+  sk_status enqueuePlainFrame(const sk_frame& frame, uint32_t total);
   sk_status finishFrame(bool wait);
   sk_status uploadCloud(const sk_cloud_view& cloud, int maxSh, World& w);
+  uint32_t instanceGuess(uint32_t sources) const;
 };
 
 }  // namespace sk
