@@ -33,6 +33,7 @@ typedef int32_t sk_status;
 #define SK_E_TIMEOUT 5     /* a bounded device wait gave up (the frame is wrong) */
 #define SK_E_UNSUPPORTED 6 /* a feature this build leaves out */
 #define SK_E_NO_WORLD 7    /* no world uploaded */
+#define SK_E_LIMIT 8       /* a size is beyond a fixed limit of the call; nothing was enqueued */
 
 #define SK_FORMAT_RGBA8 0   /* 4 bytes per pixel, row 0 on top */
 #define SK_FORMAT_RGBA32F 1 /* 16 bytes per pixel, row 0 on top */
@@ -203,6 +204,30 @@ sk_status sk_radix_argsort_device(const uint32_t* d_keys, const uint32_t* d_coun
                                   uint32_t capacity, int32_t bits, uint32_t* d_order,
                                   void* d_workspace, size_t workspace_bytes, uint32_t* d_error,
                                   void* stream);
+
+/* The same argsort with no workspace argument and no allocation. No counterpart in the
+ * reference: its Metal sort owns its buffers. For callers that may not allocate device memory
+ * while they run (cudaMalloc/cudaFree synchronise the whole device, which a render callback
+ * with a frame deadline cannot afford) and for code that owns no device allocator. The call
+ * allocates nothing and calls no allocating library; it enqueues two small memsets and the
+ * sort kernels on `stream` and returns.
+ *
+ * Limit: capacity <= SK_NOALLOC_SORT_MAX_KEYS (1,048,576 keys); a larger capacity returns
+ * SK_E_LIMIT and enqueues nothing. The workspace is a 13,115,648-byte array of this library's
+ * device module, zero when the module loads. The histogram accumulators and tile counters in
+ * it must be zero when a sort starts; each sort leaves them at zero and each call clears them
+ * again first, so the caller clears nothing. d_keys, d_count, d_order, d_error and bits mean
+ * what they mean for sk_radix_argsort_device.
+ *
+ * Setup: the first call on each device (the device current on the calling thread) looks up the
+ * array's device address, which may load the module; make that first call before any stream
+ * capture. There is one array per device: calls on one device whose sorts may overlap in time
+ * (different streams without an event between them, or several host threads) race on it and
+ * give wrong orders. Keep them ordered on one stream. */
+#define SK_NOALLOC_SORT_MAX_KEYS (1u << 20)
+sk_status sk_radix_argsort_noalloc(const uint32_t* d_keys, const uint32_t* d_count,
+                                   uint32_t capacity, int32_t bits, uint32_t* d_order,
+                                   uint32_t* d_error, void* stream);
 
 /* ---- host-side world preparation (no device needed) ----------------------------------- */
 /* Harmonics words per splat in the device layout: the reference's packed stride

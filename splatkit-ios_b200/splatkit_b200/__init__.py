@@ -30,8 +30,9 @@ SK_E_DEVICE = 4
 SK_E_TIMEOUT = 5
 SK_E_UNSUPPORTED = 6
 SK_E_NO_WORLD = 7
+SK_E_LIMIT = 8
 STATUS_NAMES = {0: "ok", 1: "invalid", 2: "out of memory", 3: "admission", 4: "device",
-                5: "timeout", 6: "unsupported", 7: "no world"}
+                5: "timeout", 6: "unsupported", 7: "no world", 8: "beyond a fixed limit"}
 
 FORMAT_RGBA8 = 0
 FORMAT_RGBA32F = 1
@@ -167,6 +168,10 @@ _SIGNATURES = {
                                                  ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_size_t, ctypes.c_void_p,
                                                  ctypes.c_void_p]),
+    "sk_radix_argsort_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_uint32, ctypes.c_int32,
+                                                  ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p]),
 }
 
 _lib: Optional[ctypes.CDLL] = None
@@ -466,6 +471,19 @@ def radix_argsort_device(keys_ptr: int, count_ptr: int, capacity: int, bits: int
                                            workspace_ptr, workspace_bytes, error_ptr, stream)
     if st != SK_OK:
         raise SplatError(st, "sk_radix_argsort_device")
+
+
+NOALLOC_SORT_MAX_KEYS = 1 << 20  # SK_NOALLOC_SORT_MAX_KEYS
+
+
+def radix_argsort_noalloc(keys_ptr: int, count_ptr: int, capacity: int, bits: int, order_ptr: int,
+                          error_ptr: int, stream: int = 0):
+    """The same sort with its workspace in the library's fixed device array: no allocation,
+    capacity at most NOALLOC_SORT_MAX_KEYS (SK_E_LIMIT beyond), calls on one device ordered."""
+    st = library().sk_radix_argsort_noalloc(keys_ptr, count_ptr, capacity, bits, order_ptr,
+                                            error_ptr, stream)
+    if st != SK_OK:
+        raise SplatError(st, "sk_radix_argsort_noalloc")
 
 
 def sort_workspace_bytes(capacity: int) -> int:
