@@ -84,44 +84,55 @@ __device__ __forceinline__ uint32_t coverageForm(const uint4 lo, const uint4 hi,
   return reach;
 }
 
-struct Pixel {
-  float T = 1.0f, r = 0.0f, g = 0.0f, b = 0.0f;
-  bool done;
+// A thread's two pixels, packed so that Blackwell's paired FP32 instructions (FADD2, FMUL2,
+// FFMA2: two independent IEEE operations, each rounded like its scalar form) work on both at once.
+struct PixelPair {
+  float2 T = make_float2(1.0f, 1.0f), r = make_float2(0.0f, 0.0f), g = make_float2(0.0f, 0.0f),
+         b = make_float2(0.0f, 0.0f);
+  bool done0, done1;
 };
 
-// One pixel against one splat; dyTerms = (m01 * dy, m11 * dy), shared by the row.
-__device__ __forceinline__ void blend(Pixel& p, const float4 w0, const float4 w1, const float4 c,
-                                      float px, float m01dy, float m11dy, float cutoff,
-                                      uint32_t& blended) {
-  if (p.done) return;
-  const float dx = __fsub_rn(px, w0.x);
-  const float u = __fmaf_rn(w0.z, dx, m01dy);
-  const float v = __fmaf_rn(w1.x, dx, m11dy);
-  if (!(fabsf(u) <= w1.z && fabsf(v) <= w1.z)) return;
-  const float q = __fmul_rn(0.5f, __fmaf_rn(u, u, __fmul_rn(v, v)));
-  if (!(q <= w1.w)) return;
-  const float alpha = fminf(c.x * __expf(-q), 1.0f);
-  const float weight = p.T * alpha;
-  p.r += weight * c.y;
-  p.g += weight * c.z;
-  p.b += weight * c.w;
-  p.T *= 1.0f - alpha;
-  ++blended;
-  if (p.T < cutoff) p.done = true;
+__device__ __forceinline__ float2 pair(float v) { return make_float2(v, v); }
+
+// Both pixels against one splat. px = the two pixel centres' x; m01dy, m11dy = m01 dy and
+// m11 dy, shared by the row. The coverage terms u, v, q are the oracle's FP32 sequence per pixel
+// (px - cx is px + (-cx) exactly); an uncovered or finished pixel takes alpha 0, which leaves
+// its colour and transmittance bit for bit as they were.
+__device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const float4 w1,
+                                          const float4 c, float2 px, float m01dy, float m11dy,
+                                          float cutoff, uint32_t& blended) {
+  const float2 dx = __fadd2_rn(px, pair(-w0.x));
+  const float2 u = __ffma2_rn(pair(w0.z), dx, pair(m01dy));
+  const float2 v = __ffma2_rn(pair(w1.x), dx, pair(m11dy));
+  const float2 q = __fmul2_rn(pair(0.5f), __ffma2_rn(u, u, __fmul2_rn(v, v)));
+  const bool c0 = !p.done0 && fabsf(u.x) <= w1.z && fabsf(v.x) <= w1.z && q.x <= w1.w;
+  const bool c1 = !p.done1 && fabsf(u.y) <= w1.z && fabsf(v.y) <= w1.z && q.y <= w1.w;
+  if (!__any_sync(0xffffffffu, c0 || c1)) return;  // the whole strip misses this splat
+  const float a0 = c0 ? fminf(c.x * __expf(-q.x), 1.0f) : 0.0f;
+  const float a1 = c1 ? fminf(c.x * __expf(-q.y), 1.0f) : 0.0f;
+  const float2 alpha = make_float2(a0, a1);
+  const float2 weight = __fmul2_rn(p.T, alpha);
+  p.r = __ffma2_rn(weight, pair(c.y), p.r);
+  p.g = __ffma2_rn(weight, pair(c.z), p.g);
+  p.b = __ffma2_rn(weight, pair(c.w), p.b);
+  p.T = __fmul2_rn(p.T, __fadd2_rn(pair(1.0f), make_float2(-a0, -a1)));
+  blended += static_cast<uint32_t>(c0) + static_cast<uint32_t>(c1);
+  p.done0 = p.done0 || p.T.x < cutoff;
+  p.done1 = p.done1 || p.T.y < cutoff;
 }
 
 template <int kFormat>
-__device__ __forceinline__ void writePixel(const CompositeArgs& a, const Pixel& p, uint32_t col,
-                                           uint32_t row) {
+__device__ __forceinline__ void writePixel(const CompositeArgs& a, float T, float r, float g,
+                                           float b, uint32_t col, uint32_t row) {
   if (col >= a.width || row >= a.height) return;
   float outR, outG, outB, outA;
   if (a.opaque) {
-    outR = p.r + p.T * a.background[0];
-    outG = p.g + p.T * a.background[1];
-    outB = p.b + p.T * a.background[2];
+    outR = r + T * a.background[0];
+    outG = g + T * a.background[1];
+    outB = b + T * a.background[2];
     outA = 1.0f;
   } else {
-    outR = p.r, outG = p.g, outB = p.b, outA = 1.0f - p.T;
+    outR = r, outG = g, outB = b, outA = 1.0f - T;
   }
   outR = fminf(fmaxf(outR, 0.0f), 1.0f);
   outG = fminf(fmaxf(outG, 0.0f), 1.0f);
@@ -154,9 +165,10 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   const float halfH = 0.5f * height;
   const uint2 range = a.ranges[tile];
   const uint32_t below = lanemaskLt();
-  Pixel p0, p1;
-  p0.done = !(col < a.width && row < a.height);
-  p1.done = !(col + 1 < a.width && row < a.height);
+  const float2 px = make_float2(px0, px1);
+  PixelPair p;
+  p.done0 = !(col < a.width && row < a.height);
+  p.done1 = !(col + 1 < a.width && row < a.height);
   uint32_t blended = 0, loaded = 0;
   for (uint32_t start = range.x; start < range.y; start += kThreads) {
     const uint32_t inBatch = min(kThreads, range.y - start);
@@ -170,7 +182,7 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
       sm.splat[threadIdx.x] = s;
     }
     __syncthreads();
-    if (!__all_sync(0xffffffffu, p0.done && p1.done)) {
+    if (!__all_sync(0xffffffffu, p.done0 && p.done1)) {
       // this warp's entries, in batch (= depth) order
       uint32_t count = 0;
       for (uint32_t c = 0; c < inBatch; c += 32) {
@@ -182,7 +194,7 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
       }
       __syncwarp();
       for (uint32_t k0 = 0; k0 < count; k0 += 16) {
-        if (__all_sync(0xffffffffu, p0.done && p1.done)) break;
+        if (__all_sync(0xffffffffu, p.done0 && p.done1)) break;
         const uint32_t k1 = min(count, k0 + 16);
         for (uint32_t k = k0; k < k1; ++k) {
           const Splat2D& s = sm.splat[sm.list[warp][k]];
@@ -191,12 +203,11 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
           const float4 c = reinterpret_cast<const float4*>(&s)[2];
           const float dy = __fsub_rn(py, w0.y);
           const float m01dy = __fmul_rn(w0.w, dy), m11dy = __fmul_rn(w1.y, dy);
-          blend(p0, w0, w1, c, px0, m01dy, m11dy, a.cutoff, blended);
-          blend(p1, w0, w1, c, px1, m01dy, m11dy, a.cutoff, blended);
+          blendPair(p, w0, w1, c, px, m01dy, m11dy, a.cutoff, blended);
         }
       }
     }
-    if (__syncthreads_count((p0.done && p1.done) ? 0 : 1) == 0) break;
+    if (__syncthreads_count((p.done0 && p.done1) ? 0 : 1) == 0) break;
   }
   // blended fragments: one 64-bit add per block
   __shared__ unsigned long long blockFragments;
@@ -209,8 +220,8 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   if (threadIdx.x == 0 && blockFragments)
     atomicAdd(reinterpret_cast<unsigned long long*>(a.fragments), blockFragments);
   if (threadIdx.x == 0 && loaded) atomicAdd(a.loaded, loaded);
-  writePixel<kFormat>(a, p0, col, row);
-  writePixel<kFormat>(a, p1, col + 1, row);
+  writePixel<kFormat>(a, p.T.x, p.r.x, p.g.x, p.b.x, col, row);
+  writePixel<kFormat>(a, p.T.y, p.r.y, p.g.y, p.b.y, col + 1, row);
 }
 
 }  // namespace
