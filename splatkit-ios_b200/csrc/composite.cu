@@ -10,11 +10,11 @@
 // termination when the remaining transmittance drops below `cutoff`.
 //
 // A block of 128 threads owns a tile; each thread owns two horizontally adjacent pixels and each
-// warp a 16x4-pixel strip. The block walks the tile's list in batches of 128 records: thread i
+// warp an 8x8-pixel quadrant. The block walks the tile's list in batches of 128 records: thread i
 // fetches record i (two 128-bit loads), turns it into the coverage form (pixel centre, inverse
-// axes, radius, log cutoff, colour) in shared memory and marks which of the four strips its
-// quad's box reaches. Each warp compacts, by ballot, the batch entries that reach it and sweeps
-// only those, both of its pixels per entry. The coverage decision (quad bound and 1/255 cutoff)
+// axes, radius, log cutoff, colour) in shared memory and marks which of the four quadrants its
+// quad overlaps (separating-axis test). Each warp compacts, by ballot, the batch entries that
+// reach it and sweeps only those, both of its pixels per entry. The coverage decision (quad bound and 1/255 cutoff)
 // is a fixed sequence of correctly rounded operations, bit-identical to the host oracle's FP32
 // formula.
 #include <cuda_runtime.h>
@@ -27,7 +27,7 @@ namespace {
 
 constexpr uint32_t kThreads = kTileSize * kTileSize / 2;  // 128: two pixels per thread
 constexpr uint32_t kWarps = kThreads / 32;
-constexpr uint32_t kStripRows = kTileSize / kWarps;  // 4 rows of 16 pixels per warp
+constexpr uint32_t kQuadrant = kTileSize / 2;  // each warp owns an 8x8 quadrant
 
 struct alignas(16) Splat2D {
   float cx, cy, m00, m01;
@@ -38,11 +38,11 @@ static_assert(sizeof(Splat2D) == 48, "Splat2D is three 16-byte words");
 
 struct CompositeSmem {
   Splat2D splat[kThreads];
-  uint8_t list[kWarps][kThreads];  // per warp: batch entries whose box reaches its strip
-  uint8_t reach[kThreads];         // per entry: bit w set when it reaches strip w
+  uint8_t list[kWarps][kThreads];  // per warp: batch entries whose quad reaches its quadrant
+  uint8_t reach[kThreads];         // per entry: bit w set when it reaches quadrant w
 };
 
-// Fills the coverage form; returns the bitmask of warp strips its box reaches.
+// Fills the coverage form; returns the bitmask of the warp quadrants its quad overlaps.
 __device__ __forceinline__ uint32_t coverageForm(const uint4 lo, const uint4 hi, float halfW,
                                                  float halfH, float tileX, float tileTop,
                                                  Splat2D& s) {
@@ -67,18 +67,25 @@ __device__ __forceinline__ uint32_t coverageForm(const uint4 lo, const uint4 hi,
     s.radius = -1.0f;
     return 0u;
   }
-  // |s|,|t| <= radius bounds the offset by radius * (|a1| + |a2|) per axis; half a pixel of
-  // slack keeps the box conservative against the rounding of the inverse.
-  const float ex = s.radius * (fabsf(a1x) + fabsf(a2x)) + 0.5f;
-  const float ey = s.radius * (fabsf(a1y) + fabsf(a2y)) + 0.5f;
-  if (s.cx + ex < tileX + 0.5f || s.cx - ex > tileX + (kTileSize - 0.5f)) return 0u;
-  const float y0 = s.cy - ey, y1 = s.cy + ey;
+  // Separating axes of the quad c + s a1 + t a2 (|s|, |t| <= radius) against each quadrant's
+  // square, taken half a pixel beyond its pixel centres (4 px from the quadrant centre): the
+  // screen x and y axes and the normals of a1 and a2. The slack keeps the test conservative
+  // against the rounding of the inverse used by the coverage decision.
+  constexpr float kHalf = 0.5f * kQuadrant;
+  const float ex = s.radius * (fabsf(a1x) + fabsf(a2x)) + kHalf;
+  const float ey = s.radius * (fabsf(a1y) + fabsf(a2y)) + kHalf;
+  const float n1x = -a1y, n1y = a1x, n2x = -a2y, n2y = a2x;
+  const float e1 = s.radius * fabsf(a2x * n1x + a2y * n1y) + kHalf * (fabsf(n1x) + fabsf(n1y));
+  const float e2 = s.radius * fabsf(a1x * n2x + a1y * n2y) + kHalf * (fabsf(n2x) + fabsf(n2y));
   uint32_t reach = 0;
 #pragma unroll
   for (uint32_t w = 0; w < kWarps; ++w) {
-    // strip w's pixel centres, y up: from tileTop - 4w - 0.5 down by three rows
-    const float top = tileTop - static_cast<float>(w * kStripRows) - 0.5f;
-    const bool hit = !(y1 < top - (kStripRows - 1) || y0 > top);
+    // quadrant w's centre, y up
+    const float qx = tileX + static_cast<float>((w & 1u) * kQuadrant) + kHalf;
+    const float qy = tileTop - static_cast<float>((w >> 1) * kQuadrant) - kHalf;
+    const float dx = qx - s.cx, dy = qy - s.cy;
+    const bool hit = fabsf(dx) <= ex && fabsf(dy) <= ey && fabsf(dx * n1x + dy * n1y) <= e1 &&
+                     fabsf(dx * n2x + dy * n2y) <= e2;
     reach |= hit ? (1u << w) : 0u;
   }
   return reach;
@@ -107,7 +114,7 @@ __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const f
   const float2 q = __fmul2_rn(pair(0.5f), __ffma2_rn(u, u, __fmul2_rn(v, v)));
   const bool c0 = !p.done0 && fabsf(u.x) <= w1.z && fabsf(v.x) <= w1.z && q.x <= w1.w;
   const bool c1 = !p.done1 && fabsf(u.y) <= w1.z && fabsf(v.y) <= w1.z && q.y <= w1.w;
-  if (!__any_sync(0xffffffffu, c0 || c1)) return;  // the whole strip misses this splat
+  if (!__any_sync(0xffffffffu, c0 || c1)) return;  // the whole quadrant misses this splat
   const float a0 = c0 ? fminf(c.x * __expf(-q.x), 1.0f) : 0.0f;
   const float a1 = c1 ? fminf(c.x * __expf(-q.y), 1.0f) : 0.0f;
   const float2 alpha = make_float2(a0, a1);
@@ -154,8 +161,8 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   const uint32_t tile = blockIdx.x;
   const uint32_t tx = tile % a.tilesX, ty = tile / a.tilesX;
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
-  const uint32_t col = tx * kTileSize + (lane % 8u) * 2u;  // and col + 1
-  const uint32_t row = ty * kTileSize + warp * kStripRows + lane / 8u;
+  const uint32_t col = tx * kTileSize + (warp & 1u) * kQuadrant + (lane % 4u) * 2u;  // and col + 1
+  const uint32_t row = ty * kTileSize + (warp >> 1) * kQuadrant + lane / 4u;
   const float height = static_cast<float>(a.height);
   const float px0 = static_cast<float>(col) + 0.5f, px1 = px0 + 1.0f;
   const float py = static_cast<float>(a.height - row) - 0.5f;  // y up, as NDC
