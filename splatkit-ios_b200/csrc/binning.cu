@@ -114,33 +114,43 @@ __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant_
     }
     __syncthreads();
     const uint32_t base = tileBase + warpBase[warp];
+    // Emission: the warp writes its items' instances one item at a time, all lanes together, so
+    // each store covers a contiguous run of the output (the item's tiles in increasing box
+    // order). Lane l takes box tiles l and l + 32 of a masked span, or every 32nd tile of a
+    // span that lists its whole box.
+    const uint32_t below = lanemaskLt();
 #pragma unroll
     for (uint32_t r = 0; r < kItems; ++r) {
-      if (cnt[r] == 0) continue;
-      uint32_t at = base + rowExclusive[r];
-      const uint32_t x0 = span[r].x & 0xffffu, y0 = span[r].x >> 16;
-      const uint32_t w = span[r].y & 0xffffu, area = span[r].y >> 16;
-      if (area > 64) {
-        for (uint32_t k = 0; k < area; ++k, ++at) {
-          if (at < a.instanceCapacity) {
-            a.instanceKeys[at] = (y0 + k / w) * a.tilesX + x0 + k % w;
-            a.instanceValues[at] = value[r];
+      const uint32_t at = base + rowExclusive[r];
+      uint32_t pending = __ballot_sync(0xffffffffu, cnt[r] != 0);
+      while (pending) {
+        const int j = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const uint32_t sx = __shfl_sync(0xffffffffu, span[r].x, j);
+        const uint32_t sy = __shfl_sync(0xffffffffu, span[r].y, j);
+        const uint32_t lo = __shfl_sync(0xffffffffu, span[r].z, j);
+        const uint32_t hi = __shfl_sync(0xffffffffu, span[r].w, j);
+        const uint32_t val = __shfl_sync(0xffffffffu, value[r], j);
+        const uint32_t first = __shfl_sync(0xffffffffu, at, j);
+        const uint32_t x0 = sx & 0xffffu, y0 = sx >> 16;
+        const uint32_t w = sy & 0xffffu, area = sy >> 16;
+        // k / w for k < area <= 16641 and w <= 129: (k + 1/2) / w is at least 1/(2w) away from
+        // an integer and the float product errs by far less, so truncation gives the quotient.
+        const float rw = 1.0f / static_cast<float>(w);
+        const uint32_t rowStart = y0 * a.tilesX + x0;
+        auto emit = [&](uint32_t k, uint32_t slot) {
+          const uint32_t q = static_cast<uint32_t>((static_cast<float>(k) + 0.5f) * rw);
+          const uint32_t id = rowStart + q * a.tilesX + (k - q * w);
+          if (slot < a.instanceCapacity) {
+            a.instanceKeys[slot] = id;
+            a.instanceValues[slot] = val;
           }
-        }
-      } else {
-        // row by row through the mask: no division
-        const uint64_t m = (static_cast<uint64_t>(span[r].w) << 32) | span[r].z;
-        const uint64_t rowBits = (w >= 64) ? ~0ull : ((1ull << w) - 1);
-        const uint32_t rows = area / w;  // area = w * rows <= 64, so row * w stays below 64
-        uint32_t rowTile = y0 * a.tilesX + x0;
-        for (uint32_t row = 0; row < rows; ++row, rowTile += a.tilesX) {
-          for (uint64_t bits = (m >> (row * w)) & rowBits; bits; bits &= bits - 1, ++at) {
-            const uint32_t x = static_cast<uint32_t>(__ffsll(static_cast<long long>(bits)) - 1);
-            if (at < a.instanceCapacity) {
-              a.instanceKeys[at] = rowTile + x;
-              a.instanceValues[at] = value[r];
-            }
-          }
+        };
+        if (area > 64) {
+          for (uint32_t k = lane; k < area; k += 32) emit(k, first + k);
+        } else {
+          if ((lo >> lane) & 1u) emit(lane, first + __popc(lo & below));
+          if (hi != 0u && ((hi >> lane) & 1u)) emit(lane + 32, first + __popc(lo) + __popc(hi & below));
         }
       }
     }
