@@ -45,9 +45,16 @@ __global__ void __launch_bounds__(kThreads) binCountKernel(const __grid_constant
   }
 }
 
+// One warp's items for the emission loop: span, and (projected index, first output slot).
+struct ItemStage {
+  uint4 span[32 * kItems];
+  uint2 value[32 * kItems];
+};
+
 // Pass 2: each block sums the totals of the blocks before it, then writes its instances.
 __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant__ BinArgs a) {
   __shared__ uint32_t warpBase[kThreads / 32];
+  __shared__ ItemStage itemStage[kThreads / 32];
   __shared__ uint32_t tileBase;
   const uint32_t n = min(*a.count, a.capacity);
   const uint32_t tiles = (n + kTileSplats - 1) / kTileSplats;
@@ -117,26 +124,31 @@ __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant_
     // Emission: the warp writes its items' instances one item at a time, all lanes together, so
     // each store covers a contiguous run of the output (the item's tiles in increasing box
     // order). Lane l takes box tiles l and l + 32 of a masked span, or every 32nd tile of a
-    // span that lists its whole box.
+    // span that lists its whole box. Items are staged in shared memory and read back by
+    // broadcast.
     const uint32_t below = lanemaskLt();
+    ItemStage& stage = itemStage[warp];
 #pragma unroll
     for (uint32_t r = 0; r < kItems; ++r) {
-      const uint32_t at = base + rowExclusive[r];
+      stage.span[r * 32 + lane] = span[r];
+      stage.value[r * 32 + lane] = make_uint2(value[r], base + rowExclusive[r]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (uint32_t r = 0; r < kItems; ++r) {
       uint32_t pending = __ballot_sync(0xffffffffu, cnt[r] != 0);
       while (pending) {
-        const int j = __ffs(pending) - 1;
+        const uint32_t j = r * 32 + (__ffs(pending) - 1);
         pending &= pending - 1;
-        const uint32_t sx = __shfl_sync(0xffffffffu, span[r].x, j);
-        const uint32_t sy = __shfl_sync(0xffffffffu, span[r].y, j);
-        const uint32_t lo = __shfl_sync(0xffffffffu, span[r].z, j);
-        const uint32_t hi = __shfl_sync(0xffffffffu, span[r].w, j);
-        const uint32_t val = __shfl_sync(0xffffffffu, value[r], j);
-        const uint32_t first = __shfl_sync(0xffffffffu, at, j);
-        const uint32_t x0 = sx & 0xffffu, y0 = sx >> 16;
-        const uint32_t w = sy & 0xffffu, area = sy >> 16;
+        const uint4 sp = stage.span[j];
+        const uint2 vf = stage.value[j];
+        const uint32_t val = vf.x, first = vf.y;
+        const uint32_t x0 = sp.x & 0xffffu, y0 = sp.x >> 16;
+        const uint32_t w = sp.y & 0xffffu, area = sp.y >> 16;
+        const uint32_t lo = sp.z, hi = sp.w;
         // k / w for k < area <= 16641 and w <= 129: (k + 1/2) / w is at least 1/(2w) away from
         // an integer and the float product errs by far less, so truncation gives the quotient.
-        const float rw = 1.0f / static_cast<float>(w);
+        const float rw = __frcp_rn(static_cast<float>(w));
         const uint32_t rowStart = y0 * a.tilesX + x0;
         auto emit = [&](uint32_t k, uint32_t slot) {
           const uint32_t q = static_cast<uint32_t>((static_cast<float>(k) + 0.5f) * rw);
