@@ -134,22 +134,24 @@ def stage_bytes(stats, bits, n=SPLATS, width=WIDTH, height=HEIGHT, sh_words=24):
     tiles = ((width + 15) // 16) * ((height + 15) // 16)
     return {
         # 32 B record per source splat, the SH record (96 B at SH3, device stride) of each
-        # survivor, then a 4 B key and a 32 B projected record per survivor
-        "cull": 32 * n + 4 * sh_words * v + 36 * v,
+        # survivor, then a 4 B key, a 32 B projected record and a 16 B tile span per survivor
+        "cull": 32 * n + 4 * sh_words * v + 52 * v,
         # one all-digit histogram read + per pass read key(+value) and write key+value; the
         # last pass skips the key write: 60 B/key at 32 bits, 28 B/key at 16 bits
         "sort": (60 if bits == 32 else 28) * v,
-        # binning reads order + projected, writes (tile, value); the 16-bit tile sort moves
-        # 28 B per instance plus the sorted key write; ranges read the keys
-        "bin": 36 * v + 8 * inst + 32 * inst + 4 * inst + 8 * tiles,
+        # count and emit each read order + span (20 B per survivor), emit writes (tile, value);
+        # the 16-bit tile sort reads the keys once for its histogram and moves 16 B per
+        # instance per pass (sorted keys written too); ranges read the keys, write 8 B per tile
+        "bin": 40 * v + 8 * inst + 4 * inst + 32 * inst + 4 * inst + 8 * tiles,
         # index + projected record per list entry read, RGBA8 image write
         "composite": 36 * read + width * height * 4,
     }
 
 
-def traffic_from_profiles(kernel_tag):
+def traffic_from_profiles(stem):
     """DRAM bytes per launch from the committed ncu summary of this kernel, when present."""
-    for path in sorted((ROOT / "profiles").glob(f"{kernel_tag}*.md")):
+    path = ROOT / "profiles" / f"{stem}.md"
+    if path.exists():
         m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", path.read_text())
         if m:
             return float(m.group(1))
@@ -308,7 +310,9 @@ def run_ours(args):
         achieved = bytes_by_stage[dominant] / (mean[dominant + "_ms"] / 1000.0) / 1e9
         kernel_tag = {"cull": "visibility", "sort": "radix_sort", "bin": "binning",
                       "composite": "composite"}[dominant]
-        traffic = traffic_from_profiles(kernel_tag)
+        profile = {"cull": "visibility_1m_sh3_1080p", "sort": "radix_sort_scatter_depth_1m_sh3_1080p",
+                   "bin": "binning_emit_1m_sh3_1080p", "composite": "composite_1m_sh3_1080p"}[dominant]
+        traffic = traffic_from_profiles(profile) if args.bits == 16 else None
         passes = 2 if args.bits == 16 else 4
         # visibility, depth sort (histogram + passes), bin count + emit, tile sort, ranges, composite
         launches_per_frame = 1 + (1 + passes) + 2 + 3 + 1 + 1
@@ -320,7 +324,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": kernel_tag, "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "algorithmic_bytes": bytes_by_stage[dominant]},
+                         "algorithmic_bytes": bytes_by_stage[dominant],
+                         "profile": f"profiles/{profile}.md"},
             "stages_ms": mean,
             "stage_gbs": {k: bytes_by_stage[k] / (mean[k + "_ms"] / 1000.0) / 1e9
                           for k in bytes_by_stage},
