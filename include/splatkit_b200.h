@@ -193,6 +193,58 @@ sk_status sk_read_cut(sk_context* ctx, uint32_t* indices, uint32_t capacity, uin
 sk_status sk_read_tile_lists(sk_context* ctx, uint32_t* ranges, uint32_t* values,
                              uint32_t capacity, uint32_t* count);
 
+/* ---- batched multi-view rendering ---------------------------------------------------------
+ * Many views, of one or several contexts' resident (flat) worlds and of different target sizes,
+ * drawn together: each stage runs once over the whole batch. The same frame pipeline and
+ * arithmetic as sk_draw, so every view's image and survivor count equal what sk_draw gives for
+ * that view with 16-bit depth keys. Submissions go round robin to `lanes` CUDA streams and
+ * overlap on the device; a submission's results (RGBA8 images, survivor counts) are copied to
+ * pinned host memory by the same stream and stay readable until its lane is reused, `lanes`
+ * submissions later. The contexts' worlds must not be replaced while a submission that draws
+ * them is in flight. The batch keeps no reference to a context beyond the submit call. */
+typedef struct sk_batch sk_batch;
+
+typedef struct {
+  int32_t device;
+  uint32_t lanes;      /* submissions in flight, >= 1 */
+  uint32_t max_views;  /* most views one submission may hold, 1..65536 */
+  uint32_t use_graphs; /* 1: each lane captures its stage sequence as a CUDA graph and replays it
+                          while its views keep their worlds, ranges and sizes */
+} sk_batch_config;
+
+typedef struct {
+  sk_context* world;   /* the context whose resident world this view draws */
+  sk_frame frame;      /* camera; at most one range (none: the whole world) */
+  uint32_t width, height;
+} sk_batch_view;
+
+typedef struct {
+  uint32_t views;
+  uint32_t visible;    /* survivors over all views */
+  uint32_t instances;  /* tile instances over all views */
+  uint32_t device_error;
+  double gpu_ms;       /* the submission's stages, device time */
+  uint64_t fragments;
+} sk_batch_stats;
+
+sk_status sk_batch_create(const sk_batch_config* config, sk_batch** out);
+void sk_batch_destroy(sk_batch* batch);
+const char* sk_batch_last_error(const sk_batch* batch);
+/* The policy every view is drawn with; sort_depth_bits must be 16. */
+sk_status sk_batch_apply_render_policy(sk_batch* batch, const sk_policy* policy);
+/* Enqueues the views and returns at once with a ticket (waits only when the next lane is still
+ * busy). All views must draw the same harmonics degree (min of the frame's and the world's). */
+sk_status sk_batch_submit(sk_batch* batch, const sk_batch_view* views, uint32_t count,
+                          uint64_t* ticket);
+sk_status sk_batch_poll(sk_batch* batch, uint64_t ticket, int32_t* done);
+sk_status sk_batch_wait(sk_batch* batch, uint64_t ticket);
+/* View `view` of a completed submission as RGBA8 rows, top row first (waits if needed). */
+sk_status sk_batch_read_image(sk_batch* batch, uint64_t ticket, uint32_t view, void* host,
+                              size_t bytes);
+sk_status sk_batch_view_visible(sk_batch* batch, uint64_t ticket, uint32_t view,
+                                uint32_t* visible);
+sk_status sk_batch_get_stats(sk_batch* batch, uint64_t ticket, sk_batch_stats* out);
+
 /* ---- component operators over caller device memory ----------------------------------- */
 /* MetalRadixSort (splatkit-ios/.../metal/sort/MetalRadixSort.h:13-54): stable ascending argsort
  * of min(*d_count, capacity) keys (d_count is a device word), 16 or 32 bits; d_keys is left

@@ -49,9 +49,13 @@ __global__ void __launch_bounds__(kThreads) binCountKernel(const __grid_constant
 struct ItemStage {
   uint4 span[32 * kItems];
   uint2 value[32 * kItems];
+  uint2 grid[32 * kItems];  // batch: (first tile id, tiles per row) of the item's view
 };
 
 // Pass 2: each block sums the totals of the blocks before it, then writes its instances.
+// kBatch: the survivors are a batch's views back to back in depth-rank order (rank i belongs to
+// view v when viewFirst[v] <= i < viewFirst[v + 1]); tile ids are batch-wide.
+template <bool kBatch>
 __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant__ BinArgs a) {
   __shared__ uint32_t warpBase[kThreads / 32];
   __shared__ ItemStage itemStage[kThreads / 32];
@@ -132,6 +136,15 @@ __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant_
     for (uint32_t r = 0; r < kItems; ++r) {
       stage.span[r * 32 + lane] = span[r];
       stage.value[r * 32 + lane] = make_uint2(value[r], base + rowExclusive[r]);
+      if constexpr (kBatch) {
+        const uint32_t i = tile * kTileSplats + warp * (32 * kItems) + r * 32 + lane;
+        uint32_t lo = 0, hi = a.viewCount;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) / 2;
+          if (__ldg(a.viewFirst + mid) <= i) lo = mid; else hi = mid;
+        }
+        stage.grid[r * 32 + lane] = make_uint2(__ldg(&a.views[lo].tileBase), __ldg(&a.views[lo].tilesX));
+      }
     }
     __syncwarp();
 #pragma unroll
@@ -149,10 +162,15 @@ __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant_
         // k / w for k < area <= 16641 and w <= 129: (k + 1/2) / w is at least 1/(2w) away from
         // an integer and the float product errs by far less, so truncation gives the quotient.
         const float rw = __frcp_rn(static_cast<float>(w));
-        const uint32_t rowStart = y0 * a.tilesX + x0;
+        uint32_t tilesX = a.tilesX, rowStart = y0 * a.tilesX + x0;
+        if constexpr (kBatch) {
+          const uint2 g = stage.grid[j];
+          tilesX = g.y;
+          rowStart = g.x + y0 * g.y + x0;
+        }
         auto emit = [&](uint32_t k, uint32_t slot) {
           const uint32_t q = static_cast<uint32_t>((static_cast<float>(k) + 0.5f) * rw);
-          const uint32_t id = rowStart + q * a.tilesX + (k - q * w);
+          const uint32_t id = rowStart + q * tilesX + (k - q * w);
           if (slot < a.instanceCapacity) {
             a.instanceKeys[slot] = id;
             a.instanceValues[slot] = val;
@@ -187,7 +205,8 @@ uint32_t binBlocks(uint32_t capacity) { return max(1u, (capacity + kTileSplats -
 cudaError_t launchBinning(const BinArgs& a, cudaStream_t stream) {
   const uint32_t grid = binBlocks(a.capacity);
   binCountKernel<<<grid, kThreads, 0, stream>>>(a);
-  binEmitKernel<<<grid, kThreads, 0, stream>>>(a);
+  if (a.viewCount > 0) binEmitKernel<true><<<grid, kThreads, 0, stream>>>(a);
+  else binEmitKernel<false><<<grid, kThreads, 0, stream>>>(a);
   return cudaGetLastError();
 }
 

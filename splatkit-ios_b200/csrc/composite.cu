@@ -128,10 +128,16 @@ __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const f
   p.done1 = p.done1 || p.T.y < cutoff;
 }
 
+// The target one tile block draws into: the context's image, or its view's part of a batch image.
+struct Target {
+  uint32_t width, height, tilesX, tile;
+  void* image;
+};
+
 template <int kFormat>
-__device__ __forceinline__ void writePixel(const CompositeArgs& a, float T, float r, float g,
-                                           float b, uint32_t col, uint32_t row) {
-  if (col >= a.width || row >= a.height) return;
+__device__ __forceinline__ void writePixel(const CompositeArgs& a, const Target& t, float T,
+                                           float r, float g, float b, uint32_t col, uint32_t row) {
+  if (col >= t.width || row >= t.height) return;
   float outR, outG, outB, outA;
   if (a.opaque) {
     outR = r + T * a.background[0];
@@ -145,37 +151,54 @@ __device__ __forceinline__ void writePixel(const CompositeArgs& a, float T, floa
   outG = fminf(fmaxf(outG, 0.0f), 1.0f);
   outB = fminf(fmaxf(outB, 0.0f), 1.0f);
   outA = fminf(fmaxf(outA, 0.0f), 1.0f);
-  const size_t at = static_cast<size_t>(row) * a.width + col;
+  const size_t at = static_cast<size_t>(row) * t.width + col;
   if constexpr (kFormat == kRgba32f) {
-    reinterpret_cast<float4*>(a.image)[at] = make_float4(outR, outG, outB, outA);
+    reinterpret_cast<float4*>(t.image)[at] = make_float4(outR, outG, outB, outA);
   } else {
     const uint32_t r8 = __float2uint_rn(outR * 255.0f), g8 = __float2uint_rn(outG * 255.0f);
     const uint32_t b8 = __float2uint_rn(outB * 255.0f), a8 = __float2uint_rn(outA * 255.0f);
-    reinterpret_cast<uint32_t*>(a.image)[at] = r8 | (g8 << 8) | (b8 << 16) | (a8 << 24);
+    reinterpret_cast<uint32_t*>(t.image)[at] = r8 | (g8 << 8) | (b8 << 16) | (a8 << 24);
   }
 }
 
-template <int kFormat>
+// kBatch: block b is batch-wide tile b; its view is the last one whose first tile is <= b.
+template <int kFormat, bool kBatch>
 __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constant__ CompositeArgs a) {
   __shared__ CompositeSmem sm;
-  const uint32_t tile = blockIdx.x;
-  const uint32_t tx = tile % a.tilesX, ty = tile / a.tilesX;
+  Target t{a.width, a.height, a.tilesX, blockIdx.x, a.image};
+  if constexpr (kBatch) {
+    uint32_t lo = 0, hi = a.viewCount;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) / 2;
+      if (__ldg(&a.views[mid].tileBase) <= blockIdx.x) lo = mid; else hi = mid;
+    }
+    const BatchView* v = a.views + lo;
+    t.width = __ldg(&v->width);
+    t.height = __ldg(&v->height);
+    t.tilesX = __ldg(&v->tilesX);
+    t.tile = blockIdx.x - __ldg(&v->tileBase);
+    t.image = static_cast<char*>(a.image) +
+              __ldg(reinterpret_cast<const unsigned long long*>(&v->pixelOffset)) *
+                  (kFormat == kRgba32f ? 16u : 4u);
+  }
+  const uint32_t tile = blockIdx.x;  // ranges are indexed batch-wide
+  const uint32_t tx = t.tile % t.tilesX, ty = t.tile / t.tilesX;
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
   const uint32_t col = tx * kTileSize + (warp & 1u) * kQuadrant + (lane % 4u) * 2u;  // and col + 1
   const uint32_t row = ty * kTileSize + (warp >> 1) * kQuadrant + lane / 4u;
-  const float height = static_cast<float>(a.height);
+  const float height = static_cast<float>(t.height);
   const float px0 = static_cast<float>(col) + 0.5f, px1 = px0 + 1.0f;
-  const float py = static_cast<float>(a.height - row) - 0.5f;  // y up, as NDC
+  const float py = static_cast<float>(t.height - row) - 0.5f;  // y up, as NDC
   const float tileX = static_cast<float>(tx * kTileSize);
   const float tileTop = height - static_cast<float>(ty * kTileSize);
-  const float halfW = 0.5f * static_cast<float>(a.width);
+  const float halfW = 0.5f * static_cast<float>(t.width);
   const float halfH = 0.5f * height;
   const uint2 range = a.ranges[tile];
   const uint32_t below = lanemaskLt();
   const float2 px = make_float2(px0, px1);
   PixelPair p;
-  p.done0 = !(col < a.width && row < a.height);
-  p.done1 = !(col + 1 < a.width && row < a.height);
+  p.done0 = !(col < t.width && row < t.height);
+  p.done1 = !(col + 1 < t.width && row < t.height);
   uint32_t blended = 0, loaded = 0;
   for (uint32_t start = range.x; start < range.y; start += kThreads) {
     const uint32_t inBatch = min(kThreads, range.y - start);
@@ -227,17 +250,22 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   if (threadIdx.x == 0 && blockFragments)
     atomicAdd(reinterpret_cast<unsigned long long*>(a.fragments), blockFragments);
   if (threadIdx.x == 0 && loaded) atomicAdd(a.loaded, loaded);
-  writePixel<kFormat>(a, p.T.x, p.r.x, p.g.x, p.b.x, col, row);
-  writePixel<kFormat>(a, p.T.y, p.r.y, p.g.y, p.b.y, col + 1, row);
+  writePixel<kFormat>(a, t, p.T.x, p.r.x, p.g.x, p.b.x, col, row);
+  writePixel<kFormat>(a, t, p.T.y, p.r.y, p.g.y, p.b.y, col + 1, row);
 }
 
 }  // namespace
 
 cudaError_t launchComposite(const CompositeArgs& a, cudaStream_t stream) {
-  const uint32_t tiles = a.tilesX * a.tilesY;
+  const uint32_t tiles = a.viewCount > 0 ? a.batchTiles : a.tilesX * a.tilesY;
   if (tiles == 0) return cudaSuccess;
-  if (a.format == kRgba32f) compositeKernel<kRgba32f><<<tiles, kThreads, 0, stream>>>(a);
-  else compositeKernel<kRgba8><<<tiles, kThreads, 0, stream>>>(a);
+  if (a.viewCount > 0) {
+    if (a.format == kRgba32f) compositeKernel<kRgba32f, true><<<tiles, kThreads, 0, stream>>>(a);
+    else compositeKernel<kRgba8, true><<<tiles, kThreads, 0, stream>>>(a);
+  } else {
+    if (a.format == kRgba32f) compositeKernel<kRgba32f, false><<<tiles, kThreads, 0, stream>>>(a);
+    else compositeKernel<kRgba8, false><<<tiles, kThreads, 0, stream>>>(a);
+  }
   return cudaGetLastError();
 }
 

@@ -257,7 +257,7 @@ cudaError_t sortResetWorkspace(const SortArgs& a, cudaStream_t stream) {
 }
 
 cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
-  const uint32_t passes = a.bits == 16 ? 2u : 4u;
+  const uint32_t passes = static_cast<uint32_t>(min(max(a.bits, 8), 32) + 7) / 8u;
   const uint32_t tiles = sortTiles(a.capacity);
   uint32_t* accum = a.histogram;
   uint32_t* bases = a.histogram + kMaxPasses * kBins;

@@ -40,6 +40,26 @@ uint32_t visibilityTileSplats();
 cudaError_t launchVisibility(const Camera* cam, const VisibilityArgs& args, int shDegree,
                              bool key16, bool indexed, cudaStream_t stream);
 
+// A batch of views (visibility.cu): one launch over every view's records, 16-bit depth keys with
+// the view id above them, survivors of all views contiguous in (view, source) order.
+struct BatchVisibilityArgs {
+  const BatchView* views;   // viewCount entries
+  const Camera* cameras;    // one per view (device)
+  uint32_t viewCount;
+  uint32_t items;           // work items: sum over views of max(1, ceil(count / 1024))
+  uint32_t* keys;
+  Projected* projected;
+  uint4* spans;
+  uint32_t* viewFirst;      // viewCount + 1 words: each view's first survivor, then the total
+  uint32_t* visibleCount;
+  uint64_t* status;         // one word per item
+  uint32_t* counters;       // two words
+  uint32_t epoch;
+  uint32_t* error;
+};
+cudaError_t launchVisibilityBatch(const BatchVisibilityArgs& args, int shDegree,
+                                  cudaStream_t stream);
+
 // ---- radix sort (radix_sort.cu) --------------------------------------------------------
 // Stable ascending sort of `count` (key, value) pairs with 8-bit digits: one histogram pass,
 // then one onesweep scatter pass per digit. valuesIn null: values are the key positions.
@@ -51,7 +71,7 @@ struct SortArgs {
   uint32_t* valuesOut;
   const uint32_t* count;  // device
   uint32_t capacity;      // count is clamped to this
-  int bits;               // 16 or 32
+  int bits;               // key bits: 8, 16, 24 or 32 (one 8-bit digit pass each)
   // workspace (sortWorkspaceBytes)
   uint32_t* keysA;
   uint32_t* keysB;
@@ -83,6 +103,10 @@ struct BinArgs {
   uint32_t* instanceCount;  // FrameCounters.instances
   uint32_t* overflow;       // FrameCounters.overflow
   uint32_t* blockSums;      // binBlocks(capacity) words of scratch
+  // a batch (viewCount > 0): tile ids are batch-wide, each view's from its table entry
+  const BatchView* views;
+  const uint32_t* viewFirst;  // viewCount + 1 words (BatchVisibilityArgs)
+  uint32_t viewCount;
 };
 uint32_t binBlocks(uint32_t capacity);
 cudaError_t launchBinning(const BinArgs& args, cudaStream_t stream);
@@ -107,6 +131,10 @@ struct CompositeArgs {
   int format;
   uint32_t* fragments;  // FrameCounters.fragments_lo/hi (64-bit add)
   uint32_t* loaded;     // FrameCounters.loaded
+  // a batch (viewCount > 0): one block per batch-wide tile, image = the batch image
+  const BatchView* views;
+  uint32_t viewCount;
+  uint32_t batchTiles;
 };
 cudaError_t launchComposite(const CompositeArgs& args, cudaStream_t stream);
 

@@ -109,4 +109,22 @@ inline constexpr uint32_t shDeviceStride(int degree) {
 
 constexpr uint32_t kTileSize = 16;  // composite tile edge in pixels
 
+// One view of a batch (device table, 64 bytes): the world range it draws, where its work items,
+// tiles and pixels start in the batch-wide arrays, and its target size. Views are listed in
+// submission order; itemStart, tileBase and pixelOffset grow with the view index.
+struct alignas(16) BatchView {
+  const GpuSplat* splats;
+  const uint32_t* sh;
+  uint32_t shStride;     // harmonics words per record of this world
+  uint32_t offset;       // first record drawn
+  uint32_t count;        // records drawn
+  uint32_t itemStart;    // first visibility work item (1024-record chunk) of this view
+  uint32_t tileBase;     // first batch-wide tile id of this view
+  uint32_t tilesX, tilesY;
+  uint32_t width, height;
+  uint32_t pad;
+  uint64_t pixelOffset;  // first pixel of this view in the batch image
+};
+static_assert(sizeof(BatchView) == 64, "BatchView is 64 bytes");
+
 }  // namespace sk

@@ -256,6 +256,115 @@ struct VisibilitySmem {
   uint32_t tileBase, tileCount;
 };
 
+// Projects one 1024-record tile into shared memory: survivors' keys and records at their
+// source slot, and per warp row the mask of survivors. indexOf(t) gives the record index of
+// tile position t, or 0xffffffff past the end. keyHigh is or-ed into every key (the view id of a
+// batch, above a 16-bit key). One record per row of the warp, not unrolled (the projection is
+// large); the next row's record is fetched while this one is projected.
+template <int D, bool kKey16, typename IndexOf>
+__device__ __forceinline__ void projectTile(VisibilitySmem& s, const Camera& cam,
+                                            const GpuSplat* __restrict__ splats,
+                                            const uint32_t* __restrict__ sh, uint32_t shStride,
+                                            uint32_t first, uint32_t keyHigh, IndexOf indexOf) {
+  const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+  uint32_t index = indexOf(first);
+  uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
+  if (index != 0xffffffffu) {
+    const uint4* p = reinterpret_cast<const uint4*>(splats + index);
+    lo = __ldg(p), hi = __ldg(p + 1);
+  }
+#pragma unroll 1
+  for (uint32_t r = 0; r < kItems; ++r) {
+    uint32_t nextIndex = 0xffffffffu;
+    uint4 nextLo = make_uint4(0, 0, 0, 0), nextHi = nextLo;
+    if (r + 1 < kItems) {
+      nextIndex = indexOf(first + (r + 1) * 32);
+      if (nextIndex != 0xffffffffu) {
+        const uint4* p = reinterpret_cast<const uint4*>(splats + nextIndex);
+        nextLo = __ldg(p), nextHi = __ldg(p + 1);
+      }
+    }
+    bool visible = false;
+    const uint32_t slot = warp * (32 * kItems) + r * 32 + lane;
+    if (index != 0xffffffffu) {
+      uint32_t key, rec[8];
+      visible = projectSplat<D, kKey16>(cam, lo, hi, index, sh, shStride, key, rec);
+      if (visible) {
+        s.key[slot] = key | keyHigh;
+        s.rec[2 * slot] = make_uint4(rec[0], rec[1], rec[2], rec[3]);
+        s.rec[2 * slot + 1] = make_uint4(rec[4], rec[5], rec[6], rec[7]);
+      }
+    }
+    const uint32_t mask = __ballot_sync(0xffffffffu, visible);
+    if (lane == 0) s.rowMask[warp][r] = mask;
+    index = nextIndex, lo = nextLo, hi = nextHi;
+  }
+  __syncwarp();
+}
+
+// Order-preserving compaction of the tile's survivors: warp totals, the tile's offset by
+// decoupled look-back over status[0 .. tile], then survivor k of the tile -> its source slot.
+// Leaves the offset and count in s.tileBase / s.tileCount.
+__device__ __forceinline__ void compactTile(VisibilitySmem& s, uint64_t* status, uint32_t tile,
+                                            uint32_t epoch, uint32_t* error) {
+  const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+  uint32_t warpTotal = 0;
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r) warpTotal += __popc(s.rowMask[warp][r]);
+  if (lane == 0) s.warpBase[warp] = warpTotal;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t mine = lane < kThreads / 32 ? s.warpBase[lane] : 0u;
+    uint32_t inclusive = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t up = __shfl_up_sync(0xffffffffu, inclusive, o);
+      if (lane >= static_cast<uint32_t>(o)) inclusive += up;
+    }
+    const uint32_t aggregate = __shfl_sync(0xffffffffu, inclusive, 31);
+    if (lane < kThreads / 32) s.warpBase[lane] = inclusive - mine;
+    uint32_t exclusive = 0;
+    if (tile == 0) {
+      if (lane == 0) storeStatus(status, makeStatus(epoch, kFlagPrefix, aggregate));
+    } else {
+      if (lane == 0) storeStatus(status + tile, makeStatus(epoch, kFlagAggregate, aggregate));
+      exclusive = warpLookback(status, tile, epoch, error);
+      if (lane == 0) storeStatus(status + tile, makeStatus(epoch, kFlagPrefix, exclusive + aggregate));
+    }
+    if (lane == 0) {
+      s.tileBase = exclusive;
+      s.tileCount = aggregate;
+    }
+  }
+  __syncthreads();
+  uint32_t pos = s.warpBase[warp];
+  const uint32_t below = lanemaskLt();
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r) {
+    const uint32_t mask = s.rowMask[warp][r];
+    if (mask & (1u << lane)) s.slotOf[pos + __popc(mask & below)] = warp * (32 * kItems) + r * 32 + lane;
+    pos += __popc(mask);
+  }
+  __syncthreads();
+}
+
+// Coalesced copy-out: consecutive threads write consecutive survivors, with the tiles each
+// survivor's quad touches on a width x height target.
+__device__ __forceinline__ void copyOutTile(const VisibilitySmem& s, uint32_t* keys,
+                                            Projected* projected, uint4* spans, float width,
+                                            float height, uint32_t tilesX, uint32_t tilesY) {
+  const uint32_t count = s.tileCount, base = s.tileBase;
+  for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
+    const uint32_t slot = s.slotOf[k];
+    keys[base + k] = s.key[slot];
+    const uint4 lo = s.rec[2 * slot], hi = s.rec[2 * slot + 1];
+    uint4* o = reinterpret_cast<uint4*>(projected + base + k);
+    o[0] = lo;
+    o[1] = hi;
+    spans[base + k] = tileSpan(lo, hi, width, height, tilesX, tilesY);
+  }
+}
+
 template <int D, bool kKey16, bool kIndexed>
 __global__ void __launch_bounds__(kThreads)
     visibilityKernel(const Camera* __restrict__ camera, const __grid_constant__ VisibilityArgs a) {
@@ -268,8 +377,6 @@ __global__ void __launch_bounds__(kThreads)
   if (tile < tiles) {
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
     const uint32_t first = tile * kTileSplats + warp * (32 * kItems) + lane;
-    // One splat per row of the warp, not unrolled (the projection is large); the next row's
-    // record is fetched while this one is projected.
     auto indexOf = [&](uint32_t t) -> uint32_t {
       if (t >= total) return 0xffffffffu;
       const uint32_t index = kIndexed ? a.indices[t] : sourceIndex(a, t);
@@ -279,96 +386,64 @@ __global__ void __launch_bounds__(kThreads)
       }
       return index;
     };
-    uint32_t index = indexOf(first);
-    uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
-    if (index != 0xffffffffu) {
-      const uint4* p = reinterpret_cast<const uint4*>(a.splats + index);
-      lo = __ldg(p), hi = __ldg(p + 1);
-    }
-#pragma unroll 1
-    for (uint32_t r = 0; r < kItems; ++r) {
-      uint32_t nextIndex = 0xffffffffu;
-      uint4 nextLo = make_uint4(0, 0, 0, 0), nextHi = nextLo;
-      if (r + 1 < kItems) {
-        nextIndex = indexOf(first + (r + 1) * 32);
-        if (nextIndex != 0xffffffffu) {
-          const uint4* p = reinterpret_cast<const uint4*>(a.splats + nextIndex);
-          nextLo = __ldg(p), nextHi = __ldg(p + 1);
-        }
-      }
-      bool visible = false;
-      const uint32_t slot = warp * (32 * kItems) + r * 32 + lane;
-      if (index != 0xffffffffu) {
-        uint32_t key, rec[8];
-        visible = projectSplat<D, kKey16>(cam, lo, hi, index, a.sh, a.shStride, key, rec);
-        if (visible) {
-          s.key[slot] = key;
-          s.rec[2 * slot] = make_uint4(rec[0], rec[1], rec[2], rec[3]);
-          s.rec[2 * slot + 1] = make_uint4(rec[4], rec[5], rec[6], rec[7]);
-        }
-      }
-      const uint32_t mask = __ballot_sync(0xffffffffu, visible);
-      if (lane == 0) s.rowMask[warp][r] = mask;
-      index = nextIndex, lo = nextLo, hi = nextHi;
-    }
-    __syncwarp();
-    uint32_t warpTotal = 0;
-#pragma unroll
-    for (uint32_t r = 0; r < kItems; ++r) warpTotal += __popc(s.rowMask[warp][r]);
-    if (lane == 0) s.warpBase[warp] = warpTotal;
-    __syncthreads();
-    if (warp == 0) {
-      const uint32_t mine = lane < kThreads / 32 ? s.warpBase[lane] : 0u;
-      uint32_t inclusive = mine;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t up = __shfl_up_sync(0xffffffffu, inclusive, o);
-        if (lane >= static_cast<uint32_t>(o)) inclusive += up;
-      }
-      const uint32_t aggregate = __shfl_sync(0xffffffffu, inclusive, 31);
-      if (lane < kThreads / 32) s.warpBase[lane] = inclusive - mine;
-      uint32_t exclusive = 0;
-      if (tile == 0) {
-        if (lane == 0) storeStatus(a.status, makeStatus(a.epoch, kFlagPrefix, aggregate));
-      } else {
-        if (lane == 0) storeStatus(a.status + tile, makeStatus(a.epoch, kFlagAggregate, aggregate));
-        exclusive = warpLookback(a.status, tile, a.epoch, a.error);
-        if (lane == 0)
-          storeStatus(a.status + tile, makeStatus(a.epoch, kFlagPrefix, exclusive + aggregate));
-      }
-      if (lane == 0) {
-        s.tileBase = exclusive;
-        s.tileCount = aggregate;
-        if (tile == tiles - 1) *a.visibleCount = exclusive + aggregate;
-      }
-    }
-    __syncthreads();
-    // survivor k of the tile <- its source slot, in source order
-    {
-      uint32_t pos = s.warpBase[warp];
-      const uint32_t below = lanemaskLt();
-#pragma unroll
-      for (uint32_t r = 0; r < kItems; ++r) {
-        const uint32_t mask = s.rowMask[warp][r];
-        if (mask & (1u << lane)) s.slotOf[pos + __popc(mask & below)] = warp * (32 * kItems) + r * 32 + lane;
-        pos += __popc(mask);
-      }
-    }
-    __syncthreads();
-    // coalesced copy-out: consecutive threads write consecutive survivors, with the tiles
-    // each survivor's quad touches
-    const uint32_t count = s.tileCount, base = s.tileBase;
-    for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
-      const uint32_t slot = s.slotOf[k];
-      a.keys[base + k] = s.key[slot];
-      const uint4 lo = s.rec[2 * slot], hi = s.rec[2 * slot + 1];
-      uint4* o = reinterpret_cast<uint4*>(a.projected + base + k);
-      o[0] = lo;
-      o[1] = hi;
-      a.spans[base + k] = tileSpan(lo, hi, cam.screenSize[0], cam.screenSize[1], a.tilesX, a.tilesY);
-    }
+    projectTile<D, kKey16>(s, cam, a.splats, a.sh, a.shStride, first, 0u, indexOf);
+    compactTile(s, a.status, tile, a.epoch, a.error);
+    if (tile == tiles - 1 && threadIdx.x == 0) *a.visibleCount = s.tileBase + s.tileCount;
+    copyOutTile(s, a.keys, a.projected, a.spans, cam.screenSize[0], cam.screenSize[1], a.tilesX,
+                a.tilesY);
   }
   if (tiles == 0 && tile == 0 && threadIdx.x == 0) *a.visibleCount = 0;
+  finishTile(a.counters);
+}
+
+// A batch of views in one launch. Work item i is a 1024-record chunk of one view's range;
+// items are numbered view by view, so one look-back chain over all items places every view's
+// survivors contiguously, in (view, source) order, and the first item of each view records
+// where that view starts. Keys carry the view id above the 16-bit depth key, so one stable
+// sort orders all views at once.
+template <int D>
+__global__ void __launch_bounds__(kThreads)
+    visibilityBatchKernel(const __grid_constant__ BatchVisibilityArgs a) {
+  __shared__ VisibilitySmem s;
+  __shared__ Camera cam;
+  __shared__ uint32_t viewOf;
+  __shared__ BatchView view;
+  const uint32_t item = takeTile(a.counters);
+  if (item < a.items) {
+    if (threadIdx.x == 0) {
+      // the last view whose first item is <= item
+      uint32_t lo = 0, hi = a.viewCount;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (__ldg(&a.views[mid].itemStart) <= item) lo = mid; else hi = mid;
+      }
+      viewOf = lo;
+    }
+    __syncthreads();
+    const uint32_t v = viewOf;
+    loadCamera(a.cameras + v, &cam);
+    if (threadIdx.x < sizeof(BatchView) / 4)
+      reinterpret_cast<uint32_t*>(&view)[threadIdx.x] =
+          __ldg(reinterpret_cast<const uint32_t*>(a.views + v) + threadIdx.x);
+    __syncthreads();
+    const uint32_t chunk = item - view.itemStart;
+    const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+    const uint32_t first = chunk * kTileSplats + warp * (32 * kItems) + lane;
+    auto indexOf = [&](uint32_t t) -> uint32_t {
+      return t < view.count ? view.offset + t : 0xffffffffu;
+    };
+    projectTile<D, true>(s, cam, view.splats, view.sh, view.shStride, first, v << 16, indexOf);
+    compactTile(s, a.status, item, a.epoch, a.error);
+    if (threadIdx.x == 0) {
+      if (chunk == 0) a.viewFirst[v] = s.tileBase;
+      if (item == a.items - 1) {
+        a.viewFirst[a.viewCount] = s.tileBase + s.tileCount;
+        *a.visibleCount = s.tileBase + s.tileCount;
+      }
+    }
+    copyOutTile(s, a.keys, a.projected, a.spans, static_cast<float>(view.width),
+                static_cast<float>(view.height), view.tilesX, view.tilesY);
+  }
   finishTile(a.counters);
 }
 
@@ -393,6 +468,18 @@ void launchDegree(const Camera* cam, const VisibilityArgs& a, bool key16, bool i
 }  // namespace
 
 uint32_t visibilityTileSplats() { return kTileSplats; }
+
+cudaError_t launchVisibilityBatch(const BatchVisibilityArgs& args, int shDegree,
+                                  cudaStream_t stream) {
+  if (args.items == 0 || args.viewCount == 0) return cudaSuccess;
+  switch (shDegree) {
+    case 0: visibilityBatchKernel<0><<<args.items, kThreads, 0, stream>>>(args); break;
+    case 1: visibilityBatchKernel<1><<<args.items, kThreads, 0, stream>>>(args); break;
+    case 2: visibilityBatchKernel<2><<<args.items, kThreads, 0, stream>>>(args); break;
+    default: visibilityBatchKernel<3><<<args.items, kThreads, 0, stream>>>(args); break;
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t launchVisibility(const Camera* cam, const VisibilityArgs& args, int shDegree,
                              bool key16, bool indexed, cudaStream_t stream) {

@@ -1,0 +1,549 @@
+// Batched multi-view rendering behind the sk_batch_* calls of include/splatkit_b200.h.
+//
+// One submission = a view table (world range, target size, where its items, tiles and pixels
+// start in the batch-wide arrays) plus one camera per view. The stages are the frame
+// pipeline's, each launched once over the whole batch:
+//   visibility (all views, one look-back chain: survivors contiguous in (view, source) order,
+//   key = view << 16 | 16-bit depth key) -> one stable radix sort of those keys (every view's
+//   depth order, views back to back) -> binning with batch-wide tile ids -> stable tile sort ->
+//   tile ranges -> composite of every tile of every view -> images, survivor counts and
+//   counters copied to pinned memory.
+// The arithmetic per view is the plain frame's, so the images and counts equal sk_draw's.
+#include "batch.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+namespace sk {
+
+BatchLane::~BatchLane() {
+  if (graph) cudaGraphExecDestroy(graph);
+  if (done) cudaEventDestroy(done);
+  if (start) cudaEventDestroy(start);
+  if (end) cudaEventDestroy(end);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+sk_status Batch::fail(sk_status code, const std::string& message) {
+  error = message;
+  return code;
+}
+
+sk_status Batch::check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SK_OK;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return fail(SK_E_OOM, std::string(what) + ": out of device memory");
+  }
+  failed = true;
+  return fail(SK_E_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+uint32_t Batch::nextEpoch(uint32_t n) {
+  const uint32_t e = epoch;
+  epoch += n;
+  if (epoch >= 0x3fff0000u) epoch = 1;
+  return e;
+}
+
+namespace {
+uint32_t bitsFor(uint64_t values) {  // key bits, a multiple of 8, for keys < values
+  uint32_t b = 8;
+  while (b < 32 && (uint64_t{1} << b) < values) b += 8;
+  return b;
+}
+}  // namespace
+
+sk_status Batch::reserve(BatchLane& l, uint32_t sources, uint32_t instances, uint32_t items,
+                         uint32_t tiles, uint32_t views, uint64_t pixels) {
+  sources = std::max(sources, 1u);
+  instances = std::max(instances, 1u);
+  cudaError_t e = cudaSuccess;
+  auto grab = [&](DeviceBuffer& b, size_t n) {
+    if (e == cudaSuccess) e = b.allocate(n);
+  };
+  auto pin = [&](PinnedBuffer& b, size_t n) {
+    if (e == cudaSuccess) e = b.allocate(n);
+  };
+  const bool grewSources = sources > l.sources, grewInstances = instances > l.instances;
+  const bool grewItems = items > l.items;
+  grab(l.keys, size_t{sources} * 4);
+  grab(l.projected, size_t{sources} * sizeof(Projected));
+  grab(l.spans, size_t{sources} * 16);
+  grab(l.order, size_t{sources} * 4);
+  grab(l.sortWorkspace, sortWorkspaceBytes(sources));
+  grab(l.binSums, size_t{binBlocks(sources)} * 4);
+  grab(l.visStatus, size_t{std::max(items, 1u)} * 8);
+  grab(l.instKeys, size_t{instances} * 4);
+  grab(l.instValues, size_t{instances} * 4);
+  grab(l.instKeysSorted, size_t{instances} * 4);
+  grab(l.instValuesSorted, size_t{instances} * 4);
+  grab(l.tileSortWorkspace, sortWorkspaceBytes(instances));
+  grab(l.ranges, size_t{std::max(tiles, 1u)} * sizeof(uint2));
+  grab(l.viewFirst, size_t{views + 1} * 4);
+  grab(l.viewTable, size_t{views} * sizeof(BatchView));
+  grab(l.cameras, size_t{views} * sizeof(Camera));
+  grab(l.image, pixels * 4);
+  const bool freshCounters = l.counters.ptr == nullptr;
+  grab(l.counters, 64 * 4);
+  grab(l.frameCounters, sizeof(FrameCounters));
+  pin(l.hostViews, size_t{views} * sizeof(BatchView));
+  pin(l.hostCameras, size_t{views} * sizeof(Camera));
+  pin(l.hostCounters, sizeof(FrameCounters));
+  pin(l.hostViewFirst, size_t{views + 1} * 4);
+  pin(l.hostImage, pixels * 4);
+  if (e == cudaSuccess && freshCounters) e = cudaMemsetAsync(l.counters.ptr, 0, 64 * 4, l.stream);
+  // fresh sort workspaces: counters and histogram accumulators start at zero
+  if (e == cudaSuccess && grewSources)
+    e = cudaMemsetAsync(l.sortWorkspace.ptr, 0, l.sortWorkspace.bytes, l.stream);
+  if (e == cudaSuccess && grewInstances)
+    e = cudaMemsetAsync(l.tileSortWorkspace.ptr, 0, l.tileSortWorkspace.bytes, l.stream);
+  // look-back status words of a fresh buffer must read "not ready"
+  if (e == cudaSuccess && grewItems) e = cudaMemsetAsync(l.visStatus.ptr, 0, l.visStatus.bytes, l.stream);
+  if (e != cudaSuccess) return check(e, "batch buffers");
+  if (grewSources || grewInstances || items > l.items || tiles > l.tiles || views > l.views ||
+      pixels > l.pixels) {
+    // buffers moved: a captured graph points at the old ones
+    if (l.graph) cudaGraphExecDestroy(l.graph);
+    l.graph = nullptr;
+    l.graphShape.clear();
+  }
+  l.sources = std::max(l.sources, sources);
+  l.instances = std::max(l.instances, instances);
+  l.items = std::max(l.items, items);
+  l.tiles = std::max(l.tiles, tiles);
+  l.views = std::max(l.views, views);
+  l.pixels = std::max(l.pixels, pixels);
+  return SK_OK;
+}
+
+sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t count) {
+  l.table.resize(count);
+  l.cams.resize(count);
+  l.worlds.resize(count);
+  uint32_t items = 0, tiles = 0, degree = 0;
+  uint64_t pixels = 0, sources = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const sk_batch_view& v = views[i];
+    auto* ctx = reinterpret_cast<Context*>(v.world);
+    if (!ctx || ctx->device != device) return fail(SK_E_INVALID, "a view has no context on this device");
+    const World& w = ctx->world;
+    if (!w.splats.ptr || w.lod) return fail(SK_E_INVALID, "a view's context holds no flat world");
+    if (v.width == 0 || v.height == 0 || v.width > 16384 || v.height > 16384)
+      return fail(SK_E_INVALID, "view size out of range");
+    uint32_t offset = 0, n = w.count;
+    if (v.frame.range_count > 1) return fail(SK_E_INVALID, "a batch view draws at most one range");
+    if (v.frame.range_count == 1) {
+      if (!v.frame.ranges) return fail(SK_E_INVALID, "range missing");
+      offset = v.frame.ranges[0].offset;
+      n = v.frame.ranges[0].count;
+      if (offset > w.count || n > w.count - offset) return fail(SK_E_INVALID, "invalid range");
+    }
+    const uint32_t d = static_cast<uint32_t>(std::max(0, std::min(v.frame.sh_degree, w.shDegree)));
+    if (i == 0) degree = d;
+    if (d != degree) return fail(SK_E_INVALID, "views of one batch draw one harmonics degree");
+    BatchView& t = l.table[i];
+    t = BatchView{};
+    t.splats = static_cast<const GpuSplat*>(w.splats.ptr);
+    t.sh = static_cast<const uint32_t*>(w.sh.ptr);
+    t.shStride = shDeviceStride(w.shDegree);
+    t.offset = offset;
+    t.count = n;
+    t.itemStart = items;
+    t.tileBase = tiles;
+    t.width = v.width;
+    t.height = v.height;
+    t.tilesX = (v.width + kTileSize - 1) / kTileSize;
+    t.tilesY = (v.height + kTileSize - 1) / kTileSize;
+    t.pixelOffset = pixels;
+    const uint64_t chunks = std::max<uint64_t>(1, (uint64_t{n} + visibilityTileSplats() - 1) /
+                                                      visibilityTileSplats());
+    if (uint64_t{items} + chunks > 0x7fffffffu || uint64_t{tiles} + t.tilesX * t.tilesY > 0xffffffffu ||
+        sources + n > 0x7fffffffu)
+      return fail(SK_E_INVALID, "batch too large");
+    items += static_cast<uint32_t>(chunks);
+    tiles += t.tilesX * t.tilesY;
+    pixels += uint64_t{v.width} * v.height;
+    sources += n;
+    l.cams[i] = cameraOf(v.frame, v.width, v.height, policy.subpixel_threshold);
+    l.worlds[i] = w.splats.ptr;
+  }
+  l.viewCount = count;
+  l.totalItems = items;
+  l.totalTiles = tiles;
+  l.totalPixels = pixels;
+  l.shDegree = degree;
+  const uint32_t guess = static_cast<uint32_t>(std::min<uint64_t>(
+      std::max<uint64_t>(l.instances, sources * 4), 0x7fffffffu));
+  sk_status st = reserve(l, static_cast<uint32_t>(sources), guess, items, tiles, count, pixels);
+  if (st != SK_OK) return st;
+  std::memcpy(l.hostViews.ptr, l.table.data(), size_t{count} * sizeof(BatchView));
+  std::memcpy(l.hostCameras.ptr, l.cams.data(), size_t{count} * sizeof(Camera));
+  return SK_OK;
+}
+
+// The stages of one submission on the lane's stream. clearStatus: zero the look-back status
+// words first (a replayed graph reuses the epochs it was captured with).
+sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
+  const cudaStream_t s = l.stream;
+  FrameCounters* fc = static_cast<FrameCounters*>(l.frameCounters.ptr);
+  uint32_t* error = &fc->error;
+  uint32_t* counters = static_cast<uint32_t*>(l.counters.ptr);
+  const auto* views = static_cast<const BatchView*>(l.viewTable.ptr);
+  const auto* viewFirst = static_cast<const uint32_t*>(l.viewFirst.ptr);
+  cudaError_t e = cudaMemsetAsync(fc, 0, sizeof(FrameCounters), s);
+  if (e == cudaSuccess && clearStatus) {
+    e = cudaMemsetAsync(l.visStatus.ptr, 0, size_t{l.totalItems} * 8, s);
+    SortArgs probe{};
+    sortBindWorkspace(probe, l.sortWorkspace.ptr, l.sources);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(probe.status, 0, sortWorkspaceBytes(l.sources) -
+                          (reinterpret_cast<char*>(probe.status) - static_cast<char*>(l.sortWorkspace.ptr)), s);
+    sortBindWorkspace(probe, l.tileSortWorkspace.ptr, l.instances);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(probe.status, 0, sortWorkspaceBytes(l.instances) -
+                          (reinterpret_cast<char*>(probe.status) - static_cast<char*>(l.tileSortWorkspace.ptr)), s);
+  }
+  if (e == cudaSuccess) {
+    BatchVisibilityArgs v{};
+    v.views = views;
+    v.cameras = static_cast<const Camera*>(l.cameras.ptr);
+    v.viewCount = l.viewCount;
+    v.items = l.totalItems;
+    v.keys = static_cast<uint32_t*>(l.keys.ptr);
+    v.projected = static_cast<Projected*>(l.projected.ptr);
+    v.spans = static_cast<uint4*>(l.spans.ptr);
+    v.viewFirst = static_cast<uint32_t*>(l.viewFirst.ptr);
+    v.visibleCount = &fc->visible;
+    v.status = static_cast<uint64_t*>(l.visStatus.ptr);
+    v.counters = counters + 0;
+    v.epoch = nextEpoch(1);
+    v.error = error;
+    e = launchVisibilityBatch(v, static_cast<int>(l.shDegree), s);
+  }
+  if (e == cudaSuccess) {
+    // depth order of every view at once: the view id sits above the 16-bit key
+    SortArgs a{};
+    a.keysIn = static_cast<const uint32_t*>(l.keys.ptr);
+    a.valuesOut = static_cast<uint32_t*>(l.order.ptr);
+    a.count = &fc->visible;
+    a.capacity = l.sources;
+    a.bits = static_cast<int>(bitsFor(uint64_t{l.viewCount} << 16));
+    sortBindWorkspace(a, l.sortWorkspace.ptr, l.sources);
+    a.epoch = nextEpoch(4);
+    a.error = error;
+    e = launchSort(a, s);
+  }
+  if (e == cudaSuccess) {
+    BinArgs b{};
+    b.spans = static_cast<const uint4*>(l.spans.ptr);
+    b.order = static_cast<const uint32_t*>(l.order.ptr);
+    b.count = &fc->visible;
+    b.capacity = l.sources;
+    b.instanceKeys = static_cast<uint32_t*>(l.instKeys.ptr);
+    b.instanceValues = static_cast<uint32_t*>(l.instValues.ptr);
+    b.instanceCapacity = l.instances;
+    b.instanceCount = &fc->instances;
+    b.overflow = &fc->overflow;
+    b.blockSums = static_cast<uint32_t*>(l.binSums.ptr);
+    b.views = views;
+    b.viewFirst = viewFirst;
+    b.viewCount = l.viewCount;
+    e = launchBinning(b, s);
+  }
+  if (e == cudaSuccess) {
+    SortArgs a{};
+    a.keysIn = static_cast<const uint32_t*>(l.instKeys.ptr);
+    a.valuesIn = static_cast<const uint32_t*>(l.instValues.ptr);
+    a.keysOut = static_cast<uint32_t*>(l.instKeysSorted.ptr);
+    a.valuesOut = static_cast<uint32_t*>(l.instValuesSorted.ptr);
+    a.count = &fc->instances;
+    a.capacity = l.instances;
+    a.bits = static_cast<int>(bitsFor(l.totalTiles));
+    sortBindWorkspace(a, l.tileSortWorkspace.ptr, l.instances);
+    a.epoch = nextEpoch(4);
+    a.error = error;
+    e = launchSort(a, s);
+  }
+  if (e == cudaSuccess)
+    e = launchTileRanges(static_cast<const uint32_t*>(l.instKeysSorted.ptr), &fc->instances,
+                         l.instances, static_cast<uint2*>(l.ranges.ptr), l.totalTiles, s);
+  if (e == cudaSuccess) {
+    CompositeArgs c{};
+    c.projected = static_cast<const Projected*>(l.projected.ptr);
+    c.values = static_cast<const uint32_t*>(l.instValuesSorted.ptr);
+    c.ranges = static_cast<const uint2*>(l.ranges.ptr);
+    for (int j = 0; j < 3; ++j) c.background[j] = static_cast<float>(policy.background[j]);
+    c.opaque = 1;
+    c.cutoff = policy.enable_early_termination ? kTransmittanceCutoff : 0.0f;
+    c.image = l.image.ptr;
+    c.format = kRgba8;
+    c.fragments = &fc->fragments_lo;
+    c.loaded = &fc->loaded;
+    c.views = views;
+    c.viewCount = l.viewCount;
+    c.batchTiles = l.totalTiles;
+    e = launchComposite(c, s);
+  }
+  return check(e, "batch stages");
+}
+
+sk_status Batch::enqueue(BatchLane& l) {
+  const cudaStream_t s = l.stream;
+  // the shape a captured graph is valid for: every view's world, range and size
+  std::vector<uint64_t> shape;
+  if (tuning.graphs) {
+    shape.reserve(size_t{l.viewCount} * 4 + 2);
+    shape.push_back(l.viewCount);
+    shape.push_back(l.shDegree);
+    for (uint32_t i = 0; i < l.viewCount; ++i) {
+      const BatchView& t = l.table[i];
+      shape.push_back(reinterpret_cast<uint64_t>(t.splats));
+      shape.push_back((uint64_t{t.offset} << 32) | t.count);
+      shape.push_back((uint64_t{t.width} << 32) | t.height);
+      shape.push_back(t.shStride);
+    }
+  }
+  cudaError_t e = cudaEventRecord(l.start, s);
+  auto body = [&](bool clearStatus) -> sk_status {
+    cudaError_t r = cudaMemcpyAsync(l.viewTable.ptr, l.hostViews.ptr,
+                                    size_t{l.viewCount} * sizeof(BatchView), cudaMemcpyHostToDevice, s);
+    if (r == cudaSuccess)
+      r = cudaMemcpyAsync(l.cameras.ptr, l.hostCameras.ptr, size_t{l.viewCount} * sizeof(Camera),
+                          cudaMemcpyHostToDevice, s);
+    if (r != cudaSuccess) return check(r, "batch upload");
+    sk_status st = enqueueStages(l, clearStatus);
+    if (st != SK_OK) return st;
+    r = cudaMemcpyAsync(l.hostCounters.ptr, l.frameCounters.ptr, sizeof(FrameCounters),
+                        cudaMemcpyDeviceToHost, s);
+    if (r == cudaSuccess)
+      r = cudaMemcpyAsync(l.hostViewFirst.ptr, l.viewFirst.ptr, size_t{l.viewCount + 1} * 4,
+                          cudaMemcpyDeviceToHost, s);
+    if (r == cudaSuccess)
+      r = cudaMemcpyAsync(l.hostImage.ptr, l.image.ptr, l.totalPixels * 4, cudaMemcpyDeviceToHost, s);
+    return check(r, "batch readback");
+  };
+  sk_status st = SK_OK;
+  if (e != cudaSuccess) return check(e, "batch");
+  if (tuning.graphs) {
+    if (!l.graph || l.graphShape != shape) {
+      if (l.graph) cudaGraphExecDestroy(l.graph);
+      l.graph = nullptr;
+      cudaGraph_t g = nullptr;
+      e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return check(e, "graph capture");
+      st = body(true);
+      const cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (st != SK_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+      }
+      if (ce != cudaSuccess) return check(ce, "graph capture");
+      e = cudaGraphInstantiate(&l.graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        l.graph = nullptr;
+        return check(e, "graph instantiate");
+      }
+      l.graphShape = shape;
+    }
+    e = cudaGraphLaunch(l.graph, s);
+    if (e != cudaSuccess) return check(e, "graph launch");
+  } else {
+    st = body(false);
+    if (st != SK_OK) return st;
+  }
+  e = cudaEventRecord(l.end, s);
+  if (e == cudaSuccess) e = cudaEventRecord(l.done, s);
+  return check(e, "batch");
+}
+
+sk_status Batch::finish(BatchLane& l, bool wait) {
+  if (!l.busy || l.harvested) return l.status;
+  if (wait) {
+    const cudaError_t e = cudaEventSynchronize(l.done);
+    if (e != cudaSuccess) return l.status = check(e, "batch wait");
+  } else if (cudaEventQuery(l.done) != cudaSuccess) {
+    cudaGetLastError();  // cudaErrorNotReady is not an error
+    return SK_OK;
+  }
+  FrameCounters c = *static_cast<const FrameCounters*>(l.hostCounters.ptr);
+  if (c.overflow) {
+    // Grow the instance buffers to what the batch needed and draw it again.
+    const uint32_t need = static_cast<uint32_t>(std::min<uint64_t>(
+        uint64_t{c.instances} + c.instances / 4 + 1024, 0x7fffffffu));
+    sk_status st = reserve(l, l.sources, need, l.items, l.tiles, l.views, l.pixels);
+    if (st == SK_OK) st = enqueue(l);
+    if (st != SK_OK) {
+      l.harvested = true;
+      return l.status = st;
+    }
+    return finish(l, true);
+  }
+  l.result = c;
+  l.harvested = true;
+  cudaEventElapsedTime(&l.gpuMs, l.start, l.end);
+  l.status = c.error ? fail(SK_E_TIMEOUT, "a bounded device wait or bounds check failed in the batch")
+                     : SK_OK;
+  return l.status;
+}
+
+BatchLane* Batch::laneOf(uint64_t ticket) {
+  for (auto& l : lanes)
+    if (l.busy && l.ticket == ticket) return &l;
+  return nullptr;
+}
+
+}  // namespace sk
+
+using sk::Batch;
+using sk::BatchLane;
+
+extern "C" {
+
+sk_status sk_batch_create(const sk_batch_config* config, sk_batch** out) {
+  if (!config || !out) return SK_E_INVALID;
+  *out = nullptr;
+  if (config->lanes == 0 || config->lanes > 16 || config->max_views == 0 || config->max_views > 65536)
+    return SK_E_INVALID;
+  int devices = 0;
+  if (cudaGetDeviceCount(&devices) != cudaSuccess || config->device < 0 || config->device >= devices) {
+    cudaGetLastError();
+    return SK_E_DEVICE;
+  }
+  if (cudaSetDevice(config->device) != cudaSuccess) return SK_E_DEVICE;
+  auto b = std::make_unique<Batch>();
+  b->device = config->device;
+  b->tuning.lanes = config->lanes;
+  b->tuning.maxViews = config->max_views;
+  b->tuning.graphs = config->use_graphs != 0;
+  sk_default_policy(&b->policy);
+  b->lanes = std::vector<BatchLane>(config->lanes);
+  for (auto& l : b->lanes) {
+    if (cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&l.start) != cudaSuccess || cudaEventCreate(&l.end) != cudaSuccess)
+      return SK_E_DEVICE;
+  }
+  *out = reinterpret_cast<sk_batch*>(b.release());
+  return SK_OK;
+}
+
+void sk_batch_destroy(sk_batch* handle) {
+  auto* b = reinterpret_cast<Batch*>(handle);
+  if (!b) return;
+  cudaSetDevice(b->device);
+  for (auto& l : b->lanes)
+    if (l.stream) cudaStreamSynchronize(l.stream);
+  delete b;
+}
+
+const char* sk_batch_last_error(const sk_batch* handle) {
+  const auto* b = reinterpret_cast<const Batch*>(handle);
+  return b ? b->error.c_str() : "no batch";
+}
+
+#define SK_BATCH(handle)                              \
+  auto* b = reinterpret_cast<Batch*>(handle);         \
+  if (!b) return SK_E_INVALID;                        \
+  if (b->failed) return SK_E_DEVICE;                  \
+  cudaSetDevice(b->device)
+
+sk_status sk_batch_apply_render_policy(sk_batch* handle, const sk_policy* p) {
+  SK_BATCH(handle);
+  if (!p) return SK_E_INVALID;
+  const bool ok = std::isfinite(p->subpixel_threshold) && p->subpixel_threshold >= 0.0f &&
+                  p->sort_depth_bits == 16 &&
+                  std::all_of(p->background, p->background + 3,
+                              [](double c) { return std::isfinite(c) && c >= 0 && c <= 1; });
+  if (!ok) return b->fail(SK_E_INVALID, "batch policy out of range (16-bit depth keys only)");
+  b->policy = *p;
+  return SK_OK;
+}
+
+sk_status sk_batch_submit(sk_batch* handle, const sk_batch_view* views, uint32_t count,
+                          uint64_t* ticket) {
+  SK_BATCH(handle);
+  if (!views || count == 0 || count > b->tuning.maxViews)
+    return b->fail(SK_E_INVALID, "a submission holds 1 to max_views views");
+  BatchLane& l = b->lanes[b->nextLane];
+  b->nextLane = (b->nextLane + 1) % static_cast<uint32_t>(b->lanes.size());
+  if (l.busy) {
+    const sk_status st = b->finish(l, true);
+    if (st == SK_E_DEVICE) return st;
+  }
+  l.busy = false;
+  sk_status st = b->prepare(l, views, count);
+  if (st != SK_OK) return st;
+  st = b->enqueue(l);
+  if (st != SK_OK) return st;
+  l.busy = true;
+  l.harvested = false;
+  l.status = SK_OK;
+  l.ticket = ++b->submitted;
+  if (ticket) *ticket = l.ticket;
+  return SK_OK;
+}
+
+sk_status sk_batch_poll(sk_batch* handle, uint64_t ticket, int32_t* done) {
+  SK_BATCH(handle);
+  BatchLane* l = b->laneOf(ticket);
+  if (!l) return b->fail(SK_E_INVALID, "unknown ticket or its lane was reused");
+  const sk_status st = b->finish(*l, false);
+  if (done) *done = l->harvested ? 1 : 0;
+  return st;
+}
+
+sk_status sk_batch_wait(sk_batch* handle, uint64_t ticket) {
+  SK_BATCH(handle);
+  BatchLane* l = b->laneOf(ticket);
+  if (!l) return b->fail(SK_E_INVALID, "unknown ticket or its lane was reused");
+  return b->finish(*l, true);
+}
+
+sk_status sk_batch_read_image(sk_batch* handle, uint64_t ticket, uint32_t view, void* host,
+                              size_t bytes) {
+  SK_BATCH(handle);
+  BatchLane* l = b->laneOf(ticket);
+  if (!l || !host) return b->fail(SK_E_INVALID, "unknown ticket or no buffer");
+  const sk_status st = b->finish(*l, true);
+  if (st != SK_OK) return st;
+  if (view >= l->viewCount) return b->fail(SK_E_INVALID, "view out of range");
+  const sk::BatchView& t = l->table[view];
+  const size_t need = size_t{t.width} * t.height * 4;
+  if (bytes < need) return b->fail(SK_E_INVALID, "image buffer too small");
+  std::memcpy(host, static_cast<const uint8_t*>(l->hostImage.ptr) + t.pixelOffset * 4, need);
+  return SK_OK;
+}
+
+sk_status sk_batch_view_visible(sk_batch* handle, uint64_t ticket, uint32_t view,
+                                uint32_t* visible) {
+  SK_BATCH(handle);
+  BatchLane* l = b->laneOf(ticket);
+  if (!l || !visible) return b->fail(SK_E_INVALID, "unknown ticket");
+  const sk_status st = b->finish(*l, true);
+  if (st != SK_OK) return st;
+  if (view >= l->viewCount) return b->fail(SK_E_INVALID, "view out of range");
+  const auto* first = static_cast<const uint32_t*>(l->hostViewFirst.ptr);
+  *visible = first[view + 1] - first[view];
+  return SK_OK;
+}
+
+sk_status sk_batch_get_stats(sk_batch* handle, uint64_t ticket, sk_batch_stats* out) {
+  SK_BATCH(handle);
+  BatchLane* l = b->laneOf(ticket);
+  if (!l || !out) return b->fail(SK_E_INVALID, "unknown ticket");
+  const sk_status st = b->finish(*l, true);
+  if (st != SK_OK && st != SK_E_TIMEOUT) return st;
+  out->views = l->viewCount;
+  out->visible = l->result.visible;
+  out->instances = l->result.instances;
+  out->device_error = l->result.error;
+  out->gpu_ms = l->gpuMs;
+  out->fragments = uint64_t{l->result.fragments_lo} | (uint64_t{l->result.fragments_hi} << 32);
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// Batched multi-view rendering: many views, of one or several resident worlds and of different
+// target sizes, drawn by one pass of each stage over the whole batch (one launch per stage).
+//
+// Each lane is a CUDA stream with its own scratch; a submission goes to the next lane and runs
+// while the host prepares the next one, so several batches overlap on the device. Results
+// (images, survivor counts, counters) are copied back into the lane's pinned memory by the
+// same stream, so they are on the host once the submission completes. A lane can capture its
+// stage sequence as a CUDA graph and replay it while its views keep their worlds and sizes.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/splatkit_b200.h"
+#include "../csrc/sk_kernels.h"
+#include "context.h"
+
+namespace sk {
+
+// Tunable launch parameters of a batch (the autotuner picks among them).
+struct BatchTuning {
+  uint32_t lanes = 2;        // submissions in flight
+  uint32_t maxViews = 64;    // views per internal pass (a submission larger than this is split)
+  bool graphs = false;       // replay captured stage sequences
+};
+
+struct BatchLane {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr, start = nullptr, end = nullptr;
+  // capacities
+  uint32_t sources = 0, instances = 0, items = 0, tiles = 0, views = 0;
+  uint64_t pixels = 0;
+  // device
+  DeviceBuffer keys, projected, spans, order, sortWorkspace, visStatus, binSums;
+  DeviceBuffer instKeys, instValues, instKeysSorted, instValuesSorted, tileSortWorkspace;
+  DeviceBuffer ranges, viewFirst, counters, frameCounters, viewTable, cameras, image;
+  // pinned host
+  PinnedBuffer hostViews, hostCameras, hostCounters, hostViewFirst, hostImage;
+  // the submission it holds
+  uint64_t ticket = 0;
+  bool busy = false, harvested = true;
+  sk_status status = SK_OK;
+  std::vector<BatchView> table;          // host copy of the view table
+  std::vector<Camera> cams;
+  std::vector<const void*> worlds;       // per view: the world it draws (graph signature)
+  uint32_t viewCount = 0, totalItems = 0, totalTiles = 0, shDegree = 0;
+  uint64_t totalPixels = 0;
+  float gpuMs = 0;
+  FrameCounters result{};
+  // captured stage sequence and the shape it was captured for
+  cudaGraphExec_t graph = nullptr;
+  std::vector<uint64_t> graphShape;
+  ~BatchLane();
+};
+
+struct Batch {
+  int device = 0;
+  BatchTuning tuning;
+  sk_policy policy{};
+  std::vector<BatchLane> lanes;
+  uint32_t nextLane = 0;
+  uint64_t submitted = 0;
+  uint32_t epoch = 1;
+  std::string error;
+  bool failed = false;
+
+  sk_status fail(sk_status code, const std::string& message);
+  sk_status check(cudaError_t e, const char* what);
+  uint32_t nextEpoch(uint32_t n);
+  sk_status reserve(BatchLane& lane, uint32_t sources, uint32_t instances, uint32_t items,
+                    uint32_t tiles, uint32_t views, uint64_t pixels);
+  // Fills the lane's view table and cameras from the request; no device work.
+  sk_status prepare(BatchLane& lane, const sk_batch_view* views, uint32_t count);
+  // Enqueues the lane's whole batch on its stream (uploads, stages, readbacks, done event).
+  sk_status enqueue(BatchLane& lane);
+  sk_status enqueueStages(BatchLane& lane, bool clearStatus);
+  // Waits for (or polls) the lane's submission; grows and redraws on instance overflow.
+  sk_status finish(BatchLane& lane, bool wait);
+  BatchLane* laneOf(uint64_t ticket);
+};
+
+}  // namespace sk

@@ -177,7 +177,7 @@ sk_status Context::reserveView(uint32_t w, uint32_t h) {
   return check(e, "view buffers");
 }
 
-Camera Context::cameraFor(const sk_frame& frame, uint32_t w, uint32_t h) const {
+Camera cameraOf(const sk_frame& frame, uint32_t w, uint32_t h, float minPixelRadius) {
   Camera c{};
   std::memcpy(c.view, frame.view, 64);
   std::memcpy(c.proj, frame.proj, 64);
@@ -189,13 +189,17 @@ Camera Context::cameraFor(const sk_frame& frame, uint32_t w, uint32_t h) const {
   c.tanHalfFov[0] = 1.0f / frame.proj[0];
   c.tanHalfFov[1] = 1.0f / frame.proj[5];
   c.outputLinear = 0;
-  c.minPixelRadius = policy.subpixel_threshold;
+  c.minPixelRadius = minPixelRadius;
   c.cameraPosition[0] = frame.camera_position[0];
   c.cameraPosition[1] = frame.camera_position[1];
   c.cameraPosition[2] = frame.camera_position[2];
   c.cameraPosition[3] = 1.0f;
   c.reveal[0] = frame.reveal_level;
   return c;
+}
+
+Camera Context::cameraFor(const sk_frame& frame, uint32_t w, uint32_t h) const {
+  return cameraOf(frame, w, h, policy.subpixel_threshold);
 }
 
 // Validates ranges before anything is written (MetalVisibilityPass.mm:150-162).

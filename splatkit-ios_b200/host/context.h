@@ -104,6 +104,9 @@ struct ViewTarget {
   uint32_t tilesY() const { return (height + kTileSize - 1) / kTileSize; }
 };
 
+// The per-view camera block of a frame on a width x height target.
+Camera cameraOf(const sk_frame& frame, uint32_t width, uint32_t height, float minPixelRadius);
+
 struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;

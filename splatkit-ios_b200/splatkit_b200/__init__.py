@@ -94,6 +94,22 @@ class _Frame(ctypes.Structure):
                 ("sh_degree", ctypes.c_int32)]
 
 
+class _BatchConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("lanes", ctypes.c_uint32),
+                ("max_views", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32)]
+
+
+class _BatchView(ctypes.Structure):
+    _fields_ = [("world", ctypes.c_void_p), ("frame", _Frame), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32)]
+
+
+class _BatchStats(ctypes.Structure):
+    _fields_ = [("views", ctypes.c_uint32), ("visible", ctypes.c_uint32),
+                ("instances", ctypes.c_uint32), ("device_error", ctypes.c_uint32),
+                ("gpu_ms", ctypes.c_double), ("fragments", ctypes.c_uint64)]
+
+
 class _Policy(ctypes.Structure):
     _fields_ = [("lod_error_pixels", ctypes.c_float), ("lod_splat_limit", ctypes.c_uint32),
                 ("alpha_threshold", ctypes.c_float), ("subpixel_threshold", ctypes.c_float),
@@ -168,6 +184,19 @@ _SIGNATURES = {
                                                  ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_size_t, ctypes.c_void_p,
                                                  ctypes.c_void_p]),
+    "sk_batch_create": (ctypes.c_int32, [ctypes.POINTER(_BatchConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "sk_batch_destroy": (None, [ctypes.c_void_p]),
+    "sk_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "sk_batch_apply_render_policy": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Policy)]),
+    "sk_batch_submit": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_BatchView), ctypes.c_uint32,
+                                         ctypes.POINTER(ctypes.c_uint64)]),
+    "sk_batch_poll": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]),
+    "sk_batch_wait": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64]),
+    "sk_batch_read_image": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
+                                             ctypes.c_void_p, ctypes.c_size_t]),
+    "sk_batch_view_visible": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
+                                               ctypes.POINTER(ctypes.c_uint32)]),
+    "sk_batch_get_stats": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(_BatchStats)]),
     "sk_radix_argsort_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_uint32, ctypes.c_int32,
                                                   ctypes.c_void_p, ctypes.c_void_p,
@@ -462,6 +491,99 @@ class Renderer:
         self._check(self._lib.sk_read_cut(self._h, _ptr(cut, _u32p), n.value, ctypes.byref(n),
                                           _ptr(stats, _u32p)), "cut")
         return cut, stats
+
+
+# ---- batched multi-view rendering ----------------------------------------------------------
+class BatchView:
+    """One view of a batch: the renderer whose resident world it draws, the frame, the size."""
+
+    def __init__(self, renderer: "Renderer", frame: Frame, width: int, height: int):
+        self.renderer, self.frame, self.width, self.height = renderer, frame, width, height
+
+
+class Batch:
+    """Many views drawn together (sk_batch_*): every stage runs once over the whole batch.
+
+    ``submit`` returns a ticket at once; results stay readable until the lane that ran the
+    ticket is reused, ``lanes`` submissions later."""
+
+    def __init__(self, device: int = 0, lanes: int = 2, max_views: int = 64, use_graphs: bool = False):
+        self._lib = library()
+        cfg = _BatchConfig(device, lanes, max_views, 1 if use_graphs else 0)
+        handle = ctypes.c_void_p()
+        st = self._lib.sk_batch_create(ctypes.byref(cfg), ctypes.byref(handle))
+        if st != SK_OK:
+            raise SplatError(st, "sk_batch_create failed (is a CUDA device visible?)")
+        self._h = handle
+        self._sizes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sk_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st != SK_OK:
+            msg = self._lib.sk_batch_last_error(self._h)
+            raise SplatError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def apply_render_policy(self, policy: Policy):
+        p = policy.native()
+        self._check(self._lib.sk_batch_apply_render_policy(self._h, ctypes.byref(p)), "policy")
+
+    def submit(self, views: Sequence[BatchView]) -> int:
+        arr = (_BatchView * len(views))()
+        keep = []
+        for i, v in enumerate(views):
+            f, ranges = v.frame.native()
+            keep.append(ranges)
+            arr[i].world = v.renderer._h
+            arr[i].frame = f
+            arr[i].width, arr[i].height = v.width, v.height
+        ticket = ctypes.c_uint64()
+        self._check(self._lib.sk_batch_submit(self._h, arr, len(views), ctypes.byref(ticket)), "submit")
+        self._sizes[ticket.value] = [(v.width, v.height) for v in views]
+        if len(self._sizes) > 64:
+            self._sizes.pop(next(iter(self._sizes)))
+        return ticket.value
+
+    def poll(self, ticket: int) -> bool:
+        done = ctypes.c_int32()
+        self._check(self._lib.sk_batch_poll(self._h, ticket, ctypes.byref(done)), "poll")
+        return bool(done.value)
+
+    def wait(self, ticket: int):
+        self._check(self._lib.sk_batch_wait(self._h, ticket), "wait")
+
+    def read_image(self, ticket: int, view: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        w, h = self._sizes[ticket][view]
+        if out is None:
+            out = np.empty((h, w, 4), np.uint8)
+        self._check(self._lib.sk_batch_read_image(self._h, ticket, view, out.ctypes.data, out.nbytes),
+                    "read_image")
+        return out
+
+    def view_visible(self, ticket: int, view: int) -> int:
+        n = ctypes.c_uint32()
+        self._check(self._lib.sk_batch_view_visible(self._h, ticket, view, ctypes.byref(n)), "visible")
+        return n.value
+
+    def stats(self, ticket: int) -> dict:
+        st = _BatchStats()
+        self._check(self._lib.sk_batch_get_stats(self._h, ticket, ctypes.byref(st)), "stats")
+        return {name: getattr(st, name) for name, _ in _BatchStats._fields_}
 
 
 def radix_argsort_device(keys_ptr: int, count_ptr: int, capacity: int, bits: int, order_ptr: int,

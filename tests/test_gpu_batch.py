@@ -1,0 +1,148 @@
+"""The batched multi-view path (sk_batch_*) against the plain per-frame path, view by view.
+
+A batch runs every stage once over all its views (several worlds, several target sizes) with
+the plain frame's arithmetic, so each view's image and survivor count must equal what sk_draw
+gives for that view with 16-bit depth keys — bit for bit, not just within tolerance.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import splatkit_b200 as sk
+from splatkit_b200 import camera as skcam
+from splatkit_b200 import synthetic
+
+SIZES = [(320, 240), (640, 480), (200, 150), (333, 177), (512, 512)]
+
+
+def proj_for(width, height):
+    return skcam.perspective(math.radians(60.0), width / height, 0.05, 200.0)
+
+
+def plain(renderer, frame, width, height):
+    renderer.resize(width, height)
+    renderer.draw(frame)
+    image = renderer.read_image(sk.FORMAT_RGBA8)
+    return image.copy(), renderer.stats()["draw_count"]
+
+
+@pytest.fixture(scope="module")
+def worlds(cuda_device):
+    a = synthetic.random_cloud(120_000, seed=3, sh_degree=3)
+    b = synthetic.random_cloud(40_000, seed=4, sh_degree=3, half_extent=6.0)
+    rs = []
+    for cloud in (a, b):
+        r = sk.Renderer(64, 64, image_format=sk.FORMAT_RGBA8)
+        r.apply_render_policy(sk.Policy(sort_depth_bits=16))
+        r.upload_world(cloud, 3)
+        rs.append((r, cloud))
+    yield rs
+    for r, _ in rs:
+        r.close()
+
+
+def views_for(worlds, count, start_frame=0, ranges=None):
+    out = []
+    for i in range(count):
+        r, cloud = worlds[i % len(worlds)]
+        w, h = SIZES[i % len(SIZES)]
+        view, eye = skcam.orbit_view(start_frame + 11 * i, radius=15.0 if i % 2 == 0 else 9.0)
+        rng = ranges[i] if ranges else [(0, cloud.count)]
+        out.append(sk.BatchView(r, sk.Frame(view, proj_for(w, h), eye, rng, 3), w, h))
+    return out
+
+
+def check_against_plain(batch, ticket, views):
+    for i, v in enumerate(views):
+        want, want_visible = plain(v.renderer, v.frame, v.width, v.height)
+        got = batch.read_image(ticket, i)
+        assert batch.view_visible(ticket, i) == want_visible, f"view {i}"
+        assert np.array_equal(got, want), (
+            f"view {i}: {np.count_nonzero(got != want)} channels differ, "
+            f"max {np.abs(got.astype(int) - want.astype(int)).max()}")
+
+
+@pytest.mark.gpu
+def test_batch_of_two_worlds_and_five_sizes_equals_plain_frames(worlds):
+    views = views_for(worlds, 10)
+    with sk.Batch(lanes=2, max_views=16) as batch:
+        ticket = batch.submit(views)
+        batch.wait(ticket)
+        stats = batch.stats(ticket)
+        assert stats["views"] == 10 and stats["device_error"] == 0
+        assert stats["visible"] == sum(batch.view_visible(ticket, i) for i in range(10))
+        check_against_plain(batch, ticket, views)
+
+
+@pytest.mark.gpu
+def test_submissions_in_flight_on_two_lanes(worlds):
+    first = views_for(worlds, 4, start_frame=5)
+    second = views_for(worlds, 6, start_frame=40,
+                       ranges=[[(1000, 30_000)], [(0, 40_000)], [(5, 100_000)], [(0, 20_000)],
+                               [(0, 120_000)], [(7, 3)]])
+    with sk.Batch(lanes=2, max_views=8) as batch:
+        t1 = batch.submit(first)
+        t2 = batch.submit(second)  # runs while the first may still be on the device
+        batch.wait(t2)
+        batch.wait(t1)
+        check_against_plain(batch, t1, first)
+        check_against_plain(batch, t2, second)
+        # a third submission reuses the first lane: its ticket is gone
+        t3 = batch.submit(first)
+        with pytest.raises(sk.SplatError):
+            batch.wait(t1)
+        check_against_plain(batch, t3, first)
+
+
+@pytest.mark.gpu
+def test_graph_replay_with_new_cameras(worlds):
+    with sk.Batch(lanes=1, max_views=8, use_graphs=True) as batch:
+        for start in (0, 17, 33):  # same worlds and sizes: captured once, replayed twice
+            views = views_for(worlds, 5, start_frame=start)
+            ticket = batch.submit(views)
+            check_against_plain(batch, ticket, views)
+
+
+@pytest.mark.gpu
+def test_instance_overflow_grows_and_redraws(cuda_device):
+    # few large splats close to the camera: far more tile instances than the first guess
+    cloud = synthetic.random_cloud(3000, seed=9, sh_degree=3, half_extent=2.0, log_scale_mean=-0.7,
+                                   log_scale_std=0.2)
+    r = sk.Renderer(64, 64, image_format=sk.FORMAT_RGBA8)
+    r.apply_render_policy(sk.Policy(sort_depth_bits=16))
+    r.upload_world(cloud, 3)
+    view, eye = skcam.orbit_view(3, radius=6.0)
+    views = [sk.BatchView(r, sk.Frame(view, proj_for(640, 480), eye, [(0, 3000)], 3), 640, 480)]
+    with sk.Batch(lanes=1, max_views=4) as batch:
+        ticket = batch.submit(views)
+        stats = batch.stats(ticket)
+        assert stats["instances"] > 4 * 3000
+        check_against_plain(batch, ticket, views)
+    r.close()
+
+
+@pytest.mark.gpu
+def test_batch_rejects_what_it_cannot_draw(worlds, cuda_device):
+    (ra, a), _ = worlds
+    low = sk.Renderer(64, 64)
+    low.upload_world(synthetic.random_cloud(1000, seed=1, sh_degree=1), 1)
+    view, eye = skcam.orbit_view(0)
+    with sk.Batch(lanes=1, max_views=2) as batch:
+        mixed = [sk.BatchView(ra, sk.Frame(view, proj_for(64, 64), eye, [(0, a.count)], 3), 64, 64),
+                 sk.BatchView(low, sk.Frame(view, proj_for(64, 64), eye, [(0, 1000)], 3), 64, 64)]
+        with pytest.raises(sk.SplatError) as info:
+            batch.submit(mixed)
+        assert info.value.status == sk.SK_E_INVALID
+        with pytest.raises(sk.SplatError):
+            batch.submit(mixed[:1] * 3)  # more than max_views
+        with pytest.raises(sk.SplatError):
+            batch.submit([sk.BatchView(ra, sk.Frame(view, proj_for(64, 64), eye, [(0, a.count + 1)], 3),
+                                       64, 64)])
+        with pytest.raises(sk.SplatError):
+            batch.apply_render_policy(sk.Policy(sort_depth_bits=32))
+        ok = batch.submit(mixed[:1])
+        batch.wait(ok)
+    low.close()
