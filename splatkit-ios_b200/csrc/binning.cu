@@ -45,20 +45,60 @@ __global__ void __launch_bounds__(kThreads) binCountKernel(const __grid_constant
   }
 }
 
-// One warp's items for the emission loop: span, and (projected index, first output slot).
+// The block's items for the emission loop.
 struct ItemStage {
-  uint4 span[32 * kItems];
-  uint2 value[32 * kItems];
-  uint2 grid[32 * kItems];  // batch: (first tile id, tiles per row) of the item's view
+  uint4 span[kTileSplats];
+  uint32_t value[kTileSplats];   // projected index
+  uint32_t offset[kTileSplats];  // first position in the block's output range
+  uint2 grid[kTileSplats];       // batch: (first tile id, tiles per row) of the item's view
+  uint32_t total;
 };
+
+// Position of the k-th (from 0) set bit of x; x holds more than k set bits. Bisection on halves.
+__device__ __forceinline__ uint32_t kthSetBit(uint32_t x, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t width = 16; width > 0; width >>= 1) {
+    const uint32_t low = __popc(x & ((1u << width) - 1u));
+    if (k >= low) {
+      k -= low;
+      x >>= width;
+      pos += width;
+    }
+  }
+  return pos;
+}
+
+// The tile ids of one item's box: id(b) for box position b = row * w + col.
+struct TileGrid {
+  uint32_t rowStart, tilesX;
+  // b / w for b < area <= 16641 and w <= 129: (b + 1/2) / w is at least 1/(2w) away from an
+  // integer and the float product errs by far less, so truncation gives the quotient.
+  __device__ __forceinline__ uint32_t id(uint32_t b, uint32_t w) const {
+    const uint32_t q = static_cast<uint32_t>((static_cast<float>(b) + 0.5f) *
+                                             __frcp_rn(static_cast<float>(w)));
+    return rowStart + q * tilesX + (b - q * w);
+  }
+};
+
+template <bool kBatch>
+__device__ __forceinline__ TileGrid gridOf(const BinArgs& a, const ItemStage& stage, uint32_t j,
+                                           const uint4 sp) {
+  const uint32_t x0 = sp.x & 0xffffu, y0 = sp.x >> 16;
+  if constexpr (kBatch) {
+    const uint2 g = stage.grid[j];
+    return TileGrid{g.x + y0 * g.y + x0, g.y};
+  }
+  return TileGrid{y0 * a.tilesX + x0, a.tilesX};
+}
 
 // Pass 2: each block sums the totals of the blocks before it, then writes its instances.
 // kBatch: the survivors are a batch's views back to back in depth-rank order (rank i belongs to
 // view v when viewFirst[v] <= i < viewFirst[v + 1]); tile ids are batch-wide.
-template <bool kBatch>
+template <bool kBatch, bool kBalanced>
 __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant__ BinArgs a) {
   __shared__ uint32_t warpBase[kThreads / 32];
-  __shared__ ItemStage itemStage[kThreads / 32];
+  __shared__ ItemStage stage;
   __shared__ uint32_t tileBase;
   const uint32_t n = min(*a.count, a.capacity);
   const uint32_t tiles = (n + kTileSplats - 1) / kTileSplats;
@@ -124,63 +164,86 @@ __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant_
       if (lane < kThreads / 32) warpBase[lane] = inc - w;
     }
     __syncthreads();
-    const uint32_t base = tileBase + warpBase[warp];
-    // Emission: the warp writes its items' instances one item at a time, all lanes together, so
-    // each store covers a contiguous run of the output (the item's tiles in increasing box
-    // order). Lane l takes box tiles l and l + 32 of a masked span, or every 32nd tile of a
-    // span that lists its whole box. Items are staged in shared memory and read back by
-    // broadcast.
-    const uint32_t below = lanemaskLt();
-    ItemStage& stage = itemStage[warp];
+    // Stage the block's items: span, projected index, first position in the block's output
+    // range [0, total) (from tileBase on), and for a batch the view's tile grid.
 #pragma unroll
     for (uint32_t r = 0; r < kItems; ++r) {
-      stage.span[r * 32 + lane] = span[r];
-      stage.value[r * 32 + lane] = make_uint2(value[r], base + rowExclusive[r]);
+      const uint32_t at = warp * (32 * kItems) + r * 32 + lane;
+      stage.span[at] = span[r];
+      stage.value[at] = value[r];
+      stage.offset[at] = warpBase[warp] + rowExclusive[r];
       if constexpr (kBatch) {
-        const uint32_t i = tile * kTileSplats + warp * (32 * kItems) + r * 32 + lane;
+        const uint32_t i = tile * kTileSplats + at;
         uint32_t lo = 0, hi = a.viewCount;
         while (hi - lo > 1) {
           const uint32_t mid = (lo + hi) / 2;
           if (__ldg(a.viewFirst + mid) <= i) lo = mid; else hi = mid;
         }
-        stage.grid[r * 32 + lane] = make_uint2(__ldg(&a.views[lo].tileBase), __ldg(&a.views[lo].tilesX));
+        stage.grid[at] = make_uint2(__ldg(&a.views[lo].tileBase), __ldg(&a.views[lo].tilesX));
       }
     }
-    __syncwarp();
+    if (warp == kThreads / 32 - 1 && lane == 31) stage.total = warpBase[warp] + warpRun;
+    __syncthreads();
+    const uint32_t itemsBegin = warp * (32 * kItems), itemsEnd = itemsBegin + 32 * kItems;
+    const uint32_t outBegin = stage.offset[itemsBegin];
+    const uint32_t outEnd = warp + 1 < kThreads / 32 ? stage.offset[itemsEnd] : stage.total;
+    if constexpr (!kBalanced) {
+      // One item at a time, all lanes together: each store covers a contiguous run of the
+      // output (the item's tiles in increasing box order). Lane l takes box tiles l and l + 32
+      // of a masked span, or every 32nd tile of a span that lists its whole box. Few
+      // instructions per instance are spent when most items have few tiles, but the warp walks
+      // its items one by one: the better choice when the grid is about one wave.
+      const uint32_t below = lanemaskLt();
 #pragma unroll
-    for (uint32_t r = 0; r < kItems; ++r) {
-      uint32_t pending = __ballot_sync(0xffffffffu, cnt[r] != 0);
-      while (pending) {
-        const uint32_t j = r * 32 + (__ffs(pending) - 1);
-        pending &= pending - 1;
-        const uint4 sp = stage.span[j];
-        const uint2 vf = stage.value[j];
-        const uint32_t val = vf.x, first = vf.y;
-        const uint32_t x0 = sp.x & 0xffffu, y0 = sp.x >> 16;
-        const uint32_t w = sp.y & 0xffffu, area = sp.y >> 16;
-        const uint32_t lo = sp.z, hi = sp.w;
-        // k / w for k < area <= 16641 and w <= 129: (k + 1/2) / w is at least 1/(2w) away from
-        // an integer and the float product errs by far less, so truncation gives the quotient.
-        const float rw = __frcp_rn(static_cast<float>(w));
-        uint32_t tilesX = a.tilesX, rowStart = y0 * a.tilesX + x0;
-        if constexpr (kBatch) {
-          const uint2 g = stage.grid[j];
-          tilesX = g.y;
-          rowStart = g.x + y0 * g.y + x0;
-        }
-        auto emit = [&](uint32_t k, uint32_t slot) {
-          const uint32_t q = static_cast<uint32_t>((static_cast<float>(k) + 0.5f) * rw);
-          const uint32_t id = rowStart + q * tilesX + (k - q * w);
-          if (slot < a.instanceCapacity) {
-            a.instanceKeys[slot] = id;
-            a.instanceValues[slot] = val;
+      for (uint32_t r = 0; r < kItems; ++r) {
+        uint32_t pending = __ballot_sync(0xffffffffu, cnt[r] != 0);
+        while (pending) {
+          const uint32_t j = itemsBegin + r * 32 + (__ffs(pending) - 1);
+          pending &= pending - 1;
+          const uint4 sp = stage.span[j];
+          const uint32_t val = stage.value[j], first = tileBase + stage.offset[j];
+          const uint32_t w = sp.y & 0xffffu, area = sp.y >> 16;
+          const TileGrid g = gridOf<kBatch>(a, stage, j, sp);
+          auto emit = [&](uint32_t k, uint32_t slot) {
+            if (slot < a.instanceCapacity) {
+              a.instanceKeys[slot] = g.id(k, w);
+              a.instanceValues[slot] = val;
+            }
+          };
+          if (area > 64) {
+            for (uint32_t k = lane; k < area; k += 32) emit(k, first + k);
+          } else {
+            if ((sp.z >> lane) & 1u) emit(lane, first + __popc(sp.z & below));
+            if (sp.w != 0u && ((sp.w >> lane) & 1u))
+              emit(lane + 32, first + __popc(sp.z) + __popc(sp.w & below));
           }
-        };
-        if (area > 64) {
-          for (uint32_t k = lane; k < area; k += 32) emit(k, first + k);
-        } else {
-          if ((lo >> lane) & 1u) emit(lane, first + __popc(lo & below));
-          if (hi != 0u && ((hi >> lane) & 1u)) emit(lane + 32, first + __popc(lo) + __popc(hi & below));
+        }
+      }
+    } else {
+      // Load-balanced over the warp's output range: lane l writes positions l, l + 32, ..., so
+      // every store is 32 consecutive slots whatever the items' sizes. The item holding
+      // position p is the last of the warp's items whose offset is <= p (a 7-step search in
+      // shared memory) and its k-th tile is decoded from the span: fewer instructions per
+      // instance than the item walk, the better choice for grids of many waves.
+      for (uint32_t p = outBegin + lane; p < outEnd; p += 32) {
+        uint32_t lo = itemsBegin, hi = itemsEnd;
+#pragma unroll
+        for (int step = 0; step < 7; ++step) {
+          const uint32_t mid = (lo + hi) / 2;
+          if (stage.offset[mid] <= p) lo = mid; else hi = mid;
+        }
+        const uint32_t j = lo, k = p - stage.offset[j];
+        const uint4 sp = stage.span[j];
+        const uint32_t w = sp.y & 0xffffu, area = sp.y >> 16;
+        uint32_t bit = k;  // box position of the k-th listed tile
+        if (area <= 64) {
+          const uint32_t nlo = __popc(sp.z);
+          bit = k < nlo ? kthSetBit(sp.z, k) : 32u + kthSetBit(sp.w, k - nlo);
+        }
+        const uint32_t slot = tileBase + p;
+        if (slot < a.instanceCapacity) {
+          a.instanceKeys[slot] = gridOf<kBatch>(a, stage, j, sp).id(bit, w);
+          a.instanceValues[slot] = stage.value[j];
         }
       }
     }
@@ -205,8 +268,13 @@ uint32_t binBlocks(uint32_t capacity) { return max(1u, (capacity + kTileSplats -
 cudaError_t launchBinning(const BinArgs& a, cudaStream_t stream) {
   const uint32_t grid = binBlocks(a.capacity);
   binCountKernel<<<grid, kThreads, 0, stream>>>(a);
-  if (a.viewCount > 0) binEmitKernel<true><<<grid, kThreads, 0, stream>>>(a);
-  else binEmitKernel<false><<<grid, kThreads, 0, stream>>>(a);
+  if (a.viewCount > 0) {
+    if (a.balanced) binEmitKernel<true, true><<<grid, kThreads, 0, stream>>>(a);
+    else binEmitKernel<true, false><<<grid, kThreads, 0, stream>>>(a);
+  } else {
+    if (a.balanced) binEmitKernel<false, true><<<grid, kThreads, 0, stream>>>(a);
+    else binEmitKernel<false, false><<<grid, kThreads, 0, stream>>>(a);
+  }
   return cudaGetLastError();
 }
 

@@ -107,6 +107,9 @@ struct BinArgs {
   const BatchView* views;
   const uint32_t* viewFirst;  // viewCount + 1 words (BatchVisibilityArgs)
   uint32_t viewCount;
+  // emission: 0 walks each warp's items one by one (best near one wave of blocks), 1 balances
+  // each warp's output over its lanes (fewer instructions per instance; best for large grids)
+  uint32_t balanced;
 };
 uint32_t binBlocks(uint32_t capacity);
 cudaError_t launchBinning(const BinArgs& args, cudaStream_t stream);

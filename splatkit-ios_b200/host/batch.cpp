@@ -251,6 +251,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     b.views = views;
     b.viewFirst = viewFirst;
     b.viewCount = l.viewCount;
+    b.balanced = tuning.balancedEmit ? 1u : 0u;
     e = launchBinning(b, s);
   }
   if (e == cudaSuccess) {

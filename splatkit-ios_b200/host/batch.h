@@ -24,6 +24,7 @@ struct BatchTuning {
   uint32_t lanes = 2;        // submissions in flight
   uint32_t maxViews = 64;    // views per internal pass (a submission larger than this is split)
   bool graphs = false;       // replay captured stage sequences
+  bool balancedEmit = true;  // binning emission strategy (BinArgs::balanced)
 };
 
 struct BatchLane {
