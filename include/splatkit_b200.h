@@ -245,6 +245,68 @@ sk_status sk_batch_view_visible(sk_batch* batch, uint64_t ticket, uint32_t view,
                                 uint32_t* visible);
 sk_status sk_batch_get_stats(sk_batch* batch, uint64_t ticket, sk_batch_stats* out);
 
+/* ---- serving: continuous batching of render requests --------------------------------------
+ * A server holds resident scenes (contexts with flat worlds, added once) and a scheduler thread.
+ * Requests are queued as they arrive; whenever one of the server's lanes is free the scheduler
+ * takes the queued requests in arrival order (up to max_batch_views views and
+ * max_batch_splats drawn records, within the memory budget) and runs them as one batch, so
+ * requests that arrive while others are on the GPU join the next batch and their work overlaps
+ * with the batches in flight. Each request's RGBA8 image is copied straight into the caller's
+ * buffer. Admission: a request is priced like the reference's gpuWorldBytes (52 bytes per drawn
+ * record plus its image) and waits until the priced bytes of the requests in flight leave room
+ * for it under memory_budget minus the resident scenes; a request that can never fit, or that
+ * has waited longer than max_queue_ms, completes with SK_E_ADMISSION. Results equal sk_draw's
+ * for the same view (16-bit depth keys, default policy). */
+typedef struct sk_server sk_server;
+
+typedef struct {
+  int32_t device;
+  uint32_t lanes;            /* batches in flight, >= 1 */
+  uint32_t max_batch_views;  /* 1..65536 */
+  uint64_t max_batch_splats; /* drawn records per batch (bounds each lane's scratch) */
+  uint64_t memory_budget;    /* bytes for resident scenes plus requests in flight */
+  double max_queue_ms;       /* shed requests that waited longer; <= 0: never */
+} sk_server_config;
+
+typedef struct {
+  uint32_t scene;  /* from sk_server_add_scene */
+  sk_frame frame;  /* camera; at most one range (none: the whole scene) */
+  uint32_t width, height;
+  void* image;     /* caller host buffer of width * height * 4 bytes, or NULL; written when the
+                      request completes; pinned memory (sk_server_alloc_host) copies fastest */
+} sk_request;
+
+typedef struct {
+  uint64_t id;
+  sk_status status;     /* SK_OK, SK_E_ADMISSION (shed or can never fit), SK_E_TIMEOUT */
+  uint32_t visible;     /* survivors of the cull */
+  uint32_t batch_views; /* views in the batch that drew it */
+  double queue_ms;      /* arrival to batch start on the host */
+  double latency_ms;    /* arrival to image on the host */
+} sk_completion;
+
+sk_status sk_server_create(const sk_server_config* config, sk_server** out);
+void sk_server_destroy(sk_server* server);
+const char* sk_server_last_error(const sk_server* server);
+/* Adds the context's resident world as a scene; the context must outlive the server and keep
+ * its world while the server runs. */
+sk_status sk_server_add_scene(sk_server* server, sk_context* world, uint32_t* scene);
+/* Queues a request (any thread); its arrival time is now. */
+sk_status sk_server_submit(sk_server* server, const sk_request* request, uint64_t* id);
+/* Moves up to `capacity` completions out, oldest first. */
+sk_status sk_server_take_completions(sk_server* server, sk_completion* out, uint32_t capacity,
+                                     uint32_t* count);
+/* Waits until every submitted request has completed. */
+sk_status sk_server_drain(sk_server* server);
+/* Replays an arrival trace: request i is submitted at arrival_us[i] microseconds after the call
+ * starts (the calling thread sleeps between arrivals), then waits for all of them; out[i]
+ * receives request i's completion. */
+sk_status sk_server_replay(sk_server* server, const sk_request* requests, const double* arrival_us,
+                           uint32_t count, sk_completion* out);
+/* Pinned host memory for request images (sk_server_free_host releases it). */
+void* sk_server_alloc_host(size_t bytes);
+void sk_server_free_host(void* ptr);
+
 /* ---- component operators over caller device memory ----------------------------------- */
 /* MetalRadixSort (splatkit-ios/.../metal/sort/MetalRadixSort.h:13-54): stable ascending argsort
  * of min(*d_count, capacity) keys (d_count is a device word), 16 or 32 bits; d_keys is left

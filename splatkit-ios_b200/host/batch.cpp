@@ -93,7 +93,7 @@ sk_status Batch::reserve(BatchLane& l, uint32_t sources, uint32_t instances, uin
   pin(l.hostCameras, size_t{views} * sizeof(Camera));
   pin(l.hostCounters, sizeof(FrameCounters));
   pin(l.hostViewFirst, size_t{views + 1} * 4);
-  pin(l.hostImage, pixels * 4);
+  if (l.destinations.empty()) pin(l.hostImage, pixels * 4);  // else views go to the caller's buffers
   if (e == cudaSuccess && freshCounters) e = cudaMemsetAsync(l.counters.ptr, 0, 64 * 4, l.stream);
   // fresh sort workspaces: counters and histogram accumulators start at zero
   if (e == cudaSuccess && grewSources)
@@ -322,8 +322,17 @@ sk_status Batch::enqueue(BatchLane& l) {
     if (r == cudaSuccess)
       r = cudaMemcpyAsync(l.hostViewFirst.ptr, l.viewFirst.ptr, size_t{l.viewCount + 1} * 4,
                           cudaMemcpyDeviceToHost, s);
-    if (r == cudaSuccess)
-      r = cudaMemcpyAsync(l.hostImage.ptr, l.image.ptr, l.totalPixels * 4, cudaMemcpyDeviceToHost, s);
+    if (l.destinations.empty()) {
+      if (r == cudaSuccess)
+        r = cudaMemcpyAsync(l.hostImage.ptr, l.image.ptr, l.totalPixels * 4, cudaMemcpyDeviceToHost, s);
+    } else {
+      for (uint32_t i = 0; i < l.viewCount && r == cudaSuccess; ++i) {
+        const BatchView& t = l.table[i];
+        if (l.destinations[i])
+          r = cudaMemcpyAsync(l.destinations[i], static_cast<const uint8_t*>(l.image.ptr) + t.pixelOffset * 4,
+                              size_t{t.width} * t.height * 4, cudaMemcpyDeviceToHost, s);
+      }
+    }
     return check(r, "batch readback");
   };
   sk_status st = SK_OK;

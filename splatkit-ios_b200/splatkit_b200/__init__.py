@@ -110,6 +110,23 @@ class _BatchStats(ctypes.Structure):
                 ("gpu_ms", ctypes.c_double), ("fragments", ctypes.c_uint64)]
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("lanes", ctypes.c_uint32),
+                ("max_batch_views", ctypes.c_uint32), ("max_batch_splats", ctypes.c_uint64),
+                ("memory_budget", ctypes.c_uint64), ("max_queue_ms", ctypes.c_double)]
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_uint32), ("frame", _Frame), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("image", ctypes.c_void_p)]
+
+
+class _Completion(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("visible", ctypes.c_uint32),
+                ("batch_views", ctypes.c_uint32), ("queue_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double)]
+
+
 class _Policy(ctypes.Structure):
     _fields_ = [("lod_error_pixels", ctypes.c_float), ("lod_splat_limit", ctypes.c_uint32),
                 ("alpha_threshold", ctypes.c_float), ("subpixel_threshold", ctypes.c_float),
@@ -197,6 +214,18 @@ _SIGNATURES = {
     "sk_batch_view_visible": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
                                                ctypes.POINTER(ctypes.c_uint32)]),
     "sk_batch_get_stats": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(_BatchStats)]),
+    "sk_server_create": (ctypes.c_int32, [ctypes.POINTER(_ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "sk_server_destroy": (None, [ctypes.c_void_p]),
+    "sk_server_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "sk_server_add_scene": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
+    "sk_server_submit": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Request), ctypes.POINTER(ctypes.c_uint64)]),
+    "sk_server_take_completions": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Completion), ctypes.c_uint32,
+                                                    ctypes.POINTER(ctypes.c_uint32)]),
+    "sk_server_drain": (ctypes.c_int32, [ctypes.c_void_p]),
+    "sk_server_replay": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Request), ctypes.POINTER(ctypes.c_double),
+                                          ctypes.c_uint32, ctypes.POINTER(_Completion)]),
+    "sk_server_alloc_host": (ctypes.c_void_p, [ctypes.c_size_t]),
+    "sk_server_free_host": (None, [ctypes.c_void_p]),
     "sk_radix_argsort_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_uint32, ctypes.c_int32,
                                                   ctypes.c_void_p, ctypes.c_void_p,
@@ -584,6 +613,122 @@ class Batch:
         st = _BatchStats()
         self._check(self._lib.sk_batch_get_stats(self._h, ticket, ctypes.byref(st)), "stats")
         return {name: getattr(st, name) for name, _ in _BatchStats._fields_}
+
+
+# ---- serving ---------------------------------------------------------------------------------
+class HostImage:
+    """A pinned host image buffer (sk_server_alloc_host) viewed as an (h, w, 4) uint8 array."""
+
+    def __init__(self, width: int, height: int):
+        self._lib = library()
+        self.nbytes = width * height * 4
+        self.ptr = self._lib.sk_server_alloc_host(self.nbytes)
+        if not self.ptr:
+            raise SplatError(SK_E_OOM, "pinned host allocation failed")
+        buf = (ctypes.c_uint8 * self.nbytes).from_address(self.ptr)
+        self.array = np.frombuffer(buf, np.uint8).reshape(height, width, 4)
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self.array = None
+            self._lib.sk_server_free_host(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Request:
+    """One render request: scene index, frame, size, and the host image it is written into."""
+
+    def __init__(self, scene: int, frame: Frame, width: int, height: int,
+                 image: Optional[HostImage] = None):
+        self.scene, self.frame, self.width, self.height, self.image = scene, frame, width, height, image
+
+    def native(self):
+        f, ranges = self.frame.native()
+        r = _Request()
+        r.scene, r.frame, r.width, r.height = self.scene, f, self.width, self.height
+        r.image = self.image.ptr if self.image is not None else None
+        return r, ranges
+
+
+COMPLETION_FIELDS = [name for name, _ in _Completion._fields_]
+
+
+class Server:
+    """Continuous-batching render server over resident scenes (sk_server_*)."""
+
+    def __init__(self, device: int = 0, lanes: int = 2, max_batch_views: int = 64,
+                 max_batch_splats: int = 64_000_000, memory_budget: int = 120 << 30,
+                 max_queue_ms: float = 0.0):
+        self._lib = library()
+        cfg = _ServerConfig(device, lanes, max_batch_views, max_batch_splats, memory_budget, max_queue_ms)
+        handle = ctypes.c_void_p()
+        st = self._lib.sk_server_create(ctypes.byref(cfg), ctypes.byref(handle))
+        if st != SK_OK:
+            raise SplatError(st, "sk_server_create failed (is a CUDA device visible?)")
+        self._h = handle
+        self._scenes = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sk_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st != SK_OK:
+            msg = self._lib.sk_server_last_error(self._h)
+            raise SplatError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def add_scene(self, renderer: "Renderer") -> int:
+        idx = ctypes.c_uint32()
+        self._check(self._lib.sk_server_add_scene(self._h, renderer._h, ctypes.byref(idx)), "add_scene")
+        self._scenes.append(renderer)
+        return idx.value
+
+    def submit(self, request: Request) -> int:
+        r, keep = request.native()
+        rid = ctypes.c_uint64()
+        self._check(self._lib.sk_server_submit(self._h, ctypes.byref(r), ctypes.byref(rid)), "submit")
+        return rid.value
+
+    def drain(self):
+        self._check(self._lib.sk_server_drain(self._h), "drain")
+
+    def take_completions(self, capacity: int = 4096) -> list:
+        out = (_Completion * capacity)()
+        n = ctypes.c_uint32()
+        self._check(self._lib.sk_server_take_completions(self._h, out, capacity, ctypes.byref(n)), "take")
+        return [{k: getattr(out[i], k) for k in COMPLETION_FIELDS} for i in range(n.value)]
+
+    def replay(self, requests: Sequence[Request], arrival_us: Sequence[float]) -> list:
+        """Submits request i at arrival_us[i] after the call starts; returns the completions."""
+        arr = (_Request * len(requests))()
+        keep = []
+        for i, req in enumerate(requests):
+            r, ranges = req.native()
+            keep.append(ranges)
+            arr[i] = r
+        times = (ctypes.c_double * len(requests))(*[float(t) for t in arrival_us])
+        out = (_Completion * len(requests))()
+        self._check(self._lib.sk_server_replay(self._h, arr, times, len(requests), out), "replay")
+        return [{k: getattr(out[i], k) for k in COMPLETION_FIELDS} for i in range(len(requests))]
 
 
 def radix_argsort_device(keys_ptr: int, count_ptr: int, capacity: int, bits: int, order_ptr: int,
