@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--bits", type=int, default=16, choices=(16, 32))
     p.add_argument("--impl", default="ours", choices=("ours", "reference"))
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batch", action="store_true", help="skip the 64-view batched comparison")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving comparison")
     return p.parse_args()
 
 
@@ -340,10 +342,174 @@ def run_ours(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(cloud, args.bits)
+        if world == 1 and not args.no_batch and args.bits == 16:
+            line["batch64"] = measure_batch(r)
+        if world == 1 and not args.no_serve and args.bits == 16:
+            line["served"] = measure_serve()
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+# ---- batched multi-view: 64 views of the 1M SH3 scene, mixed resolutions ----------------------
+BATCH_VIEWS = 64
+BATCH_SIZES = [(640, 480), (1280, 720), (1920, 1080)]
+
+
+def batch_views(renderer, rotation_deg=0.0):
+    import splatkit_b200 as sk
+    from splatkit_b200 import camera as skcam
+
+    rng = np.random.default_rng(64)
+    sizes = [BATCH_SIZES[i] for i in rng.integers(0, len(BATCH_SIZES), BATCH_VIEWS)]
+    views = []
+    for i, (w, h) in enumerate(sizes):
+        a = math.radians(360.0 * i / BATCH_VIEWS + rotation_deg)
+        eye = np.array([15.0 * math.sin(a), 0.0, 15.0 * math.cos(a)], np.float32)
+        view = skcam.look_at_view(eye, (0.0, 0.0, 0.0))
+        proj = skcam.perspective(math.radians(60.0), w / h, 0.05, 200.0)
+        views.append(sk.BatchView(renderer, sk.Frame(view, proj, eye, [(0, SPLATS)], SH_DEGREE), w, h))
+    return views
+
+
+def measure_batch(renderer):
+    """64 plain per-frame launches (draw + read back each) against the batched form (graph-captured
+    submissions on two lanes, every image read back), same views, images compared bit for bit."""
+    import torch
+
+    import splatkit_b200 as sk
+
+    views = batch_views(renderer)
+    pinned = torch.empty(1920 * 1080 * 4, dtype=torch.uint8, pin_memory=True).numpy()
+    plain_images = []
+    for rounds in range(2):
+        t0 = time.perf_counter()
+        for v in views:
+            renderer.resize(v.width, v.height)
+            renderer.draw(v.frame)
+            renderer.read_image(sk.FORMAT_RGBA8,
+                                out=pinned[:v.width * v.height * 4].reshape(v.height, v.width, 4))
+        plain_s = time.perf_counter() - t0
+    for v in views:  # the reference images, outside the timed rounds
+        renderer.resize(v.width, v.height)
+        renderer.draw(v.frame)
+        plain_images.append(renderer.read_image(sk.FORMAT_RGBA8))
+    rounds = 8
+    with sk.Batch(lanes=2, max_views=BATCH_VIEWS, use_graphs=True) as batch:
+        for k in range(2):
+            batch.wait(batch.submit(batch_views(renderer, k)))
+        t0 = time.perf_counter()
+        tickets = [batch.submit(batch_views(renderer, k % 3)) for k in range(rounds)]
+        for t in tickets[-2:]:
+            batch.wait(t)
+        batch_s = time.perf_counter() - t0
+        gpu_ms = batch.stats(tickets[-1])["gpu_ms"]
+        check = batch.submit(views)
+        same = all(np.array_equal(batch.read_image(check, i), plain_images[i]) for i in range(len(views)))
+    plain_rate = len(views) / plain_s
+    batch_rate = rounds * len(views) / batch_s
+    return {"workload": "64 views of the 1M-splat SH3 scene on a 15 m circle, resolutions drawn "
+                        "from {640x480, 1280x720, 1920x1080} (seed 64)",
+            "plain_views_per_s": plain_rate, "batched_views_per_s": batch_rate,
+            "speedup": batch_rate / plain_rate, "batched_gpu_ms_per_submission": gpu_ms,
+            "images_identical": bool(same),
+            "how": "plain: resize + draw + read_image per view; batched: 8 submissions of 64 views "
+                   "on 2 lanes, CUDA-graph replay, every image copied back; host-timed"}
+
+
+# ---- serving: Poisson requests over 8 resident scenes -----------------------------------------
+SERVE_SCENES = [200_000, 500_000, 1_000_000, 2_000_000, 3_000_000, 4_000_000, 5_000_000, 6_000_000]
+SERVE_SIZES = [(640, 480), (1280, 720), (1920, 1080), (2560, 1440), (3840, 2160)]
+
+
+def serve_trace(count, rate, seed=2000):
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1e6 / rate, count))
+    return arrivals, rng.integers(0, len(SERVE_SCENES), count), rng.integers(0, len(SERVE_SIZES), count), \
+        rng.uniform(0.0, 360.0, count)
+
+
+def measure_serve():
+    """C5: requests at 2000/s (Poisson) over 8 resident scenes (0.2-6M splats, SH3), resolutions
+    640x480..3840x2160, served with continuous batching, against the plain loop on the same trace."""
+    import splatkit_b200 as sk
+    from splatkit_b200 import camera as skcam
+    from splatkit_b200 import synthetic
+
+    renderers = []
+    for i, n in enumerate(SERVE_SCENES):
+        cloud = synthetic.random_cloud(n, seed=100 + i, sh_degree=SH_DEGREE)
+        r = sk.Renderer(64, 64, image_format=sk.FORMAT_RGBA8, time_stages=False)
+        r.apply_render_policy(sk.Policy(sort_depth_bits=16))
+        r.upload_world(cloud, SH_DEGREE)
+        renderers.append(r)
+        del cloud
+    ring = [sk.HostImage(3840, 2160) for _ in range(96)]
+
+    def frame(scene, size, angle):
+        w, h = SERVE_SIZES[size]
+        a = math.radians(angle)
+        eye = np.array([15.0 * math.sin(a), 0.0, 15.0 * math.cos(a)], np.float32)
+        proj = skcam.perspective(math.radians(60.0), w / h, 0.05, 200.0)
+        return sk.Frame(skcam.look_at_view(eye, (0.0, 0.0, 0.0)), proj, eye,
+                        [(0, SERVE_SCENES[scene])], SH_DEGREE), w, h
+
+    def served(rate, count, max_queue_ms):
+        arrivals, scene, size, angle = serve_trace(count, rate)
+        reqs = []
+        for i in range(count):
+            f, w, h = frame(scene[i], size[i], angle[i])
+            reqs.append(sk.Request(int(scene[i]), f, w, h, ring[i % len(ring)]))
+        with sk.Server(lanes=2, max_batch_views=16, max_batch_splats=96_000_000,
+                       max_queue_ms=max_queue_ms) as server:
+            for r in renderers:
+                server.add_scene(r)
+            server.replay(reqs[:32], [0.0] * 32)
+            t0 = time.perf_counter()
+            done = server.replay(reqs, arrivals)
+            elapsed = time.perf_counter() - t0
+        ok = [c for c in done if c["status"] == 0]
+        lat = np.array([c["latency_ms"] for c in ok]) if ok else np.zeros(1)
+        return {"offered_req_per_s": rate, "requests": count, "served": len(ok),
+                "served_req_per_s": len(ok) / elapsed, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)),
+                "mean_batch_views": float(np.mean([c["batch_views"] for c in ok])) if ok else 0.0}
+
+    def plain(rate, count):
+        arrivals, scene, size, angle = serve_trace(count, rate)
+        lat, busy = [], 0.0
+        t0 = time.perf_counter()
+        for i in range(count):
+            wait = arrivals[i] * 1e-6 - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            f, w, h = frame(scene[i], size[i], angle[i])
+            r = renderers[scene[i]]
+            b0 = time.perf_counter()
+            r.resize(w, h)
+            r.draw(f)
+            r.read_image(sk.FORMAT_RGBA8)
+            end = time.perf_counter()
+            busy += end - b0
+            lat.append((end - t0) * 1e3 - arrivals[i] * 1e-3)
+        lat = np.array(lat)
+        return {"offered_req_per_s": rate, "requests": count, "capacity_req_per_s": count / busy,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+
+    out = {"workload": "8 resident scenes of 0.2-6M splats (SH3, 21.7M total), Poisson arrivals, "
+                       "resolutions uniform over 640x480..3840x2160, cameras on a 15 m circle",
+           "served_2000": served(2000.0, 1000, 0.0),
+           "served_2000_shed_8ms": served(2000.0, 1000, 8.0),
+           "served_200": served(200.0, 300, 0.0),
+           "plain_2000": plain(2000.0, 400),
+           "plain_200": plain(200.0, 300)}
+    out["throughput_vs_plain"] = out["served_2000"]["served_req_per_s"] / out["plain_2000"]["capacity_req_per_s"]
+    for x in ring:
+        x.close()
+    for r in renderers:
+        r.close()
+    return out
 
 
 def cpu_baseline(cloud, bits):
