@@ -245,6 +245,23 @@ sk_status sk_batch_view_visible(sk_batch* batch, uint64_t ticket, uint32_t view,
                                 uint32_t* visible);
 sk_status sk_batch_get_stats(sk_batch* batch, uint64_t ticket, sk_batch_stats* out);
 
+/* Launch parameters the autotuner chooses among; none changes a result bit. */
+typedef struct {
+  uint32_t emission_balanced; /* tile binning: 0 walks each warp's splats one by one, 1 spreads
+                                 each warp's tile instances evenly over its lanes */
+  uint32_t sort_tile_keys;    /* keys per radix-sort scatter tile: 2048, 4096 or 6144 */
+  uint32_t lanes;             /* submissions in flight (<= the batch's lanes) */
+  double gpu_ms;              /* autotune: device time of the chosen kernels for the sample */
+  double views_per_s;         /* autotune: throughput with `lanes` in flight, images read back */
+} sk_batch_tuning;
+/* Times the sample views under every emission strategy and sort tile size (device time), then
+ * with 1..lanes submissions in flight (host time, images read back), and keeps the fastest.
+ * Waits for submissions in flight first; their tickets stay readable until their lanes are
+ * reused. */
+sk_status sk_batch_autotune(sk_batch* batch, const sk_batch_view* views, uint32_t count,
+                            sk_batch_tuning* out);
+sk_status sk_batch_set_tuning(sk_batch* batch, const sk_batch_tuning* tuning);
+
 /* ---- serving: continuous batching of render requests --------------------------------------
  * A server holds resident scenes (contexts with flat worlds, added once) and a scheduler thread.
  * Requests are queued as they arrive; whenever one of the server's lanes is free the scheduler

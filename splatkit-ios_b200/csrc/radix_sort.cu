@@ -92,42 +92,45 @@ __device__ __forceinline__ uint32_t matchDigit(uint32_t digit, bool valid) {
   return peers;
 }
 
+template <uint32_t kPer>
 struct ScatterSmem {
   uint32_t warpCount[kWarps][kBins];
   uint32_t digitTotal[kBins];
   uint32_t localOffset[kBins];
   uint32_t globalBase[kBins];
-  uint32_t stage[kTileKeys];
+  uint32_t stage[kThreads * kPer];
   uint32_t warpSums[kWarps];
 };
 
-template <bool kImplicitValues, bool kWriteKeys>
+// kPer keys per thread: tiles of 256 * kPer keys (the tile size the autotuner picks from).
+template <bool kImplicitValues, bool kWriteKeys, uint32_t kPer>
 __global__ void __launch_bounds__(kThreads)
     scatterKernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict__ valuesIn,
                   uint32_t* __restrict__ keysOut, uint32_t* __restrict__ valuesOut,
                   const uint32_t* count, uint32_t capacity, uint32_t shift,
                   const uint32_t* __restrict__ digitBase, uint64_t* status, uint32_t* counters,
                   uint32_t epoch, uint32_t* error) {
-  __shared__ ScatterSmem s;
+  __shared__ ScatterSmem<kPer> s;
+  constexpr uint32_t kTile = kThreads * kPer;
   const uint32_t tile = takeTile(counters);
   const uint32_t n = clampCount(count, capacity);
-  const uint32_t tiles = (n + kTileKeys - 1) / kTileKeys;
+  const uint32_t tiles = (n + kTile - 1) / kTile;
   if (tile < tiles) {
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
     for (uint32_t i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&s.warpCount[0][0])[i] = 0;
-    uint32_t key[kPerThread];
-    const uint32_t first = tile * kTileKeys + warp * (32 * kPerThread) + lane;
+    uint32_t key[kPer];
+    const uint32_t first = tile * kTile + warp * (32 * kPer) + lane;
 #pragma unroll
-    for (uint32_t r = 0; r < kPerThread; ++r) {
+    for (uint32_t r = 0; r < kPer; ++r) {
       const uint32_t e = first + r * 32;
       key[r] = e < n ? keysIn[e] : 0xffffffffu;
     }
     __syncthreads();
     // Rank each key among the equal digits of its warp, row by row (source order).
-    uint32_t rank[kPerThread];
+    uint32_t rank[kPer];
     const uint32_t below = lanemaskLt();
 #pragma unroll
-    for (uint32_t r = 0; r < kPerThread; ++r) {
+    for (uint32_t r = 0; r < kPer; ++r) {
       const bool valid = first + r * 32 < n;
       const uint32_t d = (key[r] >> shift) & 0xffu;
       const uint32_t peers = matchDigit(d, valid);
@@ -176,19 +179,19 @@ __global__ void __launch_bounds__(kThreads)
     s.localOffset[d] = before + inc - total;
     __syncthreads();
     // Local positions, keys staged in digit order.
-    uint32_t pos[kPerThread];
+    uint32_t pos[kPer];
 #pragma unroll
-    for (uint32_t r = 0; r < kPerThread; ++r) {
+    for (uint32_t r = 0; r < kPer; ++r) {
       const bool valid = first + r * 32 < n;
       const uint32_t dd = (key[r] >> shift) & 0xffu;
       pos[r] = valid ? s.localOffset[dd] + s.warpCount[warp][dd] + rank[r] : 0xffffffffu;
       if (valid) s.stage[pos[r]] = key[r];
     }
     __syncthreads();
-    const uint32_t inTile = min(kTileKeys, n - tile * kTileKeys);
-    uint32_t dst[kPerThread];
+    const uint32_t inTile = min(kTile, n - tile * kTile);
+    uint32_t dst[kPer];
 #pragma unroll
-    for (uint32_t r = 0; r < kPerThread; ++r) {
+    for (uint32_t r = 0; r < kPer; ++r) {
       const uint32_t i = threadIdx.x + r * kThreads;
       dst[r] = 0xffffffffu;
       if (i < inTile) {
@@ -206,13 +209,13 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
 #pragma unroll
-    for (uint32_t r = 0; r < kPerThread; ++r) {
+    for (uint32_t r = 0; r < kPer; ++r) {
       const uint32_t e = first + r * 32;
       if (pos[r] != 0xffffffffu) s.stage[pos[r]] = kImplicitValues ? e : valuesIn[e];
     }
     __syncthreads();
 #pragma unroll
-    for (uint32_t r = 0; r < kPerThread; ++r) {
+    for (uint32_t r = 0; r < kPer; ++r) {
       const uint32_t i = threadIdx.x + r * kThreads;
       if (i < inTile && dst[r] != 0xffffffffu) valuesOut[dst[r]] = s.stage[i];
     }
@@ -226,19 +229,23 @@ inline size_t alignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 uint32_t sortTileKeys() { return kTileKeys; }
 
-static uint32_t sortTiles(uint32_t capacity) {
-  return max(1u, (capacity + kTileKeys - 1) / kTileKeys);
+static uint32_t sortTiles(uint32_t capacity, uint32_t tileKeys = kTileKeys) {
+  return max(1u, (capacity + tileKeys - 1) / tileKeys);
 }
 
-size_t sortWorkspaceBytes(uint32_t capacity) {
+static uint32_t tileKeysOf(const SortArgs& a) { return a.tileKeys ? a.tileKeys : kTileKeys; }
+
+size_t sortWorkspaceBytesFor(uint32_t capacity, uint32_t minTileKeys) {
   const size_t n = alignUp(static_cast<size_t>(max(capacity, 1u)) * 4, 256);
   return 3 * n                                             // keysA, keysB, valuesTmp
          + alignUp(2 * kMaxPasses * kBins * 4, 256)        // histogram accumulators + bases
-         + alignUp(static_cast<size_t>(sortTiles(capacity)) * kBins * 8, 256)  // status
+         + alignUp(static_cast<size_t>(sortTiles(capacity, minTileKeys)) * kBins * 8, 256)  // status
          + alignUp((kMaxPasses + 1) * 2 * 4, 256);         // counters
 }
 
-void sortBindWorkspace(SortArgs& a, void* workspace, uint32_t capacity) {
+size_t sortWorkspaceBytes(uint32_t capacity) { return sortWorkspaceBytesFor(capacity, kTileKeys); }
+
+void sortBindWorkspaceFor(SortArgs& a, void* workspace, uint32_t capacity, uint32_t minTileKeys) {
   char* p = static_cast<char*>(workspace);
   const size_t n = alignUp(static_cast<size_t>(max(capacity, 1u)) * 4, 256);
   a.keysA = reinterpret_cast<uint32_t*>(p), p += n;
@@ -246,8 +253,13 @@ void sortBindWorkspace(SortArgs& a, void* workspace, uint32_t capacity) {
   a.valuesTmp = reinterpret_cast<uint32_t*>(p), p += n;
   a.histogram = reinterpret_cast<uint32_t*>(p), p += alignUp(2 * kMaxPasses * kBins * 4, 256);
   a.status = reinterpret_cast<uint64_t*>(p);
-  p += alignUp(static_cast<size_t>(sortTiles(capacity)) * kBins * 8, 256);
+  a.statusTiles = sortTiles(capacity, minTileKeys);
+  p += alignUp(static_cast<size_t>(a.statusTiles) * kBins * 8, 256);
   a.counters = reinterpret_cast<uint32_t*>(p);
+}
+
+void sortBindWorkspace(SortArgs& a, void* workspace, uint32_t capacity) {
+  sortBindWorkspaceFor(a, workspace, capacity, kTileKeys);
 }
 
 cudaError_t sortResetWorkspace(const SortArgs& a, cudaStream_t stream) {
@@ -258,10 +270,13 @@ cudaError_t sortResetWorkspace(const SortArgs& a, cudaStream_t stream) {
 
 cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
   const uint32_t passes = static_cast<uint32_t>(min(max(a.bits, 8), 32) + 7) / 8u;
-  const uint32_t tiles = sortTiles(a.capacity);
+  const uint32_t tileKeys = tileKeysOf(a);
+  if (tileKeys != 2048 && tileKeys != 4096 && tileKeys != 6144) return cudaErrorInvalidValue;
+  const uint32_t tiles = sortTiles(a.capacity, tileKeys);
+  if (tiles > a.statusTiles) return cudaErrorInvalidValue;  // the workspace was bound for larger tiles
   uint32_t* accum = a.histogram;
   uint32_t* bases = a.histogram + kMaxPasses * kBins;
-  const uint32_t histBlocks = min(tiles, 148u * 4u);
+  const uint32_t histBlocks = min(sortTiles(a.capacity), 148u * 4u);
   histogramKernel<<<histBlocks, kThreads, 0, stream>>>(a.keysIn, a.count, a.capacity, passes,
                                                        accum, bases, a.counters);
   const uint32_t* kin = a.keysIn;
@@ -274,16 +289,23 @@ cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
     const uint32_t epoch = (a.epoch + p) & 0x3fffffffu;
     const bool implicit = p == 0 && vin == nullptr;
     const bool writeKeys = kout != nullptr;
-#define SK_SCATTER(IMPLICIT, WRITE)                                                        \
-  scatterKernel<IMPLICIT, WRITE><<<tiles, kThreads, 0, stream>>>(                          \
+#define SK_SCATTER_PER(IMPLICIT, WRITE, PER)                                               \
+  scatterKernel<IMPLICIT, WRITE, PER><<<tiles, kThreads, 0, stream>>>(                     \
       kin, vin, kout, vout, a.count, a.capacity, 8 * p, bases + p * kBins, a.status,      \
       counters, epoch, a.error)
+#define SK_SCATTER(IMPLICIT, WRITE)                                                        \
+  do {                                                                                     \
+    if (tileKeys == 2048) SK_SCATTER_PER(IMPLICIT, WRITE, 8u);                             \
+    else if (tileKeys == 6144) SK_SCATTER_PER(IMPLICIT, WRITE, 24u);                       \
+    else SK_SCATTER_PER(IMPLICIT, WRITE, 16u);                                             \
+  } while (0)
     if (implicit) {
       if (writeKeys) SK_SCATTER(true, true); else SK_SCATTER(true, false);
     } else {
       if (writeKeys) SK_SCATTER(false, true); else SK_SCATTER(false, false);
     }
 #undef SK_SCATTER
+#undef SK_SCATTER_PER
     kin = kout;
     vin = vout;
   }

@@ -81,11 +81,16 @@ struct SortArgs {
   uint32_t* counters;   // 2 * 5 words
   uint32_t epoch;       // uses epoch .. epoch + 3
   uint32_t* error;
+  uint32_t tileKeys;    // keys per scatter tile: 2048, 4096 (0: the default) or 6144
+  uint32_t statusTiles; // tiles the bound status region holds (set by the bind)
 };
 uint32_t sortTileKeys();
 size_t sortWorkspaceBytes(uint32_t capacity);
 // Carves the workspace into the SortArgs fields.
 void sortBindWorkspace(SortArgs& args, void* workspace, uint32_t capacity);
+// The same for sorts that may use tiles as small as minTileKeys keys.
+size_t sortWorkspaceBytesFor(uint32_t capacity, uint32_t minTileKeys);
+void sortBindWorkspaceFor(SortArgs& args, void* workspace, uint32_t capacity, uint32_t minTileKeys);
 cudaError_t launchSort(const SortArgs& args, cudaStream_t stream);
 // Clears the counters and histogram accumulators of a bound workspace.
 cudaError_t sortResetWorkspace(const SortArgs& args, cudaStream_t stream);

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <chrono>
 #include <cstring>
 #include <memory>
 
@@ -73,14 +74,14 @@ sk_status Batch::reserve(BatchLane& l, uint32_t sources, uint32_t instances, uin
   grab(l.projected, size_t{sources} * sizeof(Projected));
   grab(l.spans, size_t{sources} * 16);
   grab(l.order, size_t{sources} * 4);
-  grab(l.sortWorkspace, sortWorkspaceBytes(sources));
+  grab(l.sortWorkspace, sortWorkspaceBytesFor(sources, kMinSortTileKeys));
   grab(l.binSums, size_t{binBlocks(sources)} * 4);
   grab(l.visStatus, size_t{std::max(items, 1u)} * 8);
   grab(l.instKeys, size_t{instances} * 4);
   grab(l.instValues, size_t{instances} * 4);
   grab(l.instKeysSorted, size_t{instances} * 4);
   grab(l.instValuesSorted, size_t{instances} * 4);
-  grab(l.tileSortWorkspace, sortWorkspaceBytes(instances));
+  grab(l.tileSortWorkspace, sortWorkspaceBytesFor(instances, kMinSortTileKeys));
   grab(l.ranges, size_t{std::max(tiles, 1u)} * sizeof(uint2));
   grab(l.viewFirst, size_t{views + 1} * 4);
   grab(l.viewTable, size_t{views} * sizeof(BatchView));
@@ -197,13 +198,13 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
   if (e == cudaSuccess && clearStatus) {
     e = cudaMemsetAsync(l.visStatus.ptr, 0, size_t{l.totalItems} * 8, s);
     SortArgs probe{};
-    sortBindWorkspace(probe, l.sortWorkspace.ptr, l.sources);
+    sortBindWorkspaceFor(probe, l.sortWorkspace.ptr, l.sources, kMinSortTileKeys);
     if (e == cudaSuccess)
-      e = cudaMemsetAsync(probe.status, 0, sortWorkspaceBytes(l.sources) -
+      e = cudaMemsetAsync(probe.status, 0, sortWorkspaceBytesFor(l.sources, kMinSortTileKeys) -
                           (reinterpret_cast<char*>(probe.status) - static_cast<char*>(l.sortWorkspace.ptr)), s);
-    sortBindWorkspace(probe, l.tileSortWorkspace.ptr, l.instances);
+    sortBindWorkspaceFor(probe, l.tileSortWorkspace.ptr, l.instances, kMinSortTileKeys);
     if (e == cudaSuccess)
-      e = cudaMemsetAsync(probe.status, 0, sortWorkspaceBytes(l.instances) -
+      e = cudaMemsetAsync(probe.status, 0, sortWorkspaceBytesFor(l.instances, kMinSortTileKeys) -
                           (reinterpret_cast<char*>(probe.status) - static_cast<char*>(l.tileSortWorkspace.ptr)), s);
   }
   if (e == cudaSuccess) {
@@ -231,7 +232,8 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     a.count = &fc->visible;
     a.capacity = l.sources;
     a.bits = static_cast<int>(bitsFor(uint64_t{l.viewCount} << 16));
-    sortBindWorkspace(a, l.sortWorkspace.ptr, l.sources);
+    sortBindWorkspaceFor(a, l.sortWorkspace.ptr, l.sources, kMinSortTileKeys);
+    a.tileKeys = tuning.sortTileKeys;
     a.epoch = nextEpoch(4);
     a.error = error;
     e = launchSort(a, s);
@@ -263,7 +265,8 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     a.count = &fc->instances;
     a.capacity = l.instances;
     a.bits = static_cast<int>(bitsFor(l.totalTiles));
-    sortBindWorkspace(a, l.tileSortWorkspace.ptr, l.instances);
+    sortBindWorkspaceFor(a, l.tileSortWorkspace.ptr, l.instances, kMinSortTileKeys);
+    a.tileKeys = tuning.sortTileKeys;
     a.epoch = nextEpoch(4);
     a.error = error;
     e = launchSort(a, s);
@@ -429,6 +432,7 @@ sk_status sk_batch_create(const sk_batch_config* config, sk_batch** out) {
   b->tuning.lanes = config->lanes;
   b->tuning.maxViews = config->max_views;
   b->tuning.graphs = config->use_graphs != 0;
+  b->tuning.activeLanes = config->lanes;
   sk_default_policy(&b->policy);
   b->lanes = std::vector<BatchLane>(config->lanes);
   for (auto& l : b->lanes) {
@@ -478,8 +482,10 @@ sk_status sk_batch_submit(sk_batch* handle, const sk_batch_view* views, uint32_t
   SK_BATCH(handle);
   if (!views || count == 0 || count > b->tuning.maxViews)
     return b->fail(SK_E_INVALID, "a submission holds 1 to max_views views");
+  const uint32_t active = std::max(1u, std::min(b->tuning.activeLanes, static_cast<uint32_t>(b->lanes.size())));
+  if (b->nextLane >= active) b->nextLane = 0;
   BatchLane& l = b->lanes[b->nextLane];
-  b->nextLane = (b->nextLane + 1) % static_cast<uint32_t>(b->lanes.size());
+  b->nextLane = (b->nextLane + 1) % active;
   if (l.busy) {
     const sk_status st = b->finish(l, true);
     if (st == SK_E_DEVICE) return st;
@@ -554,6 +560,115 @@ sk_status sk_batch_get_stats(sk_batch* handle, uint64_t ticket, sk_batch_stats* 
   out->gpu_ms = l->gpuMs;
   out->fragments = uint64_t{l->result.fragments_lo} | (uint64_t{l->result.fragments_hi} << 32);
   return st;
+}
+
+}  // extern "C"
+
+// ---- autotuner ---------------------------------------------------------------------------------
+namespace {
+
+// Draws the views once on lane l and waits; the lane is left idle.
+sk_status runOnce(Batch& b, BatchLane& l, const sk_batch_view* views, uint32_t count) {
+  if (l.busy) b.finish(l, true);
+  l.busy = false;
+  sk_status st = b.prepare(l, views, count);
+  if (st == SK_OK) st = b.enqueue(l);
+  if (st != SK_OK) return st;
+  l.busy = true;
+  l.harvested = false;
+  l.ticket = 0;
+  st = b.finish(l, true);
+  l.busy = false;
+  return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+sk_status sk_batch_autotune(sk_batch* handle, const sk_batch_view* views, uint32_t count,
+                            sk_batch_tuning* out) {
+  SK_BATCH(handle);
+  if (!views || count == 0 || count > b->tuning.maxViews || !out)
+    return b->fail(SK_E_INVALID, "autotune needs 1 to max_views views");
+  for (auto& l : b->lanes)
+    if (l.busy) b->finish(l, true);
+  for (auto& l : b->lanes) l.busy = false;
+  const bool graphs = b->tuning.graphs;
+  b->tuning.graphs = false;
+  // 1. kernel shapes, timed on the device: emission strategy x radix tile size
+  double best = 1e30;
+  sk::BatchTuning chosen = b->tuning;
+  sk::BatchLane& lane = b->lanes[0];
+  for (const bool balanced : {false, true}) {
+    for (const uint32_t tileKeys : {2048u, 4096u, 6144u}) {
+      b->tuning.balancedEmit = balanced;
+      b->tuning.sortTileKeys = tileKeys;
+      double ms = 0;
+      for (int rep = 0; rep < 3; ++rep) {  // the first run allocates and warms up
+        const sk_status st = runOnce(*b, lane, views, count);
+        if (st != SK_OK) {
+          b->tuning.graphs = graphs;
+          return st;
+        }
+        if (rep > 0) ms += lane.gpuMs;
+      }
+      if (ms < best) {
+        best = ms;
+        chosen.balancedEmit = balanced;
+        chosen.sortTileKeys = tileKeys;
+      }
+    }
+  }
+  b->tuning.balancedEmit = chosen.balancedEmit;
+  b->tuning.sortTileKeys = chosen.sortTileKeys;
+  // 2. submissions in flight, timed on the host with every image copied back
+  double bestRate = 0;
+  uint32_t bestLanes = 1;
+  for (uint32_t n = 1; n <= b->lanes.size(); ++n) {
+    b->tuning.activeLanes = n;
+    b->nextLane = 0;
+    const uint32_t rounds = 2 * n + 2;
+    std::vector<uint64_t> tickets;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (uint32_t k = 0; k < rounds; ++k) {
+      uint64_t t = 0;
+      const sk_status st = sk_batch_submit(handle, views, count, &t);
+      if (st != SK_OK) {
+        b->tuning.graphs = graphs;
+        return st;
+      }
+      tickets.push_back(t);
+    }
+    for (uint32_t k = rounds - std::min(rounds, n); k < rounds; ++k) sk_batch_wait(handle, tickets[k]);
+    const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const double rate = rounds * count / s;
+    if (rate > bestRate * 1.03) {  // more lanes only when clearly faster
+      bestRate = rate;
+      bestLanes = n;
+    }
+  }
+  b->tuning.activeLanes = bestLanes;
+  b->tuning.graphs = graphs;
+  b->nextLane = 0;
+  out->emission_balanced = chosen.balancedEmit ? 1u : 0u;
+  out->sort_tile_keys = chosen.sortTileKeys;
+  out->lanes = bestLanes;
+  out->gpu_ms = best / 2.0;
+  out->views_per_s = bestRate;
+  return SK_OK;
+}
+
+sk_status sk_batch_set_tuning(sk_batch* handle, const sk_batch_tuning* t) {
+  SK_BATCH(handle);
+  if (!t || (t->sort_tile_keys != 2048 && t->sort_tile_keys != 4096 && t->sort_tile_keys != 6144) ||
+      t->lanes == 0 || t->lanes > b->lanes.size())
+    return b->fail(SK_E_INVALID, "tuning out of range");
+  b->tuning.balancedEmit = t->emission_balanced != 0;
+  b->tuning.sortTileKeys = t->sort_tile_keys;
+  b->tuning.activeLanes = t->lanes;
+  b->nextLane = 0;
+  return SK_OK;
 }
 
 }  // extern "C"

@@ -19,12 +19,16 @@
 
 namespace sk {
 
+inline constexpr uint32_t kMinSortTileKeys = 2048;  // lane sort workspaces fit every tile size
+
 // Tunable launch parameters of a batch (the autotuner picks among them).
 struct BatchTuning {
-  uint32_t lanes = 2;        // submissions in flight
-  uint32_t maxViews = 64;    // views per internal pass (a submission larger than this is split)
-  bool graphs = false;       // replay captured stage sequences
-  bool balancedEmit = true;  // binning emission strategy (BinArgs::balanced)
+  uint32_t lanes = 2;           // lanes created
+  uint32_t activeLanes = 2;     // lanes submissions rotate over (<= lanes)
+  uint32_t maxViews = 64;       // views one submission may hold
+  bool graphs = false;          // replay captured stage sequences
+  bool balancedEmit = true;     // binning emission strategy (BinArgs::balanced)
+  uint32_t sortTileKeys = 4096; // keys per radix scatter tile: 2048, 4096 or 6144
 };
 
 struct BatchLane {

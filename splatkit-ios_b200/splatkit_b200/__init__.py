@@ -127,6 +127,11 @@ class _Completion(ctypes.Structure):
                 ("latency_ms", ctypes.c_double)]
 
 
+class _BatchTuning(ctypes.Structure):
+    _fields_ = [("emission_balanced", ctypes.c_uint32), ("sort_tile_keys", ctypes.c_uint32),
+                ("lanes", ctypes.c_uint32), ("gpu_ms", ctypes.c_double), ("views_per_s", ctypes.c_double)]
+
+
 class _Policy(ctypes.Structure):
     _fields_ = [("lod_error_pixels", ctypes.c_float), ("lod_splat_limit", ctypes.c_uint32),
                 ("alpha_threshold", ctypes.c_float), ("subpixel_threshold", ctypes.c_float),
@@ -214,6 +219,9 @@ _SIGNATURES = {
     "sk_batch_view_visible": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
                                                ctypes.POINTER(ctypes.c_uint32)]),
     "sk_batch_get_stats": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(_BatchStats)]),
+    "sk_batch_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_BatchView), ctypes.c_uint32,
+                                           ctypes.POINTER(_BatchTuning)]),
+    "sk_batch_set_tuning": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_BatchTuning)]),
     "sk_server_create": (ctypes.c_int32, [ctypes.POINTER(_ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
     "sk_server_destroy": (None, [ctypes.c_void_p]),
     "sk_server_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
@@ -587,6 +595,29 @@ class Batch:
         if len(self._sizes) > 64:
             self._sizes.pop(next(iter(self._sizes)))
         return ticket.value
+
+    @staticmethod
+    def _views(views):
+        arr = (_BatchView * len(views))()
+        keep = []
+        for i, v in enumerate(views):
+            f, ranges = v.frame.native()
+            keep.append(ranges)
+            arr[i].world = v.renderer._h
+            arr[i].frame = f
+            arr[i].width, arr[i].height = v.width, v.height
+        return arr, keep
+
+    def autotune(self, views: Sequence[BatchView]) -> dict:
+        """Times the sample under every launch shape and keeps the fastest (sk_batch_autotune)."""
+        arr, keep = self._views(views)
+        t = _BatchTuning()
+        self._check(self._lib.sk_batch_autotune(self._h, arr, len(views), ctypes.byref(t)), "autotune")
+        return {name: getattr(t, name) for name, _ in _BatchTuning._fields_}
+
+    def set_tuning(self, emission_balanced: int, sort_tile_keys: int, lanes: int):
+        t = _BatchTuning(emission_balanced, sort_tile_keys, lanes, 0.0, 0.0)
+        self._check(self._lib.sk_batch_set_tuning(self._h, ctypes.byref(t)), "set_tuning")
 
     def poll(self, ticket: int) -> bool:
         done = ctypes.c_int32()
