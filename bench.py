@@ -396,12 +396,13 @@ def measure_batch(renderer):
         renderer.draw(v.frame)
         plain_images.append(renderer.read_image(sk.FORMAT_RGBA8))
     rounds = 8
-    with sk.Batch(lanes=2, max_views=BATCH_VIEWS, use_graphs=True) as batch:
+    with sk.Batch(lanes=3, max_views=BATCH_VIEWS, use_graphs=True) as batch:
+        tuning = batch.autotune(views)
         for k in range(2):
             batch.wait(batch.submit(batch_views(renderer, k)))
         t0 = time.perf_counter()
         tickets = [batch.submit(batch_views(renderer, k % 3)) for k in range(rounds)]
-        for t in tickets[-2:]:
+        for t in tickets[-int(tuning["lanes"]):]:  # each lane's last submission
             batch.wait(t)
         batch_s = time.perf_counter() - t0
         gpu_ms = batch.stats(tickets[-1])["gpu_ms"]
@@ -413,9 +414,10 @@ def measure_batch(renderer):
                         "from {640x480, 1280x720, 1920x1080} (seed 64)",
             "plain_views_per_s": plain_rate, "batched_views_per_s": batch_rate,
             "speedup": batch_rate / plain_rate, "batched_gpu_ms_per_submission": gpu_ms,
-            "images_identical": bool(same),
-            "how": "plain: resize + draw + read_image per view; batched: 8 submissions of 64 views "
-                   "on 2 lanes, CUDA-graph replay, every image copied back; host-timed"}
+            "images_identical": bool(same), "autotuned": tuning,
+            "how": "plain: resize + draw + read_image per view; batched: autotuned (emission, "
+                   "radix tile, lanes of 3), then 8 submissions of 64 views, CUDA-graph replay, "
+                   "every image copied back; host-timed"}
 
 
 # ---- serving: Poisson requests over 8 resident scenes -----------------------------------------

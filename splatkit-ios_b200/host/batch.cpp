@@ -628,7 +628,14 @@ sk_status sk_batch_autotune(sk_batch* handle, const sk_batch_view* views, uint32
   for (uint32_t n = 1; n <= b->lanes.size(); ++n) {
     b->tuning.activeLanes = n;
     b->nextLane = 0;
-    const uint32_t rounds = 2 * n + 2;
+    for (uint32_t k = 0; k < n; ++k) {  // every lane allocates and warms up untimed
+      const sk_status st = runOnce(*b, b->lanes[k], views, count);
+      if (st != SK_OK) {
+        b->tuning.graphs = graphs;
+        return st;
+      }
+    }
+    const uint32_t rounds = 3 * n + 3;
     std::vector<uint64_t> tickets;
     const auto t0 = std::chrono::steady_clock::now();
     for (uint32_t k = 0; k < rounds; ++k) {
