@@ -10,8 +10,8 @@
 // termination when the remaining transmittance drops below `cutoff`.
 //
 // A block of 128 threads owns a tile; each thread owns two horizontally adjacent pixels and each
-// warp an 8x8-pixel quadrant. The block walks the tile's list in batches of 128 records: thread i
-// fetches record i (two 128-bit loads), turns it into the coverage form (pixel centre, inverse
+// warp an 8x8-pixel quadrant. The block walks the tile's list in batches of 256 records: thread i
+// fetches records i and i + 128 (two 128-bit loads each), turns it into the coverage form (pixel centre, inverse
 // axes, radius, log cutoff, colour) in shared memory and marks which of the four quadrants its
 // quad overlaps (separating-axis test). Each warp compacts, by ballot, the batch entries that
 // reach it and sweeps only those, both of its pixels per entry. The coverage decision (quad bound and 1/255 cutoff)
@@ -27,6 +27,7 @@ namespace {
 
 constexpr uint32_t kThreads = kTileSize * kTileSize / 2;  // 128: two pixels per thread
 constexpr uint32_t kWarps = kThreads / 32;
+constexpr uint32_t kEntries = 2 * kThreads;  // list entries staged per batch (two per thread)
 constexpr uint32_t kQuadrant = kTileSize / 2;  // each warp owns an 8x8 quadrant
 
 struct alignas(16) Splat2D {
@@ -37,9 +38,9 @@ struct alignas(16) Splat2D {
 static_assert(sizeof(Splat2D) == 48, "Splat2D is three 16-byte words");
 
 struct CompositeSmem {
-  Splat2D splat[kThreads];
-  uint8_t list[kWarps][kThreads];  // per warp: batch entries whose quad reaches its quadrant
-  uint8_t reach[kThreads];         // per entry: bit w set when it reaches quadrant w
+  Splat2D splat[kEntries];
+  uint8_t list[kWarps][kEntries];  // per warp: batch entries whose quad reaches its quadrant
+  uint8_t reach[kEntries];         // per entry: bit w set when it reaches quadrant w
 };
 
 // Fills the coverage form; returns the bitmask of the warp quadrants its quad overlaps.
@@ -200,16 +201,19 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   p.done0 = !(col < t.width && row < t.height);
   p.done1 = !(col + 1 < t.width && row < t.height);
   uint32_t blended = 0, loaded = 0;
-  for (uint32_t start = range.x; start < range.y; start += kThreads) {
-    const uint32_t inBatch = min(kThreads, range.y - start);
+  for (uint32_t start = range.x; start < range.y; start += kEntries) {
+    const uint32_t inBatch = min(kEntries, range.y - start);
     loaded += inBatch;
-    if (threadIdx.x < inBatch) {
-      const uint32_t v = a.values[start + threadIdx.x];
-      const uint4* p = reinterpret_cast<const uint4*>(a.projected + v);
-      Splat2D s;
-      sm.reach[threadIdx.x] =
-          static_cast<uint8_t>(coverageForm(__ldg(p), __ldg(p + 1), halfW, halfH, tileX, tileTop, s));
-      sm.splat[threadIdx.x] = s;
+#pragma unroll
+    for (uint32_t e = threadIdx.x; e < kEntries; e += kThreads) {
+      if (e < inBatch) {
+        const uint32_t v = a.values[start + e];
+        const uint4* p = reinterpret_cast<const uint4*>(a.projected + v);
+        Splat2D s;
+        sm.reach[e] =
+            static_cast<uint8_t>(coverageForm(__ldg(p), __ldg(p + 1), halfW, halfH, tileX, tileTop, s));
+        sm.splat[e] = s;
+      }
     }
     __syncthreads();
     if (!__all_sync(0xffffffffu, p.done0 && p.done1)) {
