@@ -366,7 +366,7 @@ __device__ __forceinline__ void copyOutTile(const VisibilitySmem& s, uint32_t* k
 }
 
 template <int D, bool kKey16, bool kIndexed>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     visibilityKernel(const Camera* __restrict__ camera, const __grid_constant__ VisibilityArgs a) {
   __shared__ VisibilitySmem s;
   __shared__ Camera cam;
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kThreads)
 // where that view starts. Keys carry the view id above the 16-bit depth key, so one stable
 // sort orders all views at once.
 template <int D>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     visibilityBatchKernel(const __grid_constant__ BatchVisibilityArgs a) {
   __shared__ VisibilitySmem s;
   __shared__ Camera cam;
