@@ -122,7 +122,7 @@ sk_status Context::reserveScratch(FrameScratch& f, uint32_t sources, uint32_t in
   grab(f.instValues, size_t{instances} * 4);
   grab(f.instKeysSorted, size_t{instances} * 4);
   grab(f.instValuesSorted, size_t{instances} * 4);
-  grab(f.tileSortWorkspace, sortWorkspaceBytes(instances));
+  grab(f.tileSortWorkspace, sortWorkspaceBytesFor(instances, kTileSortTileKeys));
   grab(f.ranges, size_t{maxTiles} * sizeof(uint2));
   grab(f.rangeBuffer, size_t{kMaxRanges} * sizeof(Range));
   grab(f.rangeStarts, size_t{kMaxRanges + 1} * 4);
@@ -334,7 +334,8 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     a.count = &fc->instances;
     a.capacity = f.instanceCapacity;
     a.bits = 16;
-    sortBindWorkspace(a, f.tileSortWorkspace.ptr, f.instanceCapacity);
+    sortBindWorkspaceFor(a, f.tileSortWorkspace.ptr, f.instanceCapacity, kTileSortTileKeys);
+    a.tileKeys = kTileSortTileKeys;
     a.epoch = nextEpoch(4);
     a.error = error;
     e = launchSort(a, s);

@@ -20,6 +20,8 @@ namespace sk {
 inline constexpr uint32_t kMaxLodBudgetPublic = 4000000;  // MetalLodSelection.h:18
 inline constexpr uint32_t kMaxRanges = 65536;             // MetalVisibilityPass.h:72
 inline constexpr float kTransmittanceCutoff = 1e-4f;
+// Scatter tile size of the plain frame's tile sort (measured: 4096 beats 2048 at 4.5M pairs).
+inline constexpr uint32_t kTileSortTileKeys = 4096;
 inline int hostThreadsPublic() {
   return static_cast<int>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
 }
