@@ -40,7 +40,7 @@ ORBIT_FRAMES = 120
 L2_FLUSH_BYTES = 256 << 20
 
 
-def parse():
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=60)
@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch", action="store_true", help="skip the 64-view batched comparison")
     p.add_argument("--no-serve", action="store_true", help="skip the serving comparison")
-    return p.parse_args()
+    return p.parse_args(argv)
 
 
 def workload_config(bits):
@@ -169,6 +169,29 @@ def measured_peaks():
 
 
 # ---- CPU baseline (oracle port of the path, all host threads) ----------------------------------
+# ---- replicas (one process per GPU, no exchange step) ------------------------------------------
+def replica_frame(step, rank):
+    """The orbit frame a replica draws at a step: ranks start 37 frames apart."""
+    return step + rank * 37
+
+
+def max_over_ranks(value, world, device="cpu"):
+    """The largest of every rank's value (the job's time is its slowest rank's); one rank: itself."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(steps, world, seconds):
+    """Whole-job frames/s: every rank drew `steps` frames within the slowest rank's time."""
+    return steps * world / seconds
+
+
 def cpu_frame(cloud_packed, sh_packed, sh_stride, view, proj, eye, bits, threads, width=WIDTH,
               height=HEIGHT, pixel_rows=None):
     from oracle.oracle import Oracle
@@ -249,7 +272,7 @@ def run_ours(args):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{device}")
 
     def frame(step):
-        view, proj, eye = frame_inputs(step + rank * 37)
+        view, proj, eye = frame_inputs(replica_frame(step, rank))
         r.draw(sk.Frame(view, proj, eye, [(0, SPLATS)], SH_DEGREE))
 
     for step in range(args.warmup):
@@ -274,13 +297,10 @@ def run_ours(args):
             stages[k].append(s[k])
         stats_list.append(s)
     torch.cuda.synchronize()
-    total_ms = float(sum(per_frame))
+    total_ms = max_over_ranks(sum(per_frame), world, f"cuda:{device}")
     if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{device}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
         torch.distributed.barrier()
-    value = args.steps * world / (total_ms / 1000.0)
+    value = aggregate_rate(args.steps, world, total_ms / 1000.0)
 
     # e2e: the public calls with the image read into pinned host memory, host-timed
     pinned = torch.empty((HEIGHT, WIDTH, 4), dtype=torch.uint8, pin_memory=True)
@@ -296,11 +316,8 @@ def run_ours(args):
         r.read_image(sk.FORMAT_RGBA8, out=host_image)
     e2e_s = time.perf_counter() - t0
     clocks.__exit__(None, None, None)
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{device}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = args.steps * world / e2e_s
+    e2e_s = max_over_ranks(e2e_s, world, f"cuda:{device}")
+    e2e_value = aggregate_rate(args.steps, world, e2e_s)
 
     if rank == 0:
         mean = {k: float(np.mean(v)) for k, v in stages.items()}
