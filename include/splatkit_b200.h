@@ -167,6 +167,32 @@ int32_t sk_gpu_failed(sk_context* ctx);                                         
 sk_status sk_upload_world(sk_context* ctx, const sk_cloud_view* cloud, int32_t max_sh_degree);
 sk_status sk_upload_lod_world(sk_context* ctx, const sk_lod_view* tree, int32_t max_sh_degree,
                               uint32_t budget);
+/* .lodsplat files (splat-core/include/splat/lod/LodFile.h:12-36): the LOD tree format the
+ * reference's offline builder writes (version 1, or 2 with selection data). */
+typedef struct {
+  uint32_t version;
+  uint32_t node_count, leaf_count;
+  int32_t sh_degree;
+  uint32_t depth;             /* refinement rounds (the tree's depth) */
+  uint32_t cluster_count;     /* version 2 */
+  uint32_t leaf_ref_count;    /* version 2 */
+  float bounds_min[3], bounds_max[3];
+} sk_lodsplat_header;
+/* readLodSplatHeader (LodFile.cpp:335-360): the header, checked against the file length. */
+sk_status sk_lodsplat_read_header(const void* data, size_t size, sk_lodsplat_header* out);
+/* decodeLodSplat (LodFile.cpp:362-423) into caller arrays sized from the header (any may be
+ * NULL): positions 3n, covariances 6n, colors 3n, alphas n, sh 3((d+1)^2-1)n for
+ * d = min(file degree, max_sh_degree), layout n, clusters and leaves (version 2). Checks the
+ * header, the topology and depth, and the attribute ranges. */
+sk_status sk_lodsplat_decode(const void* data, size_t size, int32_t max_sh_degree, float* positions,
+                             float* covariances, float* colors, float* alphas, float* sh,
+                             sk_lod_node* layout, sk_lod_cluster* clusters, uint32_t* leaves);
+/* The file (in memory, or mapped from `path`) decoded and uploaded as sk_upload_lod_world
+ * would; a version-1 file gets its selection data built at upload. */
+sk_status sk_upload_lodsplat(sk_context* ctx, const void* data, size_t size, int32_t max_sh_degree,
+                             uint32_t budget);
+sk_status sk_upload_lodsplat_file(sk_context* ctx, const char* path, int32_t max_sh_degree,
+                                  uint32_t budget);
 sk_status sk_create_slab(sk_context* ctx, uint32_t capacity, int32_t sh_degree);
 sk_status sk_upload_tile(sk_context* ctx, uint32_t offset, const sk_cloud_view* cloud);
 sk_status sk_world_info(sk_context* ctx, uint32_t* count, int32_t* sh_degree);

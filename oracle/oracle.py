@@ -300,6 +300,37 @@ class Reference:
         finally:
             self.lib.skref_free_tree(h)
 
+    def write_lodsplat(self, cloud, path: str, octree_depth: int = 0, cluster_leaves: int = 0,
+                       selection: bool = True) -> dict:
+        """Builds the tree with the reference builder, writes it as a .lodsplat (version 2 with
+        selection data, else 1) and returns its arrays."""
+        lo = None if cloud.bounds_min is None else np.ascontiguousarray(cloud.bounds_min, np.float32)
+        hi = None if cloud.bounds_max is None else np.ascontiguousarray(cloud.bounds_max, np.float32)
+        sh = None if cloud.sh is None else np.ascontiguousarray(cloud.sh, np.float32)
+        h = self.lib.skref_build_lod_tree(_p(cloud.positions), _p(cloud.covariances),
+                                          _p(cloud.colors), _p(cloud.alphas), _p(sh), cloud.count,
+                                          cloud.sh_degree, _p(lo), _p(hi), octree_depth,
+                                          cluster_leaves)
+        try:
+            if selection:
+                self.lib.skref_tree_build_selection(h)
+            if self.lib.skref_write_lodsplat(h, str(path).encode()) != 0:
+                raise RuntimeError("reference writeLodSplat failed")
+            return self._tree_arrays(h)
+        finally:
+            self.lib.skref_free_tree(h)
+
+    def decode_lodsplat(self, data: bytes, max_sh_degree: int = 3):
+        """The reference decoder's arrays, or None when it rejects the file."""
+        buf = np.frombuffer(data, np.uint8)
+        h = self.lib.skref_decode_lodsplat(buf.ctypes.data, len(buf), max_sh_degree)
+        if not h:
+            return None
+        try:
+            return self._tree_arrays(h)
+        finally:
+            self.lib.skref_free_tree(h)
+
     def make_tree(self, nodes_cloud, layout: np.ndarray, leaf_count: int,
                   selection: bool = True) -> dict:
         layout = np.ascontiguousarray(layout, LOD_NODE_DTYPE)

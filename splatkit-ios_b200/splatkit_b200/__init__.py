@@ -132,6 +132,14 @@ class _BatchTuning(ctypes.Structure):
                 ("lanes", ctypes.c_uint32), ("gpu_ms", ctypes.c_double), ("views_per_s", ctypes.c_double)]
 
 
+class _LodsplatHeader(ctypes.Structure):
+    _fields_ = [("version", ctypes.c_uint32), ("node_count", ctypes.c_uint32),
+                ("leaf_count", ctypes.c_uint32), ("sh_degree", ctypes.c_int32),
+                ("depth", ctypes.c_uint32), ("cluster_count", ctypes.c_uint32),
+                ("leaf_ref_count", ctypes.c_uint32), ("bounds_min", ctypes.c_float * 3),
+                ("bounds_max", ctypes.c_float * 3)]
+
+
 class _Policy(ctypes.Structure):
     _fields_ = [("lod_error_pixels", ctypes.c_float), ("lod_splat_limit", ctypes.c_uint32),
                 ("alpha_threshold", ctypes.c_float), ("subpixel_threshold", ctypes.c_float),
@@ -222,6 +230,11 @@ _SIGNATURES = {
     "sk_batch_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_BatchView), ctypes.c_uint32,
                                            ctypes.POINTER(_BatchTuning)]),
     "sk_batch_set_tuning": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_BatchTuning)]),
+    "sk_lodsplat_read_header": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(_LodsplatHeader)]),
+    "sk_lodsplat_decode": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32] + [ctypes.c_void_p] * 8),
+    "sk_upload_lodsplat": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
+                                            ctypes.c_uint32]),
+    "sk_upload_lodsplat_file": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_uint32]),
     "sk_server_create": (ctypes.c_int32, [ctypes.POINTER(_ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
     "sk_server_destroy": (None, [ctypes.c_void_p]),
     "sk_server_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
@@ -450,6 +463,16 @@ class Renderer:
         v = tree.view()
         self._check(self._lib.sk_upload_lod_world(self._h, ctypes.byref(v), max_sh_degree, budget),
                     "LOD upload")
+
+    def upload_lodsplat(self, source, max_sh_degree: int, budget: int):
+        """A .lodsplat file (a path, read by mapping it) or its bytes, decoded and uploaded."""
+        if isinstance(source, (bytes, bytearray, memoryview)):
+            buf = np.frombuffer(source, np.uint8)
+            self._check(self._lib.sk_upload_lodsplat(self._h, buf.ctypes.data, len(buf), max_sh_degree,
+                                                     budget), "lodsplat upload")
+        else:
+            self._check(self._lib.sk_upload_lodsplat_file(self._h, os.fsencode(str(source)), max_sh_degree,
+                                                          budget), "lodsplat upload")
 
     def create_slab(self, capacity: int, sh_degree: int):
         self._check(self._lib.sk_create_slab(self._h, capacity, sh_degree), "slab")
@@ -760,6 +783,41 @@ class Server:
         out = (_Completion * len(requests))()
         self._check(self._lib.sk_server_replay(self._h, arr, times, len(requests), out), "replay")
         return [{k: getattr(out[i], k) for k in COMPLETION_FIELDS} for i in range(len(requests))]
+
+
+# ---- .lodsplat files -------------------------------------------------------------------------
+def lodsplat_header(data: bytes) -> dict:
+    """readLodSplatHeader: the header fields, or SplatError when the file is not valid."""
+    buf = np.frombuffer(data, np.uint8)
+    h = _LodsplatHeader()
+    st = library().sk_lodsplat_read_header(buf.ctypes.data, len(buf), ctypes.byref(h))
+    if st != SK_OK:
+        raise SplatError(st, "not a valid LODSPLAT header")
+    out = {name: getattr(h, name) for name, _ in _LodsplatHeader._fields_}
+    out["bounds_min"], out["bounds_max"] = list(h.bounds_min), list(h.bounds_max)
+    return out
+
+
+def lodsplat_decode(data: bytes, max_sh_degree: int = 3) -> LodTree:
+    """decodeLodSplat into a LodTree (selection data from a version-2 file)."""
+    hd = lodsplat_header(data)
+    n, degree = hd["node_count"], min(hd["sh_degree"], max(0, min(max_sh_degree, 3)))
+    coeffs = 3 * ((degree + 1) ** 2 - 1)
+    pos, cov = np.empty((n, 3), np.float32), np.empty((n, 6), np.float32)
+    col, alp = np.empty((n, 3), np.float32), np.empty(n, np.float32)
+    sh = np.empty((n, coeffs), np.float32) if coeffs else None
+    layout = np.empty(n, LOD_NODE_DTYPE)
+    clusters = np.empty(hd["cluster_count"], LOD_CLUSTER_DTYPE) if hd["cluster_count"] else None
+    leaves = np.empty(hd["leaf_ref_count"], np.uint32) if hd["leaf_ref_count"] else None
+    buf = np.frombuffer(data, np.uint8)
+    ptrs = [a.ctypes.data if a is not None else None for a in (pos, cov, col, alp, sh, layout, clusters, leaves)]
+    st = library().sk_lodsplat_decode(buf.ctypes.data, len(buf), max_sh_degree, *ptrs)
+    if st != SK_OK:
+        raise SplatError(st, "LODSPLAT rejected")
+    cloud = Cloud(pos, cov, col, alp, sh_degree=degree, sh=sh,
+                  bounds_min=np.array(hd["bounds_min"], np.float32),
+                  bounds_max=np.array(hd["bounds_max"], np.float32))
+    return LodTree(cloud, layout, hd["leaf_count"], clusters, leaves)
 
 
 def radix_argsort_device(keys_ptr: int, count_ptr: int, capacity: int, bits: int, order_ptr: int,
