@@ -193,6 +193,24 @@ sk_status sk_upload_lodsplat(sk_context* ctx, const void* data, size_t size, int
                              uint32_t budget);
 sk_status sk_upload_lodsplat_file(sk_context* ctx, const char* path, int32_t max_sh_degree,
                                   uint32_t budget);
+/* writeLodSplat (LodFile.cpp:425-458): version 2 when the tree has selection data, else 1;
+ * refuses an existing path. */
+sk_status sk_write_lodsplat(const sk_lod_view* tree, const float* bounds_min,
+                            const float* bounds_max, const char* path);
+
+/* buildLodTree (splat-core/src/lod/LodTree.cpp:308-330, LodTree.h:58-75) on the host: the
+ * cloud's splats become the leaves of an octree of merged nodes, laid out breadth first; the
+ * same tree bit for bit as the reference's builder given the same bounds. octree_depth 0: 21;
+ * cluster_leaves 0: 32. bounds NULL: the positions' own box. build_selection: also build the
+ * selection data (buildLodSelectionData). The tree is read through sk_lod_tree_view (pointers
+ * valid until sk_lod_tree_free). */
+typedef struct sk_lod_tree sk_lod_tree;
+sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
+                            const float* bounds_max, uint32_t octree_depth, uint32_t cluster_leaves,
+                            int32_t build_selection, sk_lod_tree** out);
+sk_status sk_lod_tree_view(const sk_lod_tree* tree, sk_lod_view* out, float* bounds_min,
+                           float* bounds_max);
+void sk_lod_tree_free(sk_lod_tree* tree);
 sk_status sk_create_slab(sk_context* ctx, uint32_t capacity, int32_t sh_degree);
 sk_status sk_upload_tile(sk_context* ctx, uint32_t offset, const sk_cloud_view* cloud);
 sk_status sk_world_info(sk_context* ctx, uint32_t* count, int32_t* sh_degree);

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -239,3 +240,69 @@ sk_status sk_upload_lodsplat_file(sk_context* ctx, const char* path, int32_t max
 }
 
 }  // extern "C"
+
+// writeLodSplat (LodFile.cpp:425-458): the header, the node records, and for a tree with
+// selection data the clusters and leaf references (version 2). Refuses an existing path.
+extern "C" sk_status sk_write_lodsplat(const sk_lod_view* tree, const float* bounds_min,
+                                       const float* bounds_max, const char* path) {
+  if (!tree || !tree->layout || !path || !bounds_min || !bounds_max || tree->node_count == 0 ||
+      tree->nodes.count != tree->node_count)
+    return SK_E_INVALID;
+  const int degree = tree->nodes.sh ? std::max(0, std::min(tree->nodes.sh_degree, 3)) : 0;
+  const int64_t depth = sk::host::lodDepth(reinterpret_cast<const sk::LodNode*>(tree->layout),
+                                           tree->node_count, tree->leaf_count, nullptr);
+  if (depth < 0) return SK_E_INVALID;
+  const bool selection = tree->cluster_count > 0 && tree->clusters && tree->leaves;
+  const size_t n = tree->node_count, sh = sk::shFloats(degree);
+  const size_t stride = sk::kNodeFixedBytes + sh * 4;
+  std::vector<uint8_t> out(sk::kHeader + n * stride +
+                           (selection ? tree->cluster_count * sk::kClusterBytes + tree->leaf_ref_count * 4 : 0));
+  auto put = [&](size_t at, uint32_t v) {
+    for (int j = 0; j < 4; ++j) out[at + j] = static_cast<uint8_t>(v >> (8 * j));
+  };
+  auto putF = [&](size_t at, float f) {
+    uint32_t bits;
+    std::memcpy(&bits, &f, 4);
+    put(at, bits);
+  };
+  std::memcpy(out.data(), sk::kMagic, 8);
+  put(8, selection ? 2u : 1u);
+  put(12, tree->node_count);
+  put(16, tree->leaf_count);
+  put(20, static_cast<uint32_t>(degree));
+  put(24, static_cast<uint32_t>(depth));
+  put(28, selection ? tree->cluster_count : 0u);
+  for (int j = 0; j < 3; ++j) {
+    putF(32 + j * 4, bounds_min[j]);
+    putF(44 + j * 4, bounds_max[j]);
+  }
+  put(56, selection ? tree->leaf_ref_count : 0u);
+  put(60, selection ? static_cast<uint32_t>(sk::kClusterBytes) : 0u);
+  for (size_t i = 0; i < n; ++i) {
+    const size_t p = sk::kHeader + i * stride;
+    const sk_lod_node& node = tree->layout[i];
+    for (int j = 0; j < 3; ++j) putF(p + j * 4, node.position[j]);
+    putF(p + 12, node.size);
+    put(p + 16, node.child_start);
+    put(p + 20, node.child_count);
+    for (int j = 0; j < 6; ++j) putF(p + 24 + j * 4, tree->nodes.covariances[i * 6 + j]);
+    for (int j = 0; j < 3; ++j) putF(p + 48 + j * 4, tree->nodes.colors[i * 3 + j]);
+    putF(p + 60, tree->nodes.alphas[i]);
+    for (size_t j = 0; j < sh; ++j) putF(p + sk::kNodeFixedBytes + j * 4, tree->nodes.sh[i * sh + j]);
+  }
+  if (selection) {
+    size_t p = sk::kHeader + n * stride;
+    for (uint32_t k = 0; k < tree->cluster_count; ++k)
+      for (size_t j = 0; j < sk::kClusterBytes / 4; ++j) {
+        uint32_t word;
+        std::memcpy(&word, reinterpret_cast<const uint8_t*>(tree->clusters + k) + j * 4, 4);
+        put(p + k * sk::kClusterBytes + j * 4, word);
+      }
+    p += size_t{tree->cluster_count} * sk::kClusterBytes;
+    for (uint32_t k = 0; k < tree->leaf_ref_count; ++k) put(p + k * 4, tree->leaves[k]);
+  }
+  FILE* f = std::fopen(path, "wbx");
+  if (!f) return SK_E_INVALID;
+  const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+  return (std::fclose(f) == 0 && ok) ? SK_OK : SK_E_INVALID;
+}

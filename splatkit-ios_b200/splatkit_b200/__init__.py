@@ -235,6 +235,11 @@ _SIGNATURES = {
     "sk_upload_lodsplat": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
                                             ctypes.c_uint32]),
     "sk_upload_lodsplat_file": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_uint32]),
+    "sk_write_lodsplat": (ctypes.c_int32, [ctypes.POINTER(_LodView), _f32p, _f32p, ctypes.c_char_p]),
+    "sk_build_lod_tree": (ctypes.c_int32, [ctypes.POINTER(_Cloud), _f32p, _f32p, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "sk_lod_tree_view": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_LodView), _f32p, _f32p]),
+    "sk_lod_tree_free": (None, [ctypes.c_void_p]),
     "sk_server_create": (ctypes.c_int32, [ctypes.POINTER(_ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
     "sk_server_destroy": (None, [ctypes.c_void_p]),
     "sk_server_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
@@ -818,6 +823,62 @@ def lodsplat_decode(data: bytes, max_sh_degree: int = 3) -> LodTree:
                   bounds_min=np.array(hd["bounds_min"], np.float32),
                   bounds_max=np.array(hd["bounds_max"], np.float32))
     return LodTree(cloud, layout, hd["leaf_count"], clusters, leaves)
+
+
+def _copy_out(ptr, dtype, shape):
+    if not ptr or int(np.prod(shape)) == 0:
+        return None
+    count = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    raw = ctypes.string_at(ptr, count)
+    return np.frombuffer(raw, dtype).reshape(shape).copy()
+
+
+def build_lod_tree(cloud: Cloud, bounds_min=None, bounds_max=None, octree_depth: int = 0,
+                   cluster_leaves: int = 0, selection: bool = True) -> LodTree:
+    """buildLodTree on the host (sk_build_lod_tree): bounds default to the cloud's, else the
+    positions' own box."""
+    lib = library()
+    lo = bounds_min if bounds_min is not None else cloud.bounds_min
+    hi = bounds_max if bounds_max is not None else cloud.bounds_max
+    lo = None if lo is None else np.ascontiguousarray(lo, np.float32)
+    hi = None if hi is None else np.ascontiguousarray(hi, np.float32)
+    v = cloud.view()
+    handle = ctypes.c_void_p()
+    st = lib.sk_build_lod_tree(ctypes.byref(v), _ptr(lo), _ptr(hi), octree_depth, cluster_leaves,
+                               1 if selection else 0, ctypes.byref(handle))
+    if st != SK_OK:
+        raise SplatError(st, "sk_build_lod_tree")
+    try:
+        t = _LodView()
+        bmin, bmax = np.zeros(3, np.float32), np.zeros(3, np.float32)
+        lib.sk_lod_tree_view(handle, ctypes.byref(t), _ptr(bmin), _ptr(bmax))
+        n, d = t.node_count, t.nodes.sh_degree
+        coeffs = 3 * ((d + 1) ** 2 - 1)
+        nodes = Cloud(_copy_out(ctypes.cast(t.nodes.positions, ctypes.c_void_p).value, np.float32, (n, 3)),
+                      _copy_out(ctypes.cast(t.nodes.covariances, ctypes.c_void_p).value, np.float32, (n, 6)),
+                      _copy_out(ctypes.cast(t.nodes.colors, ctypes.c_void_p).value, np.float32, (n, 3)),
+                      _copy_out(ctypes.cast(t.nodes.alphas, ctypes.c_void_p).value, np.float32, (n,)),
+                      sh_degree=d,
+                      sh=_copy_out(ctypes.cast(t.nodes.sh, ctypes.c_void_p).value, np.float32, (n, coeffs))
+                      if coeffs else None,
+                      bounds_min=bmin, bounds_max=bmax)
+        layout = _copy_out(t.layout, LOD_NODE_DTYPE, (n,))
+        clusters = _copy_out(t.clusters, LOD_CLUSTER_DTYPE, (t.cluster_count,))
+        leaves = _copy_out(ctypes.cast(t.leaves, ctypes.c_void_p).value, np.uint32, (t.leaf_ref_count,))
+        return LodTree(nodes, layout, t.leaf_count, clusters, leaves)
+    finally:
+        lib.sk_lod_tree_free(handle)
+
+
+def write_lodsplat(tree: LodTree, path):
+    """writeLodSplat: version 2 when the tree has selection data; refuses an existing path."""
+    bmin = tree.nodes.bounds_min if tree.nodes.bounds_min is not None else np.zeros(3, np.float32)
+    bmax = tree.nodes.bounds_max if tree.nodes.bounds_max is not None else np.zeros(3, np.float32)
+    bmin, bmax = np.ascontiguousarray(bmin, np.float32), np.ascontiguousarray(bmax, np.float32)
+    v = tree.view()
+    st = library().sk_write_lodsplat(ctypes.byref(v), _ptr(bmin), _ptr(bmax), os.fsencode(str(path)))
+    if st != SK_OK:
+        raise SplatError(st, f"cannot write {path}")
 
 
 def radix_argsort_device(keys_ptr: int, count_ptr: int, capacity: int, bits: int, order_ptr: int,

@@ -1,0 +1,64 @@
+"""The host LOD tree builder (sk_build_lod_tree) and .lodsplat writer against the reference's own
+builder and writer: the same tree, selection data and file, bit for bit (CPU only)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import splatkit_b200 as sk
+from splatkit_b200 import synthetic
+
+from scenes import hierarchy_cloud
+
+
+def bounded(cloud):
+    pos = np.asarray(cloud.positions, np.float32)
+    cloud.bounds_min = pos.min(axis=0) - 0.25
+    cloud.bounds_max = pos.max(axis=0) + 0.25
+    return cloud
+
+
+CLOUDS = {
+    "grid": lambda: hierarchy_cloud(),
+    "random_sh2": lambda: bounded(synthetic.random_cloud(5000, seed=11, sh_degree=2, half_extent=4.0)),
+    "random_sh3": lambda: bounded(synthetic.random_cloud(3000, seed=12, sh_degree=3, half_extent=2.0)),
+    "clustered": lambda: bounded(synthetic.clustered_cloud(12, 400, seed=13, half_extent=30.0)),
+}
+
+
+def assert_tree_equals(ours: sk.LodTree, ref: dict):
+    n = len(ref["layout"])
+    assert len(ours.layout) == n and ours.leaf_count == ref["leaf_count"]
+    assert ours.layout.tobytes() == np.ascontiguousarray(ref["layout"]).tobytes()
+    for name, got in (("positions", ours.nodes.positions), ("covariances", ours.nodes.covariances),
+                      ("colors", ours.nodes.colors), ("alphas", ours.nodes.alphas)):
+        assert np.asarray(got, np.float32).tobytes() == np.asarray(ref[name], np.float32).tobytes(), name
+    if ref["sh"] is None:
+        assert ours.nodes.sh is None
+    else:
+        assert ours.nodes.sh.tobytes() == np.asarray(ref["sh"], np.float32).tobytes()
+    if ref["clusters"] is not None and len(ref["clusters"]):
+        assert ours.clusters.tobytes() == np.ascontiguousarray(ref["clusters"]).tobytes()
+        np.testing.assert_array_equal(ours.leaves, ref["leaves"])
+
+
+@pytest.mark.parametrize("name", sorted(CLOUDS))
+@pytest.mark.parametrize("depth,leaves", [(0, 0), (6, 8), (3, 64)])
+def test_builder_matches_the_reference_builder(reference, name, depth, leaves):
+    cloud = CLOUDS[name]()
+    ours = sk.build_lod_tree(cloud, octree_depth=depth, cluster_leaves=leaves)
+    ref = reference.build_lod_tree(cloud, octree_depth=depth, cluster_leaves=leaves)
+    assert_tree_equals(ours, ref)
+    assert sk.lod_depth(ours.layout, ours.leaf_count) == ref["depth"]
+
+
+@pytest.mark.parametrize("selection", [True, False])
+def test_written_file_is_the_reference_file(reference, tmp_path, selection):
+    cloud = CLOUDS["random_sh2"]()
+    ref = reference.write_lodsplat(cloud, tmp_path / "ref.lodsplat", selection=selection)
+    ours = sk.build_lod_tree(cloud, selection=selection)
+    sk.write_lodsplat(ours, tmp_path / "ours.lodsplat")
+    assert (tmp_path / "ours.lodsplat").read_bytes() == (tmp_path / "ref.lodsplat").read_bytes()
+    with pytest.raises(sk.SplatError):  # never overwrites
+        sk.write_lodsplat(ours, tmp_path / "ours.lodsplat")
+    assert ref["depth"] == sk.lodsplat_header((tmp_path / "ours.lodsplat").read_bytes())["depth"]
