@@ -50,6 +50,7 @@ def parse(argv=None):
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch", action="store_true", help="skip the 64-view batched comparison")
     p.add_argument("--no-serve", action="store_true", help="skip the serving comparison")
+    p.add_argument("--no-lod", action="store_true", help="skip the LOD walk")
     return p.parse_args(argv)
 
 
@@ -361,6 +362,8 @@ def run_ours(args):
             line["cpu_baseline"] = cpu_baseline(cloud, args.bits)
         if world == 1 and not args.no_batch and args.bits == 16:
             line["batch64"] = measure_batch(r)
+        if world == 1 and not args.no_lod and args.bits == 16:
+            line["lod_walk"] = measure_lod_walk()
         if world == 1 and not args.no_serve and args.bits == 16:
             line["served"] = measure_serve()
         print(json.dumps(line), flush=True)
@@ -435,6 +438,50 @@ def measure_batch(renderer):
             "how": "plain: resize + draw + read_image per view; batched: autotuned (emission, "
                    "radix tile, lanes of 3), then 8 submissions of 64 views, CUDA-graph replay, "
                    "every image copied back; host-timed"}
+
+
+# ---- LOD walk: 6M leaves in 2000 clusters, 300 frames at 1920x1080 ----------------------------
+def measure_lod_walk():
+    """The LOD workload: 2000 anisotropic clusters of 3000 splats (centres in a 200 m box), the
+    tree built on the host by the project's builder (the reference builder's tree), cut at
+    1.5 px along a 300-frame walk (eye height 1.7 m, x from -90 to 90 m, looking +x)."""
+    import splatkit_b200 as sk
+    from splatkit_b200 import camera as skcam
+    from splatkit_b200 import synthetic
+
+    cloud = synthetic.clustered_cloud(2000, 3000, seed=0)
+    pos = np.asarray(cloud.positions, np.float32)
+    cloud.bounds_min, cloud.bounds_max = pos.min(axis=0), pos.max(axis=0)
+    t0 = time.perf_counter()
+    tree = sk.build_lod_tree(cloud)
+    build_s = time.perf_counter() - t0
+    r = sk.Renderer(WIDTH, HEIGHT, image_format=sk.FORMAT_RGBA8, time_stages=True)
+    r.apply_render_policy(sk.Policy(lod_error_pixels=1.5, sort_depth_bits=16))
+    r.upload_lod_world(tree, 0, 4_000_000)
+    proj = skcam.perspective(math.radians(60.0), WIDTH / HEIGHT, 0.05, 400.0)
+
+    def frame(i):
+        x = -90.0 + 180.0 * i / 299
+        eye = np.array([x, 1.7, 0.0], np.float32)
+        r.draw(sk.Frame(skcam.look_at_view(eye, (x + 10.0, 1.7, 0.0)), proj, eye, [], 0))
+
+    for i in range(5):
+        frame(i)
+        r.wait_idle()
+    gpu_ms, select_ms, cut = [], [], []
+    for i in range(300):
+        frame(i)
+        r.wait_idle()
+        s = r.stats()
+        gpu_ms.append(s["gpu_ms"])
+        select_ms.append(s["select_ms"])
+        cut.append(s["selected_count"])
+    r.close()
+    return {"workload": "6M leaves (2000 clusters x 3000), host-built tree of "
+                        f"{len(tree.layout)} nodes, 1.5 px cut, 300-frame walk at 1920x1080",
+            "frames_per_s": 300 / (sum(gpu_ms) / 1000.0), "mean_gpu_ms": float(np.mean(gpu_ms)),
+            "mean_select_ms": float(np.mean(select_ms)), "mean_cut_splats": float(np.mean(cut)),
+            "tree_build_s": build_s}
 
 
 # ---- serving: Poisson requests over 8 resident scenes -----------------------------------------
