@@ -105,7 +105,21 @@ typedef struct {
   const sk_range* ranges;
   uint32_t range_count;
   int32_t sh_degree; /* capped by the world */
+  /* RevealUniform (splatkit-engine/include/splatkit/reveal/Reveal.h:25-35): splats below the
+   * reveal level within `band` of it glow toward `tint` (SplatProjection.metalh:177-189);
+   * band 0: no glow */
+  float reveal_band, reveal_tint_amount, reveal_brightness_boost;
+  float reveal_tint[3];
 } sk_frame;
+
+/* PartStyle (splatkit-ios/.../metal/cull/SplatVisibility.metal:5-11). */
+typedef struct {
+  float tint[3];
+  float tint_amount;
+  float brightness;
+  float opacity;
+  float reserved[2];
+} sk_part_style;
 
 /* RenderPolicy (packages/splatkit-engine/include/splatkit/rendering/RenderPolicy.h:17-40). */
 typedef struct {
@@ -214,6 +228,15 @@ void sk_lod_tree_free(sk_lod_tree* tree);
 sk_status sk_create_slab(sk_context* ctx, uint32_t capacity, int32_t sh_degree);
 sk_status sk_upload_tile(sk_context* ctx, uint32_t offset, const sk_cloud_view* cloud);
 sk_status sk_world_info(sk_context* ctx, uint32_t* count, int32_t* sh_degree);
+/* Part labels of the flat world's records [offset, offset + count) (SplatCloud::labels), kept
+ * until the next world upload; labels start at 0. */
+sk_status sk_upload_labels(sk_context* ctx, uint32_t offset, const uint16_t* labels, uint32_t count);
+/* The styles labelled parts are drawn with (Frame::labelStyles): record r with label l uses
+ * palette[states[l]] (10 palette entries, states[l] < 10; a label without a state draws
+ * unstyled). state_count 0: no styling. Applied in the cull (SplatVisibility.metal:69-84):
+ * colour = mix(colour, tint, tint_amount) * brightness, opacity *= opacity, dropped below 2/255. */
+sk_status sk_set_part_styles(sk_context* ctx, const sk_part_style* palette, const uint32_t* states,
+                             uint32_t state_count);
 
 /* ---- the frame (SplatRenderer::draw, :134) ------------------------------------------- */
 /* Enqueues LOD cut, cull, sort, binning and composite; returns without waiting. */

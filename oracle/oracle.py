@@ -67,7 +67,7 @@ class Oracle:
             "sko_half_to_float": (ctypes.c_float, [ctypes.c_uint16]),
             "sko_visibility": (ctypes.c_uint32, [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_int,
                                                  ctypes.c_int, _vp, ctypes.c_uint32, _vp,
-                                                 ctypes.c_uint32, _vp, _vp, ctypes.c_int]),
+                                                 ctypes.c_uint32, _vp, _vp, ctypes.c_int, _vp]),
             "sko_stable_argsort": (None, [_vp, ctypes.c_uint32, _vp]),
             "sko_radix_argsort": (None, [_vp, ctypes.c_uint32, ctypes.c_int, _vp, ctypes.c_int]),
             "sko_lod_select": (ctypes.c_uint32, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32,
@@ -104,7 +104,8 @@ class Oracle:
 
     def visibility(self, cam: Camera, splats: np.ndarray, sh: Optional[np.ndarray], sh_stride: int,
                    sh_degree: int, key_bits: int, ranges: Sequence = (), indices=None,
-                   threads: int = 1):
+                   threads: int = 1, parts=None):
+        """parts: None, or (labels uint16[n], palette float32[10, 8], states uint32[k])."""
         splats = np.ascontiguousarray(splats)
         sh = None if sh is None or sh_degree == 0 else np.ascontiguousarray(sh, np.uint32)
         if indices is not None:
@@ -118,9 +119,19 @@ class Oracle:
             total = int(rng_arr[:, 1].sum()) if rc else 0
         keys = np.empty(max(total, 1), np.uint32)
         proj = np.empty(max(total, 1), PROJECTED_DTYPE)
+        parts_struct, keep = None, None
+        if parts is not None:
+            labels = np.ascontiguousarray(parts[0], np.uint16)
+            palette = np.ascontiguousarray(parts[1], np.float32).reshape(10, 8)
+            states = np.ascontiguousarray(parts[2], np.uint32)
+            keep = (labels, palette, states)
+            parts_struct = (ctypes.c_void_p * 4)(labels.ctypes.data, palette.ctypes.data,
+                                                 states.ctypes.data, len(states))
         n = self.lib.sko_visibility(ctypes.addressof(cam), _p(splats), _p(sh), sh_stride,
                                     sh_degree, key_bits, _p(rng_arr), rc, _p(idx),
-                                    0 if idx is None else len(idx), _p(keys), _p(proj), threads)
+                                    0 if idx is None else len(idx), _p(keys), _p(proj), threads,
+                                    None if parts_struct is None else ctypes.addressof(parts_struct))
+        del keep
         return keys[:n].copy(), proj[:n].copy()
 
     def stable_argsort(self, keys: np.ndarray) -> np.ndarray:

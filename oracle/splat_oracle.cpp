@@ -490,6 +490,48 @@ void sko_camera_make(const float* view16, const float* proj16, const float* came
   out->reveal[0] = std::numeric_limits<float>::infinity();
 }
 
+namespace {
+
+float lowOf(uint32_t w) { return halfToFloat(static_cast<uint16_t>(w & 0xffffu)); }
+float highOf(uint32_t w) { return halfToFloat(static_cast<uint16_t>(w >> 16)); }
+
+// metal/cull/SplatVisibility.metal:69-84: a labelled part's tint, brightness and opacity on the
+// packed colours; false when the opacity drops the splat. A label without a state, or a state
+// without a palette entry, draws unstyled.
+bool stylePart(const sko_parts& parts, uint32_t index, sko_projected& p) {
+  const uint32_t label = parts.labels[index];
+  if (label >= parts.stateCount) return true;
+  const uint32_t state = parts.states[label];
+  if (state >= 10) return true;
+  const float* st = parts.palette + state * 8;  // tint[3], tintAmount, brightness, opacity
+  if (!(st[3] != 0.0f || st[4] != 1.0f || st[5] != 1.0f)) return true;
+  const float r = lowOf(p.color0), g = highOf(p.color0), b = lowOf(p.color1), a = highOf(p.color1);
+  const float r2 = (r + (st[0] - r) * st[3]) * st[4];
+  const float g2 = (g + (st[1] - g) * st[3]) * st[4];
+  const float b2 = (b + (st[2] - b) * st[3]) * st[4];
+  const float alpha = a * st[5];
+  p.color0 = packHalf2(r2, g2);
+  p.color1 = packHalf2(b2, alpha);
+  return alpha >= kQuadMinAlpha;
+}
+
+// metal/layout/SplatProjection.metalh:177-189 for an encoded-space target (outputLinear 0).
+void revealGlow(const sko_camera& cam, float height, sko_projected& p) {
+  if (!(cam.reveal[1] > 0.0f)) return;
+  float glow = std::fmin(std::fmax(1.0f - (cam.reveal[0] - height) / cam.reveal[1], 0.0f), 1.0f);
+  glow = glow * glow;
+  if (!(glow > 0.0f)) return;
+  const float r = lowOf(p.color0), g = highOf(p.color0), b = lowOf(p.color1), a = highOf(p.color1);
+  const float t = cam.reveal[2] * glow, boost = 1.0f + cam.reveal[3] * glow;
+  const float r2 = (r + (cam.revealTint[0] - r) * t) * boost;
+  const float g2 = (g + (cam.revealTint[1] - g) * t) * boost;
+  const float b2 = (b + (cam.revealTint[2] - b) * t) * boost;
+  p.color0 = packHalf2(r2, g2);
+  p.color1 = packHalf2(b2, a);
+}
+
+}  // namespace
+
 int sko_project_one(const sko_camera* cam, const sko_splat* splat, uint32_t index,
                     const uint32_t* sh, uint32_t shStride, int shDegree, int keyBits,
                     uint32_t* keyOut, sko_projected* out) {
@@ -500,7 +542,8 @@ int sko_project_one(const sko_camera* cam, const sko_splat* splat, uint32_t inde
 uint32_t sko_visibility(const sko_camera* cam, const sko_splat* splats, const uint32_t* sh,
                         uint32_t shStride, int shDegree, int keyBits, const sko_range* ranges,
                         uint32_t rangeCount, const uint32_t* indices, uint32_t indexCount,
-                        uint32_t* keysOut, sko_projected* projectedOut, int threads) {
+                        uint32_t* keysOut, sko_projected* projectedOut, int threads,
+                        const sko_parts* parts) {
   std::vector<uint32_t> sources;
   if (indices != nullptr) {
     sources.assign(indices, indices + indexCount);
@@ -518,6 +561,8 @@ uint32_t sko_visibility(const sko_camera* cam, const sko_splat* splats, const ui
       sko_projected p;
       const uint32_t index = sources[i];
       if (projectOne(*cam, splats[index], index, sh, shStride, shDegree, keyBits, &key, &p)) {
+        if (parts && parts->labels && !stylePart(*parts, index, p)) continue;
+        revealGlow(*cam, splats[index].position[1], p);
         keys[t].push_back(key);
         proj[t].push_back(p);
       }

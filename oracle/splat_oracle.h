@@ -86,10 +86,21 @@ int sko_project_one(const sko_camera* cam, const sko_splat* splat, uint32_t inde
 // The visibility pass over ranges (or, when `indices` is not null, over indices[0..indexCount)),
 // survivors compacted in source order. Returns the survivor count. `threads` > 1 splits the
 // source range over std::threads; the output is identical.
+// Part labels and styles (metal/cull/SplatVisibility.metal:4-12,69-84): palette of 10 entries of
+// 8 floats (tint rgb, tint amount, brightness, opacity, 2 reserved), states[label] < 10.
+typedef struct {
+  const uint16_t* labels;
+  const float* palette;
+  const uint32_t* states;
+  uint32_t stateCount;
+} sko_parts;
+
+// parts null: no part styling. The reveal glow follows the camera's reveal fields.
 uint32_t sko_visibility(const sko_camera* cam, const sko_splat* splats, const uint32_t* sh,
                         uint32_t shStride, int shDegree, int keyBits, const sko_range* ranges,
                         uint32_t rangeCount, const uint32_t* indices, uint32_t indexCount,
-                        uint32_t* keysOut, sko_projected* projectedOut, int threads);
+                        uint32_t* keysOut, sko_projected* projectedOut, int threads,
+                        const sko_parts* parts);
 
 // Stable ascending argsort: std::stable_sort of (key, position) pairs.
 void sko_stable_argsort(const uint32_t* keys, uint32_t n, uint32_t* orderOut);

@@ -33,6 +33,7 @@ struct VisibilityArgs {
   uint32_t* counters;  // two words
   uint32_t epoch;
   uint32_t* error;
+  PartLabels parts;  // labels.labels null: no part styling
 };
 uint32_t visibilityTileSplats();
 // `cam` is a device pointer: the kernels stage it in shared memory, so a captured graph can be

@@ -53,6 +53,26 @@ struct Range {
   uint32_t count;
 };
 
+// PartStyle (splatkit-ios/.../metal/cull/SplatVisibility.metal:5-11): how a labelled part is
+// drawn. A world label picks a state, a state picks one of kPartStyles palette entries.
+struct PartStyle {
+  float tint[3];
+  float tintAmount;
+  float brightness;
+  float opacity;
+  float reserved[2];
+};
+static_assert(sizeof(PartStyle) == 32, "PartStyle is 32 bytes");
+constexpr uint32_t kPartStyles = 10;
+
+// Part labels of a flat world and the styles they are drawn with (all device pointers).
+struct PartLabels {
+  const uint16_t* labels;   // one per world record; null: no styling
+  const PartStyle* palette; // kPartStyles entries
+  const uint32_t* states;   // stateCount entries, each < kPartStyles
+  uint32_t stateCount;
+};
+
 struct LodNode {
   float position[3];
   float size;

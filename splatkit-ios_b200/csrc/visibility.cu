@@ -235,6 +235,42 @@ __device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, 
   return true;
 }
 
+// SplatVisibility.metal:69-84: a labelled part's tint, brightness and opacity applied to the
+// packed colours, in the same rounded steps as the host; false when the opacity drops the splat.
+// A label without a state, or a state without a palette entry, draws unstyled.
+__device__ __forceinline__ bool styleRecord(const PartLabels& parts, uint32_t index, uint32_t* rec) {
+  const uint32_t label = parts.labels[index];
+  if (label >= parts.stateCount) return true;
+  const uint32_t state = __ldg(parts.states + label);
+  if (state >= kPartStyles) return true;
+  const PartStyle st = parts.palette[state];
+  if (!(st.tintAmount != 0.0f || st.brightness != 1.0f || st.opacity != 1.0f)) return true;
+  const float r = lowHalf(rec[4]), g = highHalf(rec[4]), b = lowHalf(rec[5]), a = highHalf(rec[5]);
+  const float r2 = (r + (st.tint[0] - r) * st.tintAmount) * st.brightness;
+  const float g2 = (g + (st.tint[1] - g) * st.tintAmount) * st.brightness;
+  const float b2 = (b + (st.tint[2] - b) * st.tintAmount) * st.brightness;
+  const float alpha = a * st.opacity;
+  rec[4] = packHalf2(r2, g2);
+  rec[5] = packHalf2(b2, alpha);
+  return alpha >= kQuadMinAlpha;
+}
+
+// SplatProjection.metalh:177-189 for an encoded-space target: splats below the reveal level
+// within `band` of it glow toward the reveal tint and brighten.
+__device__ __forceinline__ void revealGlow(const Camera& cam, float height, uint32_t* rec) {
+  if (!(cam.reveal[1] > 0.0f)) return;
+  float glow = fminf(fmaxf(1.0f - (cam.reveal[0] - height) / cam.reveal[1], 0.0f), 1.0f);
+  glow = glow * glow;
+  if (!(glow > 0.0f)) return;
+  const float r = lowHalf(rec[4]), g = highHalf(rec[4]), b = lowHalf(rec[5]), a = highHalf(rec[5]);
+  const float t = cam.reveal[2] * glow, boost = 1.0f + cam.reveal[3] * glow;
+  const float r2 = (r + (cam.revealTint[0] - r) * t) * boost;
+  const float g2 = (g + (cam.revealTint[1] - g) * t) * boost;
+  const float b2 = (b + (cam.revealTint[2] - b) * t) * boost;
+  rec[4] = packHalf2(r2, g2);
+  rec[5] = packHalf2(b2, a);
+}
+
 __device__ __forceinline__ uint32_t sourceIndex(const VisibilityArgs& a, uint32_t t) {
   if (a.rangeCount == 1) return a.single.offset + t;
   // SplatVisibility.metal:30-37: the range whose start is the last one <= t.
@@ -257,7 +293,8 @@ struct VisibilitySmem {
 };
 
 // Projects one 1024-record tile into shared memory: survivors' keys and records at their
-// source slot, and per warp row the mask of survivors. indexOf(t) gives the record index of
+// source slot, and per warp row the mask of survivors. Part styles (when labels are given) and
+// the reveal glow are applied to each survivor's record after its projection. indexOf(t) gives the record index of
 // tile position t, or 0xffffffff past the end. keyHigh is or-ed into every key (the view id of a
 // batch, above a 16-bit key). One record per row of the warp, not unrolled (the projection is
 // large); the next row's record is fetched while this one is projected.
@@ -265,7 +302,8 @@ template <int D, bool kKey16, typename IndexOf>
 __device__ __forceinline__ void projectTile(VisibilitySmem& s, const Camera& cam,
                                             const GpuSplat* __restrict__ splats,
                                             const uint32_t* __restrict__ sh, uint32_t shStride,
-                                            uint32_t first, uint32_t keyHigh, IndexOf indexOf) {
+                                            const PartLabels& parts, uint32_t first,
+                                            uint32_t keyHigh, IndexOf indexOf) {
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
   uint32_t index = indexOf(first);
   uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
@@ -289,6 +327,8 @@ __device__ __forceinline__ void projectTile(VisibilitySmem& s, const Camera& cam
     if (index != 0xffffffffu) {
       uint32_t key, rec[8];
       visible = projectSplat<D, kKey16>(cam, lo, hi, index, sh, shStride, key, rec);
+      if (visible && parts.labels) visible = styleRecord(parts, index, rec);
+      if (visible) revealGlow(cam, asF(lo.y), rec);
       if (visible) {
         s.key[slot] = key | keyHigh;
         s.rec[2 * slot] = make_uint4(rec[0], rec[1], rec[2], rec[3]);
@@ -386,7 +426,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       }
       return index;
     };
-    projectTile<D, kKey16>(s, cam, a.splats, a.sh, a.shStride, first, 0u, indexOf);
+    projectTile<D, kKey16>(s, cam, a.splats, a.sh, a.shStride, a.parts, first, 0u, indexOf);
     compactTile(s, a.status, tile, a.epoch, a.error);
     if (tile == tiles - 1 && threadIdx.x == 0) *a.visibleCount = s.tileBase + s.tileCount;
     copyOutTile(s, a.keys, a.projected, a.spans, cam.screenSize[0], cam.screenSize[1], a.tilesX,
@@ -432,7 +472,8 @@ __global__ void __launch_bounds__(kThreads, 4)
     auto indexOf = [&](uint32_t t) -> uint32_t {
       return t < view.count ? view.offset + t : 0xffffffffu;
     };
-    projectTile<D, true>(s, cam, view.splats, view.sh, view.shStride, first, v << 16, indexOf);
+    projectTile<D, true>(s, cam, view.splats, view.sh, view.shStride, PartLabels{}, first, v << 16,
+                         indexOf);
     compactTile(s, a.status, item, a.epoch, a.error);
     if (threadIdx.x == 0) {
       if (chunk == 0) a.viewFirst[v] = s.tileBase;

@@ -195,6 +195,10 @@ Camera cameraOf(const sk_frame& frame, uint32_t w, uint32_t h, float minPixelRad
   c.cameraPosition[2] = frame.camera_position[2];
   c.cameraPosition[3] = 1.0f;
   c.reveal[0] = frame.reveal_level;
+  c.reveal[1] = frame.reveal_band;
+  c.reveal[2] = frame.reveal_tint_amount;
+  c.reveal[3] = frame.reveal_brightness_boost;
+  for (int j = 0; j < 3; ++j) c.revealTint[j] = frame.reveal_tint[j];
   return c;
 }
 
@@ -292,6 +296,10 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     v.counters = counters + 0;
     v.epoch = nextEpoch(1);
     v.error = error;
+    if (!lod && labels.ptr && styleStateCount > 0)
+      v.parts = PartLabels{static_cast<const uint16_t*>(labels.ptr),
+                           static_cast<const PartStyle*>(stylePalette.ptr),
+                           static_cast<const uint32_t*>(styleStateTable.ptr), styleStateCount};
     e = launchVisibility(view.camera, v, degree, key16, lod, s);
   }
   if (timed) cudaEventRecord(f.events[2], s);
@@ -604,6 +612,7 @@ sk_status sk_upload_world(sk_context* handle, const sk_cloud_view* cloud, int32_
                            ctx->scratch.maxTiles, ctx->stream);
   if (st != SK_OK) return st;
   ctx->world = std::move(fresh);
+  ctx->labels.release();  // labels belong to the world they were uploaded for
   return SK_OK;
 }
 
@@ -626,6 +635,7 @@ sk_status sk_create_slab(sk_context* handle, uint32_t capacity, int32_t shDegree
   fresh.count = capacity;
   fresh.shDegree = shDegree;
   ctx->world = std::move(fresh);
+  ctx->labels.release();  // labels belong to the world they were uploaded for
   return SK_OK;
 }
 
@@ -706,6 +716,7 @@ sk_status sk_upload_lod_world(sk_context* handle, const sk_lod_view* tree, int32
                            ctx->scratch.maxTiles, ctx->stream);
   if (st != SK_OK) return st;
   ctx->world = std::move(fresh);
+  ctx->labels.release();  // labels belong to the world they were uploaded for
   ctx->threshold.reset(ctx->threshold.policyPixels());
   return SK_OK;
 }
@@ -886,6 +897,52 @@ sk_status sk_radix_argsort_device(const uint32_t* d_keys, const uint32_t* d_coun
   cudaError_t e = sk::sortResetWorkspace(a, s);
   if (e == cudaSuccess) e = sk::launchSort(a, s);
   return e == cudaSuccess ? SK_OK : SK_E_DEVICE;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+sk_status sk_upload_labels(sk_context* handle, uint32_t offset, const uint16_t* labels, uint32_t count) {
+  SK_CTX(handle);
+  if (!labels || !ctx->world.splats.ptr || ctx->world.lod || offset > ctx->world.count ||
+      count > ctx->world.count - offset)
+    return ctx->fail(SK_E_INVALID, "labels need a flat world and a range inside it");
+  sk_status st = ctx->finishFrame(true);
+  if (st == SK_E_DEVICE) return st;
+  const bool fresh = ctx->labels.ptr == nullptr;
+  cudaError_t e = ctx->labels.allocate(size_t{ctx->world.count} * 2);
+  if (e == cudaSuccess && fresh) e = cudaMemset(ctx->labels.ptr, 0, ctx->labels.bytes);
+  if (e == cudaSuccess && count)
+    e = cudaMemcpy(static_cast<uint16_t*>(ctx->labels.ptr) + offset, labels, size_t{count} * 2,
+                   cudaMemcpyHostToDevice);
+  return ctx->check(e, "labels");
+}
+
+sk_status sk_set_part_styles(sk_context* handle, const sk_part_style* palette, const uint32_t* states,
+                             uint32_t state_count) {
+  SK_CTX(handle);
+  if (state_count > 65536 || (state_count && (!palette || !states)))
+    return ctx->fail(SK_E_INVALID, "part styles: palette and states required");
+  for (uint32_t i = 0; i < state_count; ++i)
+    if (states[i] >= sk::kPartStyles) return ctx->fail(SK_E_INVALID, "a state names no palette entry");
+  sk_status st = ctx->finishFrame(true);
+  if (st == SK_E_DEVICE) return st;
+  if (state_count == 0) {
+    ctx->styleStateCount = 0;
+    return SK_OK;
+  }
+  static_assert(sizeof(sk_part_style) == sizeof(sk::PartStyle), "PartStyle layout");
+  cudaError_t e = ctx->stylePalette.allocate(sk::kPartStyles * sizeof(sk::PartStyle));
+  if (e == cudaSuccess) e = ctx->styleStateTable.allocate(size_t{state_count} * 4);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ctx->stylePalette.ptr, palette, sk::kPartStyles * sizeof(sk::PartStyle),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ctx->styleStateTable.ptr, states, size_t{state_count} * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return ctx->check(e, "part styles");
+  ctx->styleStateCount = state_count;
+  return SK_OK;
 }
 
 }  // extern "C"

@@ -119,6 +119,9 @@ struct Context {
   uint32_t lodLimit = 0;
   host::LodThreshold threshold;
   World world;
+  // part labels of the flat world (cleared with it) and the styles they are drawn with
+  DeviceBuffer labels, stylePalette, styleStateTable;
+  uint32_t styleStateCount = 0;
   FrameScratch scratch;
   // the plain renderer's own view: image, counters, camera
   DeviceBuffer image, frameCounters, camera;

@@ -133,6 +133,10 @@ class CudaSplatRenderer final : public SplatRenderer {
     f.camera_position[1] = frame.cameraPosition.y;
     f.camera_position[2] = frame.cameraPosition.z;
     f.reveal_level = frame.reveal.level;
+    f.reveal_band = frame.reveal.band;
+    f.reveal_tint_amount = frame.reveal.tintAmount;
+    f.reveal_brightness_boost = frame.reveal.brightnessBoost;
+    for (int j = 0; j < 3; ++j) f.reveal_tint[j] = frame.reveal.tint[j];
     f.ranges = reinterpret_cast<const sk_range*>(frame.ranges);
     f.range_count = frame.rangeCount;
     f.sh_degree = frame.shDegree;

@@ -91,7 +91,15 @@ class _Frame(ctypes.Structure):
     _fields_ = [("view", ctypes.c_float * 16), ("proj", ctypes.c_float * 16),
                 ("camera_position", ctypes.c_float * 3), ("reveal_level", ctypes.c_float),
                 ("ranges", ctypes.POINTER(_Range)), ("range_count", ctypes.c_uint32),
-                ("sh_degree", ctypes.c_int32)]
+                ("sh_degree", ctypes.c_int32), ("reveal_band", ctypes.c_float),
+                ("reveal_tint_amount", ctypes.c_float), ("reveal_brightness_boost", ctypes.c_float),
+                ("reveal_tint", ctypes.c_float * 3)]
+
+
+class _PartStyle(ctypes.Structure):
+    _fields_ = [("tint", ctypes.c_float * 3), ("tint_amount", ctypes.c_float),
+                ("brightness", ctypes.c_float), ("opacity", ctypes.c_float),
+                ("reserved", ctypes.c_float * 2)]
 
 
 class _BatchConfig(ctypes.Structure):
@@ -240,6 +248,9 @@ _SIGNATURES = {
                                            ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     "sk_lod_tree_view": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_LodView), _f32p, _f32p]),
     "sk_lod_tree_free": (None, [ctypes.c_void_p]),
+    "sk_upload_labels": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32]),
+    "sk_set_part_styles": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_PartStyle), ctypes.c_void_p,
+                                            ctypes.c_uint32]),
     "sk_server_create": (ctypes.c_int32, [ctypes.POINTER(_ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
     "sk_server_destroy": (None, [ctypes.c_void_p]),
     "sk_server_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
@@ -381,6 +392,10 @@ class Frame:
     ranges: Sequence[tuple] = ()
     sh_degree: int = 0
     reveal_level: float = float("inf")
+    reveal_band: float = 0.0  # RevealUniform (Reveal.h:25-35); 0: no glow
+    reveal_tint_amount: float = 0.0
+    reveal_brightness_boost: float = 0.0
+    reveal_tint: Sequence[float] = (1.0, 1.0, 1.0)
 
     def native(self):
         f = _Frame()
@@ -393,6 +408,11 @@ class Frame:
         for i in range(3):
             f.camera_position[i] = float(pos[i])
         f.reveal_level = self.reveal_level
+        f.reveal_band = self.reveal_band
+        f.reveal_tint_amount = self.reveal_tint_amount
+        f.reveal_brightness_boost = self.reveal_brightness_boost
+        for i in range(3):
+            f.reveal_tint[i] = float(self.reveal_tint[i])
         ranges = (_Range * max(1, len(self.ranges)))(*[_Range(int(o), int(c)) for o, c in self.ranges])
         f.ranges = ctypes.cast(ranges, ctypes.POINTER(_Range)) if len(self.ranges) else None
         f.range_count = len(self.ranges)
@@ -478,6 +498,26 @@ class Renderer:
         else:
             self._check(self._lib.sk_upload_lodsplat_file(self._h, os.fsencode(str(source)), max_sh_degree,
                                                           budget), "lodsplat upload")
+
+    def upload_labels(self, labels: np.ndarray, offset: int = 0):
+        """Part labels (uint16) of world records [offset, offset + len(labels))."""
+        lab = np.ascontiguousarray(labels, np.uint16)
+        self._check(self._lib.sk_upload_labels(self._h, offset, lab.ctypes.data, len(lab)), "labels")
+
+    def set_part_styles(self, palette, states):
+        """palette: up to 10 (tint rgb, tint_amount, brightness, opacity); states[label] -> entry."""
+        pal = (_PartStyle * 10)()
+        for i in range(10):
+            pal[i].tint[0] = pal[i].tint[1] = pal[i].tint[2] = 1.0
+            pal[i].tint_amount, pal[i].brightness, pal[i].opacity = 0.0, 1.0, 1.0
+        for i, entry in enumerate(palette):
+            tint, amount, brightness, opacity = entry
+            for j in range(3):
+                pal[i].tint[j] = float(tint[j])
+            pal[i].tint_amount, pal[i].brightness, pal[i].opacity = amount, brightness, opacity
+        st = np.ascontiguousarray(states, np.uint32)
+        self._check(self._lib.sk_set_part_styles(self._h, pal, st.ctypes.data if len(st) else None,
+                                                 len(st)), "part styles")
 
     def create_slab(self, capacity: int, sh_degree: int):
         self._check(self._lib.sk_create_slab(self._h, capacity, sh_degree), "slab")
