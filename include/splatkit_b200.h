@@ -254,9 +254,9 @@ sk_status sk_read_visible(sk_context* ctx, uint32_t* keys, void* projected, uint
 sk_status sk_read_order(sk_context* ctx, uint32_t* order, uint32_t capacity, uint32_t* count);
 sk_status sk_read_cut(sk_context* ctx, uint32_t* indices, uint32_t capacity, uint32_t* count,
                       uint32_t* lod_counters6);
-/* The last frame's tile lists: ranges[2 * t], ranges[2 * t + 1] = [start, end) of 16x16 tile
- * t (row major) in `values`, which holds projected-record indices front to back per tile.
- * ranges needs 2 * tiles words; *count receives the number of list entries. */
+/* The last frame's binning lists: ranges[2 * c], ranges[2 * c + 1] = [start, end) of 32x32
+ * binning cell c (row major) in `values`, which holds projected-record indices front to back
+ * per cell. ranges needs 2 * cells words; *count receives the number of list entries. */
 sk_status sk_read_tile_lists(sk_context* ctx, uint32_t* ranges, uint32_t* values,
                              uint32_t capacity, uint32_t* count);
 

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant_
           const uint32_t mid = (lo + hi) / 2;
           if (__ldg(a.viewFirst + mid) <= i) lo = mid; else hi = mid;
         }
-        stage.grid[at] = make_uint2(__ldg(&a.views[lo].tileBase), __ldg(&a.views[lo].tilesX));
+        stage.grid[at] = make_uint2(__ldg(&a.views[lo].binBase), __ldg(&a.views[lo].binsX));
       }
     }
     if (warp == kThreads / 32 - 1 && lane == 31) stage.total = warpBase[warp] + warpRun;

@@ -9,8 +9,9 @@
 // mask between four draw batches are replaced by FP32 accumulation and per-pixel early
 // termination when the remaining transmittance drops below `cutoff`.
 //
-// A block of 128 threads owns a tile; each thread owns two horizontally adjacent pixels and each
-// warp an 8x8-pixel quadrant. The block walks the tile's list in batches of 256 records: thread i
+// A block of 128 threads owns a 16x16 tile; each thread owns two horizontally adjacent pixels and
+// each warp an 8x8-pixel quadrant. The tile reads the list of the 32x32 binning cell it lies in
+// (the splats touching the cell, front to back) in batches of 256 records: thread i
 // fetches records i and i + 128 (two 128-bit loads each), turns it into the coverage form (pixel centre, inverse
 // axes, radius, log cutoff, colour) in shared memory and marks which of the four quadrants its
 // quad overlaps (separating-axis test). Each warp compacts, by ballot, the batch entries that
@@ -131,7 +132,7 @@ __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const f
 
 // The target one tile block draws into: the context's image, or its view's part of a batch image.
 struct Target {
-  uint32_t width, height, tilesX, tile;
+  uint32_t width, height, tilesX, tile, binsX, binBase;
   void* image;
 };
 
@@ -166,7 +167,7 @@ __device__ __forceinline__ void writePixel(const CompositeArgs& a, const Target&
 template <int kFormat, bool kBatch>
 __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constant__ CompositeArgs a) {
   __shared__ CompositeSmem sm;
-  Target t{a.width, a.height, a.tilesX, blockIdx.x, a.image};
+  Target t{a.width, a.height, a.tilesX, blockIdx.x, a.binsX, 0u, a.image};
   if constexpr (kBatch) {
     uint32_t lo = 0, hi = a.viewCount;
     while (hi - lo > 1) {
@@ -178,12 +179,15 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
     t.height = __ldg(&v->height);
     t.tilesX = __ldg(&v->tilesX);
     t.tile = blockIdx.x - __ldg(&v->tileBase);
+    t.binsX = __ldg(&v->binsX);
+    t.binBase = __ldg(&v->binBase);
     t.image = static_cast<char*>(a.image) +
               __ldg(reinterpret_cast<const unsigned long long*>(&v->pixelOffset)) *
                   (kFormat == kRgba32f ? 16u : 4u);
   }
-  const uint32_t tile = blockIdx.x;  // ranges are indexed batch-wide
   const uint32_t tx = t.tile % t.tilesX, ty = t.tile / t.tilesX;
+  // the binning cell holding this tile (cells are 2x2 tiles)
+  const uint32_t bin = t.binBase + (ty / 2) * t.binsX + tx / 2;
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
   const uint32_t col = tx * kTileSize + (warp & 1u) * kQuadrant + (lane % 4u) * 2u;  // and col + 1
   const uint32_t row = ty * kTileSize + (warp >> 1) * kQuadrant + lane / 4u;
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   const float tileTop = height - static_cast<float>(ty * kTileSize);
   const float halfW = 0.5f * static_cast<float>(t.width);
   const float halfH = 0.5f * height;
-  const uint2 range = a.ranges[tile];
+  const uint2 range = a.ranges[bin];
   const uint32_t below = lanemaskLt();
   const float2 px = make_float2(px0, px1);
   PixelPair p;

@@ -26,8 +26,8 @@ struct VisibilityArgs {
   uint32_t total;              // ranges mode: sum of counts; indexed mode: capacity bound
   uint32_t* keys;
   Projected* projected;
-  uint4* spans;  // per survivor: the 16x16 tiles its quad touches (sk_tiles.cuh)
-  uint32_t tilesX, tilesY;
+  uint4* spans;  // per survivor: the binning cells its quad touches (sk_tiles.cuh)
+  uint32_t tilesX, tilesY;  // binning cells (kBinSize pixels) per row and column
   uint32_t* visibleCount;
   uint64_t* status;    // one word per 1024-splat tile
   uint32_t* counters;  // two words
@@ -102,8 +102,8 @@ struct BinArgs {
   const uint32_t* order;  // depth order (indices into projected)
   const uint32_t* count;  // survivors (device)
   uint32_t capacity;      // bound on count
-  uint32_t width, height, tilesX, tilesY;
-  uint32_t* instanceKeys;    // tile id per instance
+  uint32_t width, height, tilesX, tilesY;  // tilesX/Y: binning cells per row and column
+  uint32_t* instanceKeys;    // binning cell per instance
   uint32_t* instanceValues;  // projected index per instance
   uint32_t instanceCapacity;
   uint32_t* instanceCount;  // FrameCounters.instances
@@ -120,8 +120,8 @@ struct BinArgs {
 uint32_t binBlocks(uint32_t capacity);
 cudaError_t launchBinning(const BinArgs& args, cudaStream_t stream);
 
-// Tile [start, end) ranges from the tile-sorted instance keys. ranges: tilesX * tilesY uint2,
-// cleared by the launcher.
+// Per binning cell, the [start, end) range of its entries in the cell-sorted instance keys.
+// ranges: one uint2 per cell, cleared by the launcher.
 cudaError_t launchTileRanges(const uint32_t* sortedKeys, const uint32_t* instanceCount,
                              uint32_t instanceCapacity, uint2* ranges, uint32_t tiles,
                              cudaStream_t stream);
@@ -131,8 +131,9 @@ enum PixelFormat : int { kRgba8 = 0, kRgba32f = 1 };
 struct CompositeArgs {
   const Projected* projected;
   const uint32_t* values;  // tile-sorted projected indices
-  const uint2* ranges;
-  uint32_t width, height, tilesX, tilesY;
+  const uint2* ranges;  // per binning cell
+  uint32_t width, height, tilesX, tilesY;  // composite tiles (kTileSize pixels)
+  uint32_t binsX;                          // binning cells per row
   float background[3];
   int opaque;
   float cutoff;  // transmittance below which a pixel stops

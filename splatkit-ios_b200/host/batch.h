@@ -51,7 +51,7 @@ struct BatchLane {
   std::vector<Camera> cams;
   std::vector<const void*> worlds;       // per view: the world it draws (graph signature)
   std::vector<void*> destinations;       // per view: pinned host image to copy into (else hostImage)
-  uint32_t viewCount = 0, totalItems = 0, totalTiles = 0, shDegree = 0;
+  uint32_t viewCount = 0, totalItems = 0, totalTiles = 0, totalBins = 0, shDegree = 0;
   uint64_t totalPixels = 0;
   float gpuMs = 0;
   FrameCounters result{};

@@ -227,6 +227,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
   const int degree = std::max(0, std::min(frame.sh_degree, world.shDegree));
   const bool key16 = policy.sort_depth_bits == 16;
   const uint32_t tilesX = view.tilesX(), tilesY = view.tilesY();
+  const uint32_t binsX = view.binsX(), binsY = view.binsY();
   uint32_t* counters = static_cast<uint32_t*>(f.counters.ptr);
   FrameCounters* fc = view.counters;
   uint32_t* error = &fc->error;
@@ -289,8 +290,8 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     v.keys = static_cast<uint32_t*>(f.keys.ptr);
     v.projected = static_cast<Projected*>(f.projected.ptr);
     v.spans = static_cast<uint4*>(f.spans.ptr);
-    v.tilesX = tilesX;
-    v.tilesY = tilesY;
+    v.tilesX = binsX;
+    v.tilesY = binsY;
     v.visibleCount = &fc->visible;
     v.status = static_cast<uint64_t*>(f.visStatus.ptr);
     v.counters = counters + 0;
@@ -324,7 +325,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     b.order = static_cast<const uint32_t*>(f.order.ptr);
     b.count = &fc->visible;
     b.capacity = f.sources;
-    b.width = view.width, b.height = view.height, b.tilesX = tilesX, b.tilesY = tilesY;
+    b.width = view.width, b.height = view.height, b.tilesX = binsX, b.tilesY = binsY;
     b.instanceKeys = static_cast<uint32_t*>(f.instKeys.ptr);
     b.instanceValues = static_cast<uint32_t*>(f.instValues.ptr);
     b.instanceCapacity = f.instanceCapacity;
@@ -350,7 +351,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
   }
   if (e == cudaSuccess)
     e = launchTileRanges(static_cast<const uint32_t*>(f.instKeysSorted.ptr), &fc->instances,
-                         f.instanceCapacity, static_cast<uint2*>(f.ranges.ptr), tilesX * tilesY, s);
+                         f.instanceCapacity, static_cast<uint2*>(f.ranges.ptr), binsX * binsY, s);
   if (timed) cudaEventRecord(f.events[4], s);
   if (e == cudaSuccess) {
     CompositeArgs c{};
@@ -358,6 +359,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     c.values = static_cast<const uint32_t*>(f.instValuesSorted.ptr);
     c.ranges = static_cast<const uint2*>(f.ranges.ptr);
     c.width = view.width, c.height = view.height, c.tilesX = tilesX, c.tilesY = tilesY;
+    c.binsX = binsX;
     for (int j = 0; j < 3; ++j) c.background[j] = static_cast<float>(policy.background[j]);
     c.opaque = 1;
     c.cutoff = policy.enable_early_termination ? kTransmittanceCutoff : 0.0f;
@@ -863,8 +865,9 @@ sk_status sk_read_tile_lists(sk_context* handle, uint32_t* ranges, uint32_t* val
   const uint32_t n = std::min(ctx->lastCounters.instances, ctx->scratch.instanceCapacity);
   if (count) *count = n;
   cudaError_t e = cudaSuccess;
-  const size_t tiles = size_t{(ctx->width + 15) / 16} * ((ctx->height + 15) / 16);
-  if (ranges) e = cudaMemcpy(ranges, ctx->scratch.ranges.ptr, tiles * 8, cudaMemcpyDeviceToHost);
+  const size_t bins = size_t{(ctx->width + sk::kBinSize - 1) / sk::kBinSize} *
+                      ((ctx->height + sk::kBinSize - 1) / sk::kBinSize);
+  if (ranges) e = cudaMemcpy(ranges, ctx->scratch.ranges.ptr, bins * 8, cudaMemcpyDeviceToHost);
   const uint32_t copy = std::min(n, capacity);
   if (e == cudaSuccess && values && copy)
     e = cudaMemcpy(values, ctx->scratch.instValuesSorted.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);

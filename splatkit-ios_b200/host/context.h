@@ -104,6 +104,8 @@ struct ViewTarget {
   const Camera* camera = nullptr;          // device, written before the pipeline runs
   uint32_t tilesX() const { return (width + kTileSize - 1) / kTileSize; }
   uint32_t tilesY() const { return (height + kTileSize - 1) / kTileSize; }
+  uint32_t binsX() const { return (width + kBinSize - 1) / kBinSize; }
+  uint32_t binsY() const { return (height + kBinSize - 1) / kBinSize; }
 };
 
 // The per-view camera block of a frame on a width x height target.

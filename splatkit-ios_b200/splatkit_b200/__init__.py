@@ -576,9 +576,10 @@ class Renderer:
         return order
 
     def read_tile_lists(self):
-        """(ranges (tiles, 2), values): each 16x16 tile's front-to-back projected indices."""
-        tiles = ((self.width + 15) // 16) * ((self.height + 15) // 16)
-        ranges = np.zeros((tiles, 2), np.uint32)
+        """(ranges (cells, 2), values): each 32x32 binning cell's front-to-back projected indices
+        (a composite tile of 16x16 pixels reads the list of the cell it lies in)."""
+        cells = ((self.width + 31) // 32) * ((self.height + 31) // 32)
+        ranges = np.zeros((cells, 2), np.uint32)
         n = ctypes.c_uint32()
         self._check(self._lib.sk_read_tile_lists(self._h, _ptr(ranges, _u32p), None, 0,
                                                  ctypes.byref(n)), "tile lists")
