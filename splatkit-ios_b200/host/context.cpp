@@ -332,6 +332,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     b.instanceCount = &fc->instances;
     b.overflow = &fc->overflow;
     b.blockSums = static_cast<uint32_t*>(f.binSums.ptr);
+    b.balanced = 1;
     e = launchBinning(b, s);
   }
   if (e == cudaSuccess) {
