@@ -45,7 +45,8 @@ typedef struct {
   int32_t device;                /* CUDA device ordinal */
   uint32_t width, height;        /* draw extent of the headless target */
   int32_t image_format;          /* SK_FORMAT_RGBA8 or SK_FORMAT_RGBA32F on the device */
-  uint32_t time_stages;          /* 1: record per-stage CUDA events (stats); 0: none */
+  uint32_t time_stages;          /* 1: per-stage CUDA events (stats.*_ms); 2: frame events only
+                                    (stats.gpu_ms; keeps the stage kernels chained); 0: none */
 } sk_config;
 
 /* A SplatCloud (packages/splat-core/include/splat/formats/SplatCloud.h:30-51), structure of
@@ -245,6 +246,9 @@ sk_status sk_draw(sk_context* ctx, const sk_frame* frame);
 sk_status sk_read_image(sk_context* ctx, void* host, size_t bytes, int32_t format);
 sk_status sk_wait_idle(sk_context* ctx);
 sk_status sk_get_stats(sk_context* ctx, sk_stats* out);
+/* Switches the event timing of later frames (sk_config.time_stages' values); waits for the
+ * frame in flight first. */
+sk_status sk_set_timing(sk_context* ctx, uint32_t time_stages);
 
 /* Readbacks of the last frame for parity checks: the survivors in source order (keys and
  * 32-byte projected records), the depth order (indices into the projected records) and the

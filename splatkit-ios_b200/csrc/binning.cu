@@ -14,6 +14,7 @@
 
 #include "sk_device.cuh"
 #include "sk_kernels.h"
+#include "sk_launch.cuh"
 #include "sk_tiles.cuh"
 
 namespace sk {
@@ -25,6 +26,7 @@ constexpr uint32_t kTileSplats = kThreads * kItems;
 
 // Pass 1: instances per block of 1024 depth ranks (no waiting on other blocks).
 __global__ void __launch_bounds__(kThreads) binCountKernel(const __grid_constant__ BinArgs a) {
+  chainedKernelStart();
   __shared__ uint32_t warpSum[kThreads / 32];
   const uint32_t n = min(*a.count, a.capacity);
   const uint32_t block = blockIdx.x;
@@ -97,6 +99,7 @@ __device__ __forceinline__ TileGrid gridOf(const BinArgs& a, const ItemStage& st
 // view v when viewFirst[v] <= i < viewFirst[v + 1]); tile ids are batch-wide.
 template <bool kBatch, bool kBalanced>
 __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant__ BinArgs a) {
+  chainedKernelStart();
   __shared__ uint32_t warpBase[kThreads / 32];
   __shared__ ItemStage stage;
   __shared__ uint32_t tileBase;
@@ -252,6 +255,7 @@ __global__ void __launch_bounds__(kThreads) binEmitKernel(const __grid_constant_
 
 __global__ void rangesKernel(const uint32_t* __restrict__ keys, const uint32_t* count,
                              uint32_t capacity, uint2* ranges, uint32_t tiles) {
+  chainedKernelStart();
   const uint32_t n = min(*count, capacity);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t k = keys[i];
@@ -267,25 +271,28 @@ uint32_t binBlocks(uint32_t capacity) { return max(1u, (capacity + kTileSplats -
 
 cudaError_t launchBinning(const BinArgs& a, cudaStream_t stream) {
   const uint32_t grid = binBlocks(a.capacity);
-  binCountKernel<<<grid, kThreads, 0, stream>>>(a);
+  cudaError_t e = launchChained(binCountKernel, grid, kThreads, stream, a);
+  if (e != cudaSuccess) return e;
   if (a.viewCount > 0) {
-    if (a.balanced) binEmitKernel<true, true><<<grid, kThreads, 0, stream>>>(a);
-    else binEmitKernel<true, false><<<grid, kThreads, 0, stream>>>(a);
+    e = launchChained(a.balanced ? binEmitKernel<true, true> : binEmitKernel<true, false>, grid,
+                      kThreads, stream, a);
   } else {
-    if (a.balanced) binEmitKernel<false, true><<<grid, kThreads, 0, stream>>>(a);
-    else binEmitKernel<false, false><<<grid, kThreads, 0, stream>>>(a);
+    e = launchChained(a.balanced ? binEmitKernel<false, true> : binEmitKernel<false, false>, grid,
+                      kThreads, stream, a);
   }
-  return cudaGetLastError();
+  return e;
+}
+
+cudaError_t clearTileRanges(uint2* ranges, uint32_t tiles, cudaStream_t stream) {
+  return cudaMemsetAsync(ranges, 0, static_cast<size_t>(tiles) * sizeof(uint2), stream);
 }
 
 cudaError_t launchTileRanges(const uint32_t* sortedKeys, const uint32_t* instanceCount,
                              uint32_t instanceCapacity, uint2* ranges, uint32_t tiles,
                              cudaStream_t stream) {
-  cudaError_t e = cudaMemsetAsync(ranges, 0, static_cast<size_t>(tiles) * sizeof(uint2), stream);
-  if (e != cudaSuccess) return e;
   const uint32_t grid = max(1u, min(148u * 8u, (instanceCapacity + 255u) / 256u));
-  rangesKernel<<<grid, 256, 0, stream>>>(sortedKeys, instanceCount, instanceCapacity, ranges, tiles);
-  return cudaGetLastError();
+  return launchChained(rangesKernel, grid, 256, stream, sortedKeys, instanceCount, instanceCapacity,
+                       ranges, tiles);
 }
 
 }  // namespace sk

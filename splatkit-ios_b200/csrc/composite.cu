@@ -22,6 +22,7 @@
 
 #include "sk_device.cuh"
 #include "sk_kernels.h"
+#include "sk_launch.cuh"
 
 namespace sk {
 namespace {
@@ -166,6 +167,7 @@ __device__ __forceinline__ void writePixel(const CompositeArgs& a, const Target&
 // kBatch: block b is batch-wide tile b; its view is the last one whose first tile is <= b.
 template <int kFormat, bool kBatch>
 __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constant__ CompositeArgs a) {
+  chainedKernelStart();
   __shared__ CompositeSmem sm;
   Target t{a.width, a.height, a.tilesX, blockIdx.x, a.binsX, 0u, a.image};
   if constexpr (kBatch) {
@@ -267,14 +269,12 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
 cudaError_t launchComposite(const CompositeArgs& a, cudaStream_t stream) {
   const uint32_t tiles = a.viewCount > 0 ? a.batchTiles : a.tilesX * a.tilesY;
   if (tiles == 0) return cudaSuccess;
-  if (a.viewCount > 0) {
-    if (a.format == kRgba32f) compositeKernel<kRgba32f, true><<<tiles, kThreads, 0, stream>>>(a);
-    else compositeKernel<kRgba8, true><<<tiles, kThreads, 0, stream>>>(a);
-  } else {
-    if (a.format == kRgba32f) compositeKernel<kRgba32f, false><<<tiles, kThreads, 0, stream>>>(a);
-    else compositeKernel<kRgba8, false><<<tiles, kThreads, 0, stream>>>(a);
-  }
-  return cudaGetLastError();
+  const bool f32 = a.format == kRgba32f;
+  if (a.viewCount > 0)
+    return launchChained(f32 ? compositeKernel<kRgba32f, true> : compositeKernel<kRgba8, true>, tiles,
+                         kThreads, stream, a);
+  return launchChained(f32 ? compositeKernel<kRgba32f, false> : compositeKernel<kRgba8, false>, tiles,
+                       kThreads, stream, a);
 }
 
 }  // namespace sk

@@ -15,6 +15,7 @@
 
 #include "sk_device.cuh"
 #include "sk_kernels.h"
+#include "sk_launch.cuh"
 
 namespace sk {
 namespace {
@@ -34,6 +35,7 @@ __device__ __forceinline__ uint32_t clampCount(const uint32_t* count, uint32_t c
 __global__ void __launch_bounds__(kThreads)
     histogramKernel(const uint32_t* __restrict__ keys, const uint32_t* count, uint32_t capacity,
                     uint32_t passes, uint32_t* accum, uint32_t* bases, uint32_t* counters) {
+  chainedKernelStart();
   __shared__ uint32_t h[kMaxPasses][kBins];
   for (uint32_t i = threadIdx.x; i < kMaxPasses * kBins; i += kThreads) (&h[0][0])[i] = 0;
   __syncthreads();
@@ -110,6 +112,7 @@ __global__ void __launch_bounds__(kThreads)
                   const uint32_t* count, uint32_t capacity, uint32_t shift,
                   const uint32_t* __restrict__ digitBase, uint64_t* status, uint32_t* counters,
                   uint32_t epoch, uint32_t* error) {
+  chainedKernelStart();
   __shared__ ScatterSmem<kPer> s;
   constexpr uint32_t kTile = kThreads * kPer;
   const uint32_t tile = takeTile(counters);
@@ -277,8 +280,9 @@ cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
   uint32_t* accum = a.histogram;
   uint32_t* bases = a.histogram + kMaxPasses * kBins;
   const uint32_t histBlocks = min(sortTiles(a.capacity), 148u * 4u);
-  histogramKernel<<<histBlocks, kThreads, 0, stream>>>(a.keysIn, a.count, a.capacity, passes,
-                                                       accum, bases, a.counters);
+  cudaError_t e = launchChained(histogramKernel, histBlocks, kThreads, stream, a.keysIn, a.count,
+                                a.capacity, passes, accum, bases, a.counters);
+  if (e != cudaSuccess) return e;
   const uint32_t* kin = a.keysIn;
   const uint32_t* vin = a.valuesIn;
   for (uint32_t p = 0; p < passes; ++p) {
@@ -290,9 +294,9 @@ cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
     const bool implicit = p == 0 && vin == nullptr;
     const bool writeKeys = kout != nullptr;
 #define SK_SCATTER_PER(IMPLICIT, WRITE, PER)                                               \
-  scatterKernel<IMPLICIT, WRITE, PER><<<tiles, kThreads, 0, stream>>>(                     \
-      kin, vin, kout, vout, a.count, a.capacity, 8 * p, bases + p * kBins, a.status,      \
-      counters, epoch, a.error)
+  e = launchChained(scatterKernel<IMPLICIT, WRITE, PER>, tiles, kThreads, stream, kin, vin,  \
+                    kout, vout, a.count, a.capacity, 8 * p, bases + p * kBins, a.status,   \
+                    counters, epoch, a.error)
 #define SK_SCATTER(IMPLICIT, WRITE)                                                        \
   do {                                                                                     \
     if (tileKeys == 2048) SK_SCATTER_PER(IMPLICIT, WRITE, 8u);                             \
@@ -306,6 +310,7 @@ cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
     }
 #undef SK_SCATTER
 #undef SK_SCATTER_PER
+    if (e != cudaSuccess) return e;
     kin = kout;
     vin = vout;
   }

@@ -92,6 +92,17 @@ __device__ __forceinline__ float lnF32(float x) {
                    __fadd_rn(lnm, __fmul_rn(fe, 1.428606820309417e-06f)));
 }
 
+// ---- programmatic dependent launch --------------------------------------------------------
+// The frame's kernels are launched with programmatic stream serialization (launchChained): a
+// kernel's blocks may be dispatched while its predecessor's last blocks still run, which hides
+// the launch gap between dependent kernels. Every such kernel first waits for the predecessor
+// to finish and flush (griddepcontrol.wait; a no-op when launched without the attribute), then
+// lets its own successor be dispatched once all of its blocks are running.
+__device__ __forceinline__ void chainedKernelStart() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Copies the 208-byte camera from device memory into shared memory (the caller syncs).
 __device__ __forceinline__ void loadCamera(const Camera* __restrict__ src, Camera* dst) {
   constexpr uint32_t kWords = sizeof(Camera) / 4;

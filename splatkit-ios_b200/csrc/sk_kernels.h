@@ -121,7 +121,9 @@ uint32_t binBlocks(uint32_t capacity);
 cudaError_t launchBinning(const BinArgs& args, cudaStream_t stream);
 
 // Per binning cell, the [start, end) range of its entries in the cell-sorted instance keys.
-// ranges: one uint2 per cell, cleared by the launcher.
+// ranges: one uint2 per cell, cleared beforehand by clearTileRanges (cells with no entry keep
+// (0, 0)); the clear is issued early so the chained kernels of a frame run back to back.
+cudaError_t clearTileRanges(uint2* ranges, uint32_t tiles, cudaStream_t stream);
 cudaError_t launchTileRanges(const uint32_t* sortedKeys, const uint32_t* instanceCount,
                              uint32_t instanceCapacity, uint2* ranges, uint32_t tiles,
                              cudaStream_t stream);

@@ -14,6 +14,7 @@
 
 #include "sk_device.cuh"
 #include "sk_kernels.h"
+#include "sk_launch.cuh"
 #include "sk_tiles.cuh"
 
 namespace sk {
@@ -408,6 +409,7 @@ __device__ __forceinline__ void copyOutTile(const VisibilitySmem& s, uint32_t* k
 template <int D, bool kKey16, bool kIndexed>
 __global__ void __launch_bounds__(kThreads, 4)
     visibilityKernel(const Camera* __restrict__ camera, const __grid_constant__ VisibilityArgs a) {
+  chainedKernelStart();
   __shared__ VisibilitySmem s;
   __shared__ Camera cam;
   loadCamera(camera, &cam);
@@ -444,6 +446,7 @@ __global__ void __launch_bounds__(kThreads, 4)
 template <int D>
 __global__ void __launch_bounds__(kThreads, 4)
     visibilityBatchKernel(const __grid_constant__ BatchVisibilityArgs a) {
+  chainedKernelStart();
   __shared__ VisibilitySmem s;
   __shared__ Camera cam;
   __shared__ uint32_t viewOf;
@@ -491,7 +494,7 @@ __global__ void __launch_bounds__(kThreads, 4)
 
 template <int D, bool kKey16, bool kIndexed>
 void launchOne(const Camera* cam, const VisibilityArgs& a, uint32_t grid, cudaStream_t stream) {
-  visibilityKernel<D, kKey16, kIndexed><<<grid, kThreads, 0, stream>>>(cam, a);
+  launchChained(visibilityKernel<D, kKey16, kIndexed>, grid, kThreads, stream, cam, a);
 }
 
 template <int D>
@@ -514,10 +517,10 @@ cudaError_t launchVisibilityBatch(const BatchVisibilityArgs& args, int shDegree,
                                   cudaStream_t stream) {
   if (args.items == 0 || args.viewCount == 0) return cudaSuccess;
   switch (shDegree) {
-    case 0: visibilityBatchKernel<0><<<args.items, kThreads, 0, stream>>>(args); break;
-    case 1: visibilityBatchKernel<1><<<args.items, kThreads, 0, stream>>>(args); break;
-    case 2: visibilityBatchKernel<2><<<args.items, kThreads, 0, stream>>>(args); break;
-    default: visibilityBatchKernel<3><<<args.items, kThreads, 0, stream>>>(args); break;
+    case 0: launchChained(visibilityBatchKernel<0>, args.items, kThreads, stream, args); break;
+    case 1: launchChained(visibilityBatchKernel<1>, args.items, kThreads, stream, args); break;
+    case 2: launchChained(visibilityBatchKernel<2>, args.items, kThreads, stream, args); break;
+    default: launchChained(visibilityBatchKernel<3>, args.items, kThreads, stream, args); break;
   }
   return cudaGetLastError();
 }

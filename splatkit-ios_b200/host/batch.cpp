@@ -200,6 +200,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
   const auto* views = static_cast<const BatchView*>(l.viewTable.ptr);
   const auto* viewFirst = static_cast<const uint32_t*>(l.viewFirst.ptr);
   cudaError_t e = cudaMemsetAsync(fc, 0, sizeof(FrameCounters), s);
+  if (e == cudaSuccess) e = clearTileRanges(static_cast<uint2*>(l.ranges.ptr), l.totalBins, s);
   if (e == cudaSuccess && clearStatus) {
     e = cudaMemsetAsync(l.visStatus.ptr, 0, size_t{l.totalItems} * 8, s);
     SortArgs probe{};

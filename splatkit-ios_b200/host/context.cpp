@@ -223,7 +223,10 @@ sk_status Context::validateRanges(const sk_frame& frame, uint32_t* total) const 
 }
 
 sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, const sk_frame& frame,
-                                   uint32_t total, cudaStream_t s, bool timed) {
+                                   uint32_t total, cudaStream_t s, uint32_t timing) {
+  // Events between stages separate the chained launches, so frame-only timing records just
+  // the outer pair.
+  const bool timed = timing == 1;
   const int degree = std::max(0, std::min(frame.sh_degree, world.shDegree));
   const bool key16 = policy.sort_depth_bits == 16;
   const uint32_t tilesX = view.tilesX(), tilesY = view.tilesY();
@@ -232,7 +235,8 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
   FrameCounters* fc = view.counters;
   uint32_t* error = &fc->error;
   cudaError_t e = cudaMemsetAsync(fc, 0, sizeof(FrameCounters), s);
-  if (timed) cudaEventRecord(f.events[0], s);
+  if (e == cudaSuccess) e = clearTileRanges(static_cast<uint2*>(f.ranges.ptr), binsX * binsY, s);
+  if (timing != 0) cudaEventRecord(f.events[0], s);
 
   const bool lod = world.lod;
   if (lod && e == cudaSuccess) {
@@ -370,7 +374,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     c.loaded = &fc->loaded;
     e = launchComposite(c, s);
   }
-  if (timed) cudaEventRecord(f.events[5], s);
+  if (timing != 0) cudaEventRecord(f.events[5], s);
   if (e == cudaSuccess && view.hostCounters)
     e = cudaMemcpyAsync(view.hostCounters, fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s);
   return check(e, "frame");
@@ -423,9 +427,10 @@ sk_status Context::finishFrame(bool wait) {
     return finishFrame(true);
   }
   lastCounters = c;
-  if (timeStages) {
+  if (timeStages != 0) {
     float ms[5] = {0, 0, 0, 0, 0};
-    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], scratch.events[i], scratch.events[i + 1]);
+    if (timeStages == 1)
+      for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], scratch.events[i], scratch.events[i + 1]);
     float all = 0;
     cudaEventElapsedTime(&all, scratch.events[0], scratch.events[5]);
     stats.select_ms = ms[0], stats.cull_ms = ms[1], stats.sort_ms = ms[2];
@@ -501,7 +506,7 @@ sk_status sk_create(const sk_config* config, sk_context** out) {
   ctx->width = config->width;
   ctx->height = config->height;
   ctx->imageFormat = config->image_format;
-  ctx->timeStages = config->time_stages != 0;
+  ctx->timeStages = std::min<uint32_t>(config->time_stages, 2);
   sk_default_policy(&ctx->policy);
   ctx->threshold.reset(ctx->policy.lod_error_pixels);
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SK_E_DEVICE;
@@ -792,6 +797,15 @@ sk_status sk_read_image(sk_context* handle, void* host, size_t bytes, int32_t fo
     if (format == SK_FORMAT_BGRA8) std::swap(rgba[0], rgba[2]);
     std::memcpy(out + i * 4, rgba, 4);
   }
+  return SK_OK;
+}
+
+sk_status sk_set_timing(sk_context* handle, uint32_t time_stages) {
+  SK_CTX(handle);
+  if (time_stages > 2) return SK_E_INVALID;
+  const sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  ctx->timeStages = time_stages;
   return SK_OK;
 }
 

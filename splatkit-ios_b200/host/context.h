@@ -116,7 +116,7 @@ struct Context {
   cudaStream_t stream = nullptr;
   uint32_t width = 0, height = 0;
   int imageFormat = SK_FORMAT_RGBA8;
-  bool timeStages = true;
+  uint32_t timeStages = 1;  // 0 none, 1 per stage, 2 frame only
   sk_policy policy{};
   uint32_t lodLimit = 0;
   host::LodThreshold threshold;
@@ -154,7 +154,7 @@ struct Context {
   sk_status validateRanges(const sk_frame& frame, uint32_t* total) const;
   // The whole frame pipeline for one view on stream s; nothing waits on the host.
   sk_status enqueuePipeline(FrameScratch& f, const ViewTarget& v, const sk_frame& frame,
-                            uint32_t total, cudaStream_t s, bool timed);
+                            uint32_t total, cudaStream_t s, uint32_t timing);
   ViewTarget plainView();
   sk_status enqueuePlainFrame(const sk_frame& frame, uint32_t total);
   sk_status finishFrame(bool wait);

@@ -199,6 +199,7 @@ _SIGNATURES = {
                                        ctypes.c_int32]),
     "sk_wait_idle": (ctypes.c_int32, [ctypes.c_void_p]),
     "sk_get_stats": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Stats)]),
+    "sk_set_timing": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     "sk_read_visible": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_void_p, ctypes.c_uint32,
                                          _u32p]),
     "sk_read_order": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_uint32, _u32p]),
@@ -425,9 +426,11 @@ class Renderer:
     """A headless splat renderer on one CUDA device (``CudaSplatRenderer``'s Python mirror)."""
 
     def __init__(self, width: int, height: int, device: int = 0, image_format: int = FORMAT_RGBA8,
-                 time_stages: bool = True):
+                 time_stages: bool | str = True):
+        # True: per-stage events; "frame": the frame's own pair only (stage kernels stay chained)
         self._lib = library()
-        cfg = _Config(device, width, height, image_format, 1 if time_stages else 0)
+        timing = 2 if time_stages == "frame" else (1 if time_stages else 0)
+        cfg = _Config(device, width, height, image_format, timing)
         handle = ctypes.c_void_p()
         st = self._lib.sk_create(ctypes.byref(cfg), ctypes.byref(handle))
         if st != SK_OK:
@@ -471,6 +474,11 @@ class Renderer:
     def apply_render_policy(self, policy: Policy):
         p = policy.native()
         self._check(self._lib.sk_apply_render_policy(self._h, ctypes.byref(p)), "policy")
+
+    def set_timing(self, time_stages: bool | str):
+        """True: per-stage events; "frame": the frame's own pair only; False: none."""
+        timing = 2 if time_stages == "frame" else (1 if time_stages else 0)
+        self._check(self._lib.sk_set_timing(self._h, timing), "timing")
 
     def available_memory(self) -> int:
         v = ctypes.c_uint64()
