@@ -249,6 +249,13 @@ sk_status sk_get_stats(sk_context* ctx, sk_stats* out);
 /* Switches the event timing of later frames (sk_config.time_stages' values); waits for the
  * frame in flight first. */
 sk_status sk_set_timing(sk_context* ctx, uint32_t time_stages);
+/* How each binning cell's front-to-back list is built. SK_BINNING_AUTO: written in place from
+ * per-block cell counts when the target has at most 4096 cells (32 x 32 pixels each), else by
+ * a stable sort of (cell, splat) pairs; SK_BINNING_SORTED: always the sort. Both give the same
+ * lists. Waits for the frame in flight first. */
+#define SK_BINNING_AUTO 0u
+#define SK_BINNING_SORTED 1u
+sk_status sk_set_binning(sk_context* ctx, uint32_t mode);
 
 /* Readbacks of the last frame for parity checks: the survivors in source order (keys and
  * 32-byte projected records), the depth order (indices into the projected records) and the

@@ -56,30 +56,11 @@ struct ItemStage {
   uint32_t total;
 };
 
-// Position of the k-th (from 0) set bit of x; x holds more than k set bits. Bisection on halves.
-__device__ __forceinline__ uint32_t kthSetBit(uint32_t x, uint32_t k) {
-  uint32_t pos = 0;
-#pragma unroll
-  for (uint32_t width = 16; width > 0; width >>= 1) {
-    const uint32_t low = __popc(x & ((1u << width) - 1u));
-    if (k >= low) {
-      k -= low;
-      x >>= width;
-      pos += width;
-    }
-  }
-  return pos;
-}
-
-// The tile ids of one item's box: id(b) for box position b = row * w + col.
+// The tile ids of one item's box: id(b) for box position b = row * w + col (boxCell).
 struct TileGrid {
   uint32_t rowStart, tilesX;
-  // b / w for b < area <= 16641 and w <= 129: (b + 1/2) / w is at least 1/(2w) away from an
-  // integer and the float product errs by far less, so truncation gives the quotient.
   __device__ __forceinline__ uint32_t id(uint32_t b, uint32_t w) const {
-    const uint32_t q = static_cast<uint32_t>((static_cast<float>(b) + 0.5f) *
-                                             __frcp_rn(static_cast<float>(w)));
-    return rowStart + q * tilesX + (b - q * w);
+    return boxCell(rowStart, b, w, tilesX);
   }
 };
 

@@ -1,0 +1,332 @@
+// Direct cell-major lists: each binning cell's front-to-back list of survivors, written in place.
+//
+// Binning + a stable sort of (cell, projected index) pairs by cell + a ranges pass build the
+// same lists (binning.cu, radix_sort.cu). On a target of at most kDirectMaxCells cells this file
+// builds them without the sort:
+//   1. count: every block of 1024 depth ranks histograms its instances by cell;
+//   2. scan: per cell, the running sum of the block histograms (32 cells per block of this pass,
+//      the rows held in registers) gives each block's first slot in the cell's list; the lists'
+//      starts come from a decoupled look-back across the groups of 32 cells, in cell order; the
+//      ranges and the instance count follow;
+//   3. emit: every block histograms its 8 warps' ranks (128 each) by cell again, so that warp w
+//      starts each cell after warps 0..w-1, then each warp walks its output 32 entries at a time
+//      in depth order and writes each entry at its cell's next slot (lanes of one round that
+//      share a cell take consecutive slots).
+// Entries of a cell therefore appear in depth order, which is exactly what the stable sort
+// gives.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "sk_device.cuh"
+#include "sk_kernels.h"
+#include "sk_launch.cuh"
+#include "sk_tiles.cuh"
+
+namespace sk {
+namespace {
+
+constexpr uint32_t kThreads = 256;
+constexpr uint32_t kWarps = kThreads / 32;
+constexpr uint32_t kItems = 4;                    // ranks per lane
+constexpr uint32_t kChunk = 32 * kItems;          // ranks per warp
+constexpr uint32_t kBlockRanks = kThreads * kItems;  // 1024
+constexpr uint32_t kScanThreads = 1024;
+constexpr uint32_t kScanWarps = kScanThreads / 32;
+constexpr uint32_t kRowsInRegisters = 32;         // block rows one scan warp keeps
+
+struct Work {
+  uint32_t* blockCounts;  // blocks x cells
+  uint32_t* blockStarts;  // blocks x cells: the block's first slot in each cell's list
+  uint64_t* status;       // one look-back word per group of 32 cells
+};
+
+__host__ __device__ inline uint32_t cellWords(uint32_t cells) { return (cells + 1) / 2; }
+__host__ __device__ inline size_t align16(size_t n) { return (n + 15) & ~size_t{15}; }
+__host__ __device__ inline uint32_t cellGroups(uint32_t cells) { return (cells + 31) / 32; }
+__host__ __device__ inline uint32_t blocksFor(uint32_t capacity) {
+  return (capacity + kBlockRanks - 1) / kBlockRanks;
+}
+
+__host__ __device__ inline Work workOf(void* workspace, uint32_t blocks, uint32_t cells) {
+  uint8_t* p = static_cast<uint8_t*>(workspace);
+  Work w;
+  w.blockCounts = reinterpret_cast<uint32_t*>(p);
+  p += align16(size_t{blocks} * cells * 4);
+  w.blockStarts = reinterpret_cast<uint32_t*>(p);
+  p += align16(size_t{blocks} * cells * 4);
+  w.status = reinterpret_cast<uint64_t*>(p);
+  return w;
+}
+
+size_t workBytes(uint32_t blocks, uint32_t cells) {
+  return 2 * align16(size_t{blocks} * cells * 4) + size_t{cellGroups(cells)} * 8;
+}
+
+// Pass 1: each block's instances per cell.
+__global__ void __launch_bounds__(kThreads)
+    cellCountKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells) {
+  chainedKernelStart();
+  __shared__ uint32_t hist[kDirectMaxCells];
+  const uint32_t n = min(*a.count, a.capacity);
+  const uint32_t begin = blockIdx.x * kBlockRanks;
+  if (begin >= n) return;  // rows of idle blocks are never read
+  for (uint32_t c = threadIdx.x; c < cells; c += kThreads) hist[c] = 0;
+  __syncthreads();
+  uint32_t value[kItems];
+  uint4 span[kItems];
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r) {
+    const uint32_t i = begin + r * kThreads + threadIdx.x;
+    value[r] = i < n ? __ldg(a.order + i) : 0xffffffffu;
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r)
+    span[r] = value[r] != 0xffffffffu ? __ldg(a.spans + value[r]) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r)
+    visitCells(span[r], a.tilesX, [](uint32_t c) { atomicAdd(&hist[c], 1u); });
+  __syncthreads();
+  uint32_t* row = work.blockCounts + size_t{blockIdx.x} * cells;
+  for (uint32_t c = threadIdx.x; c < cells; c += kThreads) row[c] = hist[c];
+}
+
+// Pass 2: one block per group of 32 cells (groups handed out in start order, so a group only
+// waits on groups already running). Lane = cell of the group; warp w scans a contiguous share
+// of the block rows, the first 32 of them kept in registers between the two sweeps.
+__global__ void __launch_bounds__(kScanThreads, 1)
+    cellScanKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells, uint2* ranges,
+                   uint32_t* counters, uint32_t epoch, uint32_t* error) {
+  chainedKernelStart();
+  __shared__ uint32_t part[kScanWarps][33];
+  __shared__ uint32_t cellStart[32];
+  const uint32_t group = takeTile(counters);
+  const uint32_t n = min(*a.count, a.capacity);
+  const uint32_t active = blocksFor(n);
+  const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+  const uint32_t cell = group * 32 + lane;
+  const bool valid = cell < cells;
+  const uint32_t share = (active + kScanWarps - 1) / kScanWarps;
+  const uint32_t r0 = min(warp * share, active), r1 = min(r0 + share, active);
+  const uint32_t* counts = work.blockCounts + cell;
+  uint32_t v[kRowsInRegisters];
+  uint32_t sum = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kRowsInRegisters; ++k) {
+    const uint32_t row = r0 + k;
+    v[k] = valid && row < r1 ? __ldcg(counts + size_t{row} * cells) : 0u;
+    sum += v[k];
+  }
+  if (valid)
+    for (uint32_t row = r0 + kRowsInRegisters; row < r1; ++row)
+      sum += __ldcg(counts + size_t{row} * cells);
+  part[warp][lane] = sum;
+  __syncthreads();
+  uint32_t run = 0;
+  for (uint32_t w = 0; w < warp; ++w) run += part[w][lane];
+  if (warp == 0) {
+    uint32_t total = 0;
+    for (uint32_t w = 0; w < kScanWarps; ++w) total += part[w][lane];
+    uint32_t inc = total;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= static_cast<uint32_t>(o)) inc += up;
+    }
+    const uint32_t aggregate = __shfl_sync(0xffffffffu, inc, 31);
+    uint32_t before = 0;
+    if (group == 0) {
+      if (lane == 0) storeStatus(work.status, makeStatus(epoch, kFlagPrefix, aggregate));
+    } else {
+      if (lane == 0) storeStatus(work.status + group, makeStatus(epoch, kFlagAggregate, aggregate));
+      before = warpLookback(work.status, group, epoch, error);
+      if (lane == 0)
+        storeStatus(work.status + group, makeStatus(epoch, kFlagPrefix, before + aggregate));
+    }
+    const uint32_t start = before + inc - total;
+    cellStart[lane] = start;
+    if (valid)
+      ranges[cell] = make_uint2(min(start, a.instanceCapacity),
+                                min(start + total, a.instanceCapacity));
+    if (group == gridDim.x - 1 && lane == 31) {
+      *a.instanceCount = before + aggregate;
+      *a.overflow = before + aggregate > a.instanceCapacity ? 1u : 0u;
+    }
+  }
+  __syncthreads();
+  if (valid) {
+    run += cellStart[lane];
+    uint32_t* starts = work.blockStarts + cell;
+#pragma unroll
+    for (uint32_t k = 0; k < kRowsInRegisters; ++k) {
+      const uint32_t row = r0 + k;
+      if (row < r1) starts[size_t{row} * cells] = run;
+      run += v[k];
+    }
+    for (uint32_t row = r0 + kRowsInRegisters; row < r1; ++row) {
+      starts[size_t{row} * cells] = run;
+      run += __ldcg(counts + size_t{row} * cells);
+    }
+  }
+  finishTile(counters);
+}
+
+// Pass 3. Dynamic shared memory: kWarps x words per-warp slot counters (16-bit halves: a warp's
+// slots count from the block's first slot in the cell, at most 1024 on), then each cell's first
+// slot for the block.
+__global__ void __launch_bounds__(kThreads)
+    cellEmitKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells) {
+  chainedKernelStart();
+  extern __shared__ uint32_t cellSmem[];
+  __shared__ uint4 stageSpan[kWarps][kChunk];
+  __shared__ uint32_t stageValue[kWarps][kChunk];
+  __shared__ uint32_t stageOffset[kWarps][kChunk];
+  __shared__ uint32_t startItem[kWarps][32];
+  const uint32_t n = min(*a.count, a.capacity);
+  const uint32_t begin = blockIdx.x * kBlockRanks;
+  if (begin >= n) return;
+  const uint32_t words = cellWords(cells);
+  uint32_t* slots = cellSmem;
+  uint32_t* where = cellSmem + kWarps * words;
+  for (uint32_t i = threadIdx.x; i < kWarps * words; i += kThreads) slots[i] = 0;
+  const uint32_t* starts = work.blockStarts + size_t{blockIdx.x} * cells;
+  for (uint32_t c = threadIdx.x; c < cells; c += kThreads) where[c] = __ldcg(starts + c);
+  __syncthreads();
+
+  const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+  uint32_t* mine = slots + warp * words;
+  uint4* sSpan = stageSpan[warp];
+  uint32_t* sValue = stageValue[warp];
+  uint32_t* sOffset = stageOffset[warp];
+  uint32_t* sStart = startItem[warp];
+  uint32_t value[kItems];
+  uint4 span[kItems];
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r) {
+    const uint32_t i = begin + warp * kChunk + r * 32 + lane;
+    value[r] = i < n ? __ldg(a.order + i) : 0xffffffffu;
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r) {
+    span[r] = value[r] != 0xffffffffu ? __ldg(a.spans + value[r]) : make_uint4(0, 0, 0, 0);
+    visitCells(span[r], a.tilesX,
+               [mine](uint32_t c) { atomicAdd(mine + (c >> 1), 1u << ((c & 1u) * 16)); });
+  }
+  // the warp's items in (row, lane) order = depth order, with their first output position
+  uint32_t total = 0;
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r) {
+    const uint32_t cnt = spanCount(span[r]);
+    uint32_t inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= static_cast<uint32_t>(o)) inc += up;
+    }
+    sSpan[r * 32 + lane] = span[r];
+    sValue[r * 32 + lane] = value[r];
+    sOffset[r * 32 + lane] = total + inc - cnt;
+    total += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  __syncthreads();
+  // warp w's first slot per cell: the counts of warps 0..w-1 (both halves of a word at once)
+  for (uint32_t q = threadIdx.x; q < words; q += kThreads) {
+    uint32_t run = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kWarps; ++w) {
+      const uint32_t v = slots[w * words + q];
+      slots[w * words + q] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+
+  // Output position p of the warp belongs to the last item whose offset is <= p. Per round of
+  // 32 positions, the items that open inside the round (offset in [p0, p0 + 32) and at least one
+  // entry) mark their offset in a bit mask, and a lane takes the last mark at or before it, or
+  // the item that held the round's first position.
+  const uint32_t below = lanemaskLt();
+  int cur = -1;           // the item holding position p0
+  uint32_t curStart = 0;  // its offset
+  for (uint32_t p0 = 0; p0 < total; p0 += 32) {
+    uint32_t opening = 0;
+    for (int base = cur + 1; base < static_cast<int>(kChunk); base += 32) {
+      const int j = base + static_cast<int>(lane);
+      const uint32_t s = j < static_cast<int>(kChunk) ? sOffset[j] : 0xffffffffu;
+      uint32_t next = __shfl_down_sync(0xffffffffu, s, 1);  // the following item's offset
+      if (lane == 31 || j + 1 >= static_cast<int>(kChunk))
+        next = j + 1 < static_cast<int>(kChunk) ? sOffset[j + 1] : total;
+      const bool inside = s < p0 + 32;
+      const bool opens = inside && next > s;
+      if (opens) sStart[s - p0] = static_cast<uint32_t>(j);
+      opening |= __reduce_or_sync(0xffffffffu, opens ? 1u << (s - p0) : 0u);
+      if (!__shfl_sync(0xffffffffu, inside, 31)) break;
+    }
+    __syncwarp();
+    const uint32_t p = p0 + lane;
+    const uint32_t upTo = opening & (0xffffffffu >> (31 - lane));
+    int item = cur;
+    uint32_t itemStart = curStart;
+    if (upTo != 0u) {
+      const uint32_t h = 31 - __clz(upTo);
+      item = static_cast<int>(sStart[h]);
+      itemStart = p0 + h;
+    }
+    cur = __shfl_sync(0xffffffffu, item, 31);
+    curStart = __shfl_sync(0xffffffffu, itemStart, 31);
+    const bool valid = p < total;
+    uint32_t cell = 0xffffffffu, val = 0;
+    if (valid) {
+      cell = spanCell(sSpan[item], p - itemStart, a.tilesX);
+      val = sValue[item];
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, cell);
+    const uint32_t half = (cell & 1u) * 16;
+    uint32_t slot = 0;
+    if (valid) slot = where[cell] + ((mine[cell >> 1] >> half) & 0xffffu) + __popc(peers & below);
+    __syncwarp();
+    if (valid && lane == 31 - __clz(peers)) atomicAdd(mine + (cell >> 1), __popc(peers) << half);
+    __syncwarp();
+    if (valid && slot < a.instanceCapacity) a.instanceValues[slot] = val;
+  }
+}
+
+size_t emitDynamicBytes(uint32_t cells) {
+  return (size_t{kWarps} * cellWords(cells) + cells) * sizeof(uint32_t);
+}
+
+}  // namespace
+
+bool cellListsFit(uint32_t capacity, uint32_t cells) {
+  return cells > 0 && cells <= kDirectMaxCells && capacity > 0;
+}
+
+size_t cellListBytes(uint32_t capacity, uint32_t cells) {
+  return workBytes(blocksFor(std::max(capacity, 1u)), std::max(cells, 1u));
+}
+
+cudaError_t launchCellLists(const BinArgs& a, const CellLists& lists, cudaStream_t stream) {
+  const uint32_t cells = lists.cells;
+  if (!cellListsFit(a.capacity, cells) || cells != a.tilesX * a.tilesY)
+    return cudaErrorInvalidValue;
+  static bool configured = false;
+  if (!configured) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(cellEmitKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(emitDynamicBytes(kDirectMaxCells)));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const uint32_t blocks = blocksFor(a.capacity);
+  const Work work = workOf(lists.workspace, blocks, cells);
+  cudaError_t e = launchChained(cellCountKernel, blocks, kThreads, stream, a, work, cells);
+  if (e != cudaSuccess) return e;
+  e = launchChained(cellScanKernel, cellGroups(cells), kScanThreads, stream, a, work, cells,
+                    lists.ranges, lists.counters, lists.epoch, lists.error);
+  if (e != cudaSuccess) return e;
+  return launchChainedShared(cellEmitKernel, blocks, kThreads, emitDynamicBytes(cells), stream, a,
+                             work, cells);
+}
+
+}  // namespace sk

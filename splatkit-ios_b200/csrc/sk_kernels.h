@@ -128,6 +128,26 @@ cudaError_t launchTileRanges(const uint32_t* sortedKeys, const uint32_t* instanc
                              uint32_t instanceCapacity, uint2* ranges, uint32_t tiles,
                              cudaStream_t stream);
 
+// Direct cell-major lists (cell_lists.cu): the per-cell lists that binning + stable tile sort +
+// ranges produce, written in place on targets of at most kDirectMaxCells binning cells. A count
+// pass histograms every block of 1024 depth ranks by cell, a scan pass turns the histograms
+// into each block's first position in every cell's list (and the lists' ranges, by look-back
+// across groups of cells), and the emission pass writes each instance there in depth order.
+// args.instanceValues receives the lists; instanceKeys and blockSums are unused.
+constexpr uint32_t kDirectMaxCells = 4096;
+struct CellLists {
+  uint32_t cells;       // binning cells of the target (args.tilesX * args.tilesY)
+  void* workspace;      // cellListBytes(capacity, cells), no clearing needed
+  uint2* ranges;        // per cell [start, end), clamped to the instance capacity
+  uint32_t* counters;   // two words, zero before the first launch (each launch restores them)
+  uint32_t epoch;       // look-back epoch, fresh per launch
+  uint32_t* error;      // SK_DEVERR_* bits
+};
+// Whether a target of `cells` cells takes the direct path.
+bool cellListsFit(uint32_t capacity, uint32_t cells);
+size_t cellListBytes(uint32_t capacity, uint32_t cells);
+cudaError_t launchCellLists(const BinArgs& args, const CellLists& lists, cudaStream_t stream);
+
 // ---- composite (composite.cu) ----------------------------------------------------------
 enum PixelFormat : int { kRgba8 = 0, kRgba32f = 1 };
 struct CompositeArgs {

@@ -9,12 +9,12 @@
 namespace sk {
 
 template <typename... Params, typename... Args>
-cudaError_t launchChained(void (*kernel)(Params...), dim3 grid, dim3 block, cudaStream_t stream,
-                          Args&&... args) {
+cudaError_t launchChainedShared(void (*kernel)(Params...), dim3 grid, dim3 block,
+                                size_t dynamicSmemBytes, cudaStream_t stream, Args&&... args) {
   cudaLaunchConfig_t config{};
   config.gridDim = grid;
   config.blockDim = block;
-  config.dynamicSmemBytes = 0;
+  config.dynamicSmemBytes = dynamicSmemBytes;
   config.stream = stream;
   cudaLaunchAttribute attribute[1];
   attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -22,6 +22,12 @@ cudaError_t launchChained(void (*kernel)(Params...), dim3 grid, dim3 block, cuda
   config.attrs = attribute;
   config.numAttrs = 1;
   return cudaLaunchKernelEx(&config, kernel, std::forward<Args>(args)...);
+}
+
+template <typename... Params, typename... Args>
+cudaError_t launchChained(void (*kernel)(Params...), dim3 grid, dim3 block, cudaStream_t stream,
+                          Args&&... args) {
+  return launchChainedShared(kernel, grid, block, 0, stream, std::forward<Args>(args)...);
 }
 
 }  // namespace sk

@@ -86,4 +86,67 @@ __device__ __forceinline__ uint32_t spanCount(const uint4 s) {
   return static_cast<uint32_t>(__popc(s.z) + __popc(s.w));
 }
 
+// Position of the k-th (from 0) set bit of x; x holds more than k set bits. Bisection on halves.
+__device__ __forceinline__ uint32_t kthSetBit(uint32_t x, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t width = 16; width > 0; width >>= 1) {
+    const uint32_t low = __popc(x & ((1u << width) - 1u));
+    if (k >= low) {
+      k -= low;
+      x >>= width;
+      pos += width;
+    }
+  }
+  return pos;
+}
+
+// Cell of box position b of a box w cells wide whose first cell is `first`, on a grid tilesX
+// cells wide. b / w in float: (b + 1/2) / w lies at least 1/(2w) from an integer, and the fast
+// divide errs by at most 2 ulp of the quotient, less than that for b < 2^19 (a box holds at most
+// 512 x 512 cells), so truncation gives the quotient.
+__device__ __forceinline__ uint32_t boxCell(uint32_t first, uint32_t b, uint32_t w,
+                                            uint32_t tilesX) {
+  const uint32_t q = static_cast<uint32_t>(
+      __fdividef(static_cast<float>(b) + 0.5f, static_cast<float>(w)));
+  return first + q * tilesX + (b - q * w);
+}
+
+// First cell of a span's box on a grid tilesX cells wide.
+__device__ __forceinline__ uint32_t spanFirstCell(const uint4 s, uint32_t tilesX) {
+  return (s.x >> 16) * tilesX + (s.x & 0xffffu);
+}
+
+// The k-th (from 0) cell a span lists, k < spanCount(s).
+__device__ __forceinline__ uint32_t spanCell(const uint4 s, uint32_t k, uint32_t tilesX) {
+  const uint32_t w = s.y & 0xffffu, area = s.y >> 16;
+  uint32_t bit = k;
+  if (area <= 64) {
+    const uint32_t nlo = __popc(s.z);
+    bit = k < nlo ? kthSetBit(s.z, k) : 32u + kthSetBit(s.w, k - nlo);
+  }
+  return boxCell(spanFirstCell(s, tilesX), bit, w, tilesX);
+}
+
+// visit(cell) for every cell a span lists. A masked span is walked by its own lane; a box of
+// more than 64 cells by the whole warp. Every lane of the warp calls this.
+template <typename Visit>
+__device__ __forceinline__ void visitCells(const uint4 s, uint32_t tilesX, Visit visit) {
+  const uint32_t w = s.y & 0xffffu, area = s.y >> 16;
+  const uint32_t first = spanFirstCell(s, tilesX);
+  if (area <= 64) {
+    for (uint32_t m = s.z; m != 0u; m &= m - 1) visit(boxCell(first, __ffs(m) - 1, w, tilesX));
+    for (uint32_t m = s.w; m != 0u; m &= m - 1) visit(boxCell(first, 31 + __ffs(m), w, tilesX));
+  }
+  uint32_t big = __ballot_sync(0xffffffffu, area > 64);
+  while (big != 0u) {
+    const uint32_t src = __ffs(big) - 1;
+    big &= big - 1;
+    const uint32_t bw = __shfl_sync(0xffffffffu, w, src);
+    const uint32_t barea = __shfl_sync(0xffffffffu, area, src);
+    const uint32_t bfirst = __shfl_sync(0xffffffffu, first, src);
+    for (uint32_t k = threadIdx.x & 31u; k < barea; k += 32) visit(boxCell(bfirst, k, bw, tilesX));
+  }
+}
+
 }  // namespace sk

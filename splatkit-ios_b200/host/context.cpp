@@ -124,6 +124,7 @@ sk_status Context::reserveScratch(FrameScratch& f, uint32_t sources, uint32_t in
   grab(f.instValuesSorted, size_t{instances} * 4);
   grab(f.tileSortWorkspace, sortWorkspaceBytesFor(instances, kTileSortTileKeys));
   grab(f.ranges, size_t{maxTiles} * sizeof(uint2));
+  grab(f.cellLists, cellListBytes(sources, std::min(std::max(maxTiles, f.maxTiles), kDirectMaxCells)));
   grab(f.rangeBuffer, size_t{kMaxRanges} * sizeof(Range));
   grab(f.rangeStarts, size_t{kMaxRanges + 1} * 4);
   const bool fresh = f.counters.ptr == nullptr;
@@ -234,8 +235,12 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
   uint32_t* counters = static_cast<uint32_t*>(f.counters.ptr);
   FrameCounters* fc = view.counters;
   uint32_t* error = &fc->error;
+  // Direct cell lists write every range; the sorted path only those of non-empty cells.
+  const uint32_t cells = binsX * binsY;
+  const bool direct = binningMode == SK_BINNING_AUTO && cellListsFit(f.sources, cells) &&
+                      f.cellLists.bytes >= cellListBytes(f.sources, cells);
   cudaError_t e = cudaMemsetAsync(fc, 0, sizeof(FrameCounters), s);
-  if (e == cudaSuccess) e = clearTileRanges(static_cast<uint2*>(f.ranges.ptr), binsX * binsY, s);
+  if (e == cudaSuccess && !direct) e = clearTileRanges(static_cast<uint2*>(f.ranges.ptr), cells, s);
   if (timing != 0) cudaEventRecord(f.events[0], s);
 
   const bool lod = world.lod;
@@ -323,7 +328,28 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     e = launchSort(a, s);
   }
   if (timed) cudaEventRecord(f.events[3], s);
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess && direct) {
+    // each cell's list written in place, front to back, with its range
+    BinArgs b{};
+    b.spans = static_cast<const uint4*>(f.spans.ptr);
+    b.order = static_cast<const uint32_t*>(f.order.ptr);
+    b.count = &fc->visible;
+    b.capacity = f.sources;
+    b.width = view.width, b.height = view.height, b.tilesX = binsX, b.tilesY = binsY;
+    b.instanceValues = static_cast<uint32_t*>(f.instValuesSorted.ptr);
+    b.instanceCapacity = f.instanceCapacity;
+    b.instanceCount = &fc->instances;
+    b.overflow = &fc->overflow;
+    CellLists cl{};
+    cl.cells = cells;
+    cl.workspace = f.cellLists.ptr;
+    cl.ranges = static_cast<uint2*>(f.ranges.ptr);
+    cl.counters = counters + 8;
+    cl.epoch = nextEpoch(1);
+    cl.error = error;
+    e = launchCellLists(b, cl, s);
+  }
+  if (e == cudaSuccess && !direct) {
     BinArgs b{};
     b.spans = static_cast<const uint4*>(f.spans.ptr);
     b.order = static_cast<const uint32_t*>(f.order.ptr);
@@ -339,7 +365,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     b.balanced = 1;
     e = launchBinning(b, s);
   }
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess && !direct) {
     SortArgs a{};
     a.keysIn = static_cast<const uint32_t*>(f.instKeys.ptr);
     a.valuesIn = static_cast<const uint32_t*>(f.instValues.ptr);
@@ -354,7 +380,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     a.error = error;
     e = launchSort(a, s);
   }
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && !direct)
     e = launchTileRanges(static_cast<const uint32_t*>(f.instKeysSorted.ptr), &fc->instances,
                          f.instanceCapacity, static_cast<uint2*>(f.ranges.ptr), binsX * binsY, s);
   if (timed) cudaEventRecord(f.events[4], s);
@@ -797,6 +823,15 @@ sk_status sk_read_image(sk_context* handle, void* host, size_t bytes, int32_t fo
     if (format == SK_FORMAT_BGRA8) std::swap(rgba[0], rgba[2]);
     std::memcpy(out + i * 4, rgba, 4);
   }
+  return SK_OK;
+}
+
+sk_status sk_set_binning(sk_context* handle, uint32_t mode) {
+  SK_CTX(handle);
+  if (mode != SK_BINNING_AUTO && mode != SK_BINNING_SORTED) return SK_E_INVALID;
+  const sk_status st = ctx->finishFrame(true);
+  if (st != SK_OK) return st;
+  ctx->binningMode = mode;
   return SK_OK;
 }
 

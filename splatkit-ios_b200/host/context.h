@@ -82,6 +82,7 @@ struct FrameScratch {
   DeviceBuffer keys, projected, spans, order, sortWorkspace, visStatus, binSums;
   DeviceBuffer instKeys, instValues, instKeysSorted, instValuesSorted, tileSortWorkspace;
   DeviceBuffer ranges, rangeBuffer, rangeStarts, counters;
+  DeviceBuffer cellLists;  // direct cell-major lists: block x cell counts and starts
   DeviceBuffer lodIndices, lodFrontier[2], lodCosts, lodOffsets, lodPackets, lodState, lodStatus,
       lodCounters;
   uint32_t lodFrontierCapacity = 0;
@@ -117,6 +118,7 @@ struct Context {
   uint32_t width = 0, height = 0;
   int imageFormat = SK_FORMAT_RGBA8;
   uint32_t timeStages = 1;  // 0 none, 1 per stage, 2 frame only
+  uint32_t binningMode = SK_BINNING_AUTO;
   sk_policy policy{};
   uint32_t lodLimit = 0;
   host::LodThreshold threshold;

@@ -200,6 +200,7 @@ _SIGNATURES = {
     "sk_wait_idle": (ctypes.c_int32, [ctypes.c_void_p]),
     "sk_get_stats": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Stats)]),
     "sk_set_timing": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    "sk_set_binning": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     "sk_read_visible": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_void_p, ctypes.c_uint32,
                                          _u32p]),
     "sk_read_order": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_uint32, _u32p]),
@@ -474,6 +475,12 @@ class Renderer:
     def apply_render_policy(self, policy: Policy):
         p = policy.native()
         self._check(self._lib.sk_apply_render_policy(self._h, ctypes.byref(p)), "policy")
+
+    def set_binning(self, mode: str):
+        """"auto": cell lists written in place on targets of up to 4096 cells, else sorted;
+        "sorted": always the stable (cell, splat) sort. Both give the same lists."""
+        code = {"auto": 0, "sorted": 1}[mode]
+        self._check(self._lib.sk_set_binning(self._h, code), "binning")
 
     def set_timing(self, time_stages: bool | str):
         """True: per-stage events; "frame": the frame's own pair only; False: none."""
