@@ -45,8 +45,9 @@ typedef struct {
   int32_t device;                /* CUDA device ordinal */
   uint32_t width, height;        /* draw extent of the headless target */
   int32_t image_format;          /* SK_FORMAT_RGBA8 or SK_FORMAT_RGBA32F on the device */
-  uint32_t time_stages;          /* 1: per-stage CUDA events (stats.*_ms); 2: frame events only
-                                    (stats.gpu_ms; keeps the stage kernels chained); 0: none */
+  uint32_t time_stages;          /* 1: per-stage CUDA events (stats.*_ms) and fragment counts;
+                                    2: frame events only (stats.gpu_ms; keeps the stage kernels
+                                    chained); 0: none */
 } sk_config;
 
 /* A SplatCloud (packages/splat-core/include/splat/formats/SplatCloud.h:30-51), structure of
@@ -162,7 +163,7 @@ typedef struct {
   uint32_t lod_evaluated;
   uint32_t instances;      /* tile instances */
   uint32_t device_error;   /* SK_DEVERR bits of the last frame */
-  uint64_t fragments;      /* blended pixel x splat pairs */
+  uint64_t fragments;      /* blended pixel x splat pairs (counted when time_stages is 1) */
   float lod_pixels;        /* the adapted LOD threshold in use */
   uint32_t instances_read; /* tile-list records the composite read before termination */
 } sk_stats;

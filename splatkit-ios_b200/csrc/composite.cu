@@ -35,7 +35,7 @@ constexpr uint32_t kQuadrant = kTileSize / 2;  // each warp owns an 8x8 quadrant
 struct alignas(16) Splat2D {
   float cx, cy, m00, m01;
   float m10, m11, radius, lcut;
-  float alpha, r, g, b;
+  float lpeak, r, g, b;  // lpeak = log2 of the peak alpha
 };
 static_assert(sizeof(Splat2D) == 48, "Splat2D is three 16-byte words");
 
@@ -59,8 +59,9 @@ __device__ __forceinline__ uint32_t coverageForm(const uint4 lo, const uint4 hi,
   s.m01 = -__fmul_rn(a2x, inv);
   s.m10 = -__fmul_rn(a1y, inv);
   s.m11 = __fmul_rn(a1x, inv);
-  s.alpha = highHalf(hi.y);
-  s.lcut = lnF32(__fmul_rn(255.0f, s.alpha));
+  const float peak = highHalf(hi.y);
+  s.lcut = lnF32(__fmul_rn(255.0f, peak));
+  s.lpeak = __log2f(peak);
   s.radius = asF(hi.z);
   s.r = lowHalf(hi.x);
   s.g = highHalf(hi.x);
@@ -96,18 +97,28 @@ __device__ __forceinline__ uint32_t coverageForm(const uint4 lo, const uint4 hi,
 
 // A thread's two pixels, packed so that Blackwell's paired FP32 instructions (FADD2, FMUL2,
 // FFMA2: two independent IEEE operations, each rounded like its scalar form) work on both at once.
+// A pixel is finished once its transmittance T is below the cutoff (T never grows); a pixel
+// outside the target starts at T = -1.
 struct PixelPair {
   float2 T = make_float2(1.0f, 1.0f), r = make_float2(0.0f, 0.0f), g = make_float2(0.0f, 0.0f),
          b = make_float2(0.0f, 0.0f);
-  bool done0, done1;
 };
 
 __device__ __forceinline__ float2 pair(float v) { return make_float2(v, v); }
 
+// 2^x by the hardware approximation (relative error about 2^-22).
+__device__ __forceinline__ float exp2Approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Both pixels against one splat. px = the two pixel centres' x; m01dy, m11dy = m01 dy and
 // m11 dy, shared by the row. The coverage terms u, v, q are the oracle's FP32 sequence per pixel
 // (px - cx is px + (-cx) exactly); an uncovered or finished pixel takes alpha 0, which leaves
-// its colour and transmittance bit for bit as they were.
+// its colour and transmittance bit for bit as they were. alpha = min(1, 2^(log2 peak - q log2 e))
+// and T -= T alpha.
+template <bool kCount>
 __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const float4 w1,
                                           const float4 c, float2 px, float m01dy, float m11dy,
                                           float cutoff, uint32_t& blended) {
@@ -115,20 +126,19 @@ __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const f
   const float2 u = __ffma2_rn(pair(w0.z), dx, pair(m01dy));
   const float2 v = __ffma2_rn(pair(w1.x), dx, pair(m11dy));
   const float2 q = __fmul2_rn(pair(0.5f), __ffma2_rn(u, u, __fmul2_rn(v, v)));
-  const bool c0 = !p.done0 && fabsf(u.x) <= w1.z && fabsf(v.x) <= w1.z && q.x <= w1.w;
-  const bool c1 = !p.done1 && fabsf(u.y) <= w1.z && fabsf(v.y) <= w1.z && q.y <= w1.w;
+  const bool c0 = p.T.x >= cutoff && fabsf(u.x) <= w1.z && fabsf(v.x) <= w1.z && q.x <= w1.w;
+  const bool c1 = p.T.y >= cutoff && fabsf(u.y) <= w1.z && fabsf(v.y) <= w1.z && q.y <= w1.w;
   if (!__any_sync(0xffffffffu, c0 || c1)) return;  // the whole quadrant misses this splat
-  const float a0 = c0 ? fminf(c.x * __expf(-q.x), 1.0f) : 0.0f;
-  const float a1 = c1 ? fminf(c.x * __expf(-q.y), 1.0f) : 0.0f;
+  const float2 e = __ffma2_rn(q, pair(-1.4426950408889634f), pair(c.x));
+  const float a0 = c0 ? fminf(exp2Approx(e.x), 1.0f) : 0.0f;
+  const float a1 = c1 ? fminf(exp2Approx(e.y), 1.0f) : 0.0f;
   const float2 alpha = make_float2(a0, a1);
   const float2 weight = __fmul2_rn(p.T, alpha);
   p.r = __ffma2_rn(weight, pair(c.y), p.r);
   p.g = __ffma2_rn(weight, pair(c.z), p.g);
   p.b = __ffma2_rn(weight, pair(c.w), p.b);
-  p.T = __fmul2_rn(p.T, __fadd2_rn(pair(1.0f), make_float2(-a0, -a1)));
-  blended += static_cast<uint32_t>(c0) + static_cast<uint32_t>(c1);
-  p.done0 = p.done0 || p.T.x < cutoff;
-  p.done1 = p.done1 || p.T.y < cutoff;
+  p.T = __ffma2_rn(pair(-1.0f), weight, p.T);
+  if constexpr (kCount) blended += static_cast<uint32_t>(c0) + static_cast<uint32_t>(c1);
 }
 
 // The target one tile block draws into: the context's image, or its view's part of a batch image.
@@ -165,7 +175,8 @@ __device__ __forceinline__ void writePixel(const CompositeArgs& a, const Target&
 }
 
 // kBatch: block b is batch-wide tile b; its view is the last one whose first tile is <= b.
-template <int kFormat, bool kBatch>
+// kCount: count blended fragments (a statistic; without it the loop saves an add per splat).
+template <int kFormat, bool kBatch, bool kCount>
 __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constant__ CompositeArgs a) {
   chainedKernelStart();
   __shared__ CompositeSmem sm;
@@ -204,8 +215,10 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   const uint32_t below = lanemaskLt();
   const float2 px = make_float2(px0, px1);
   PixelPair p;
-  p.done0 = !(col < t.width && row < t.height);
-  p.done1 = !(col + 1 < t.width && row < t.height);
+  if (!(col < t.width && row < t.height)) p.T.x = -1.0f;
+  if (!(col + 1 < t.width && row < t.height)) p.T.y = -1.0f;
+  const float cutoff = a.cutoff;
+  auto finished = [&] { return p.T.x < cutoff && p.T.y < cutoff; };
   uint32_t blended = 0, loaded = 0;
   for (uint32_t start = range.x; start < range.y; start += kEntries) {
     const uint32_t inBatch = min(kEntries, range.y - start);
@@ -222,7 +235,7 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
       }
     }
     __syncthreads();
-    if (!__all_sync(0xffffffffu, p.done0 && p.done1)) {
+    if (!__all_sync(0xffffffffu, finished())) {
       // this warp's entries, in batch (= depth) order
       uint32_t count = 0;
       for (uint32_t c = 0; c < inBatch; c += 32) {
@@ -234,8 +247,9 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
       }
       __syncwarp();
       for (uint32_t k0 = 0; k0 < count; k0 += 16) {
-        if (__all_sync(0xffffffffu, p.done0 && p.done1)) break;
+        if (__all_sync(0xffffffffu, finished())) break;
         const uint32_t k1 = min(count, k0 + 16);
+#pragma unroll 2
         for (uint32_t k = k0; k < k1; ++k) {
           const Splat2D& s = sm.splat[sm.list[warp][k]];
           const float4 w0 = reinterpret_cast<const float4*>(&s)[0];
@@ -243,11 +257,11 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
           const float4 c = reinterpret_cast<const float4*>(&s)[2];
           const float dy = __fsub_rn(py, w0.y);
           const float m01dy = __fmul_rn(w0.w, dy), m11dy = __fmul_rn(w1.y, dy);
-          blendPair(p, w0, w1, c, px, m01dy, m11dy, a.cutoff, blended);
+          blendPair<kCount>(p, w0, w1, c, px, m01dy, m11dy, cutoff, blended);
         }
       }
     }
-    if (__syncthreads_count((p.done0 && p.done1) ? 0 : 1) == 0) break;
+    if (__syncthreads_count(finished() ? 0 : 1) == 0) break;
   }
   // blended fragments: one 64-bit add per block
   __shared__ unsigned long long blockFragments;
@@ -257,7 +271,7 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
   for (int o = 16; o > 0; o >>= 1) warpSum += __shfl_xor_sync(0xffffffffu, warpSum, o);
   if (lane == 0 && warpSum) atomicAdd(&blockFragments, static_cast<unsigned long long>(warpSum));
   __syncthreads();
-  if (threadIdx.x == 0 && blockFragments)
+  if (kCount && threadIdx.x == 0 && blockFragments)
     atomicAdd(reinterpret_cast<unsigned long long*>(a.fragments), blockFragments);
   if (threadIdx.x == 0 && loaded) atomicAdd(a.loaded, loaded);
   writePixel<kFormat>(a, t, p.T.x, p.r.x, p.g.x, p.b.x, col, row);
@@ -269,12 +283,16 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
 cudaError_t launchComposite(const CompositeArgs& a, cudaStream_t stream) {
   const uint32_t tiles = a.viewCount > 0 ? a.batchTiles : a.tilesX * a.tilesY;
   if (tiles == 0) return cudaSuccess;
-  const bool f32 = a.format == kRgba32f;
-  if (a.viewCount > 0)
-    return launchChained(f32 ? compositeKernel<kRgba32f, true> : compositeKernel<kRgba8, true>, tiles,
-                         kThreads, stream, a);
-  return launchChained(f32 ? compositeKernel<kRgba32f, false> : compositeKernel<kRgba8, false>, tiles,
-                       kThreads, stream, a);
+  const bool f32 = a.format == kRgba32f, count = a.countFragments != 0;
+  void (*kernel)(CompositeArgs);
+  if (a.viewCount > 0) {
+    kernel = f32 ? (count ? compositeKernel<kRgba32f, true, true> : compositeKernel<kRgba32f, true, false>)
+                 : (count ? compositeKernel<kRgba8, true, true> : compositeKernel<kRgba8, true, false>);
+  } else {
+    kernel = f32 ? (count ? compositeKernel<kRgba32f, false, true> : compositeKernel<kRgba32f, false, false>)
+                 : (count ? compositeKernel<kRgba8, false, true> : compositeKernel<kRgba8, false, false>);
+  }
+  return launchChained(kernel, tiles, kThreads, stream, a);
 }
 
 }  // namespace sk

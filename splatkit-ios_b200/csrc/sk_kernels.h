@@ -161,7 +161,8 @@ struct CompositeArgs {
   float cutoff;  // transmittance below which a pixel stops
   void* image;   // row 0 on top
   int format;
-  uint32_t* fragments;  // FrameCounters.fragments_lo/hi (64-bit add)
+  uint32_t* fragments;  // FrameCounters.fragments_lo/hi (64-bit add), when countFragments
+  uint32_t countFragments;
   uint32_t* loaded;     // FrameCounters.loaded
   // a batch (viewCount > 0): one block per batch-wide tile, image = the batch image
   const BatchView* views;

@@ -291,6 +291,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     c.image = l.image.ptr;
     c.format = kRgba8;
     c.fragments = &fc->fragments_lo;
+    c.countFragments = 1;
     c.loaded = &fc->loaded;
     c.views = views;
     c.viewCount = l.viewCount;

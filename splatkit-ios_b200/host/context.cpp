@@ -397,6 +397,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     c.image = view.image;
     c.format = imageFormat == SK_FORMAT_RGBA32F ? kRgba32f : kRgba8;
     c.fragments = &fc->fragments_lo;
+    c.countFragments = timing == 1 ? 1u : 0u;
     c.loaded = &fc->loaded;
     e = launchComposite(c, s);
   }
