@@ -43,7 +43,7 @@ L2_FLUSH_BYTES = 256 << 20
 def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=60)
+    p.add_argument("--steps", type=int, default=400)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--bits", type=int, default=16, choices=(16, 32))
     p.add_argument("--impl", default="ours", choices=("ours", "reference"))
@@ -86,7 +86,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -134,7 +134,8 @@ class ClockSampler:
 # ---- algorithmic bytes per stage ---------------------------------------------------------------
 def stage_bytes(stats, bits, n=SPLATS, width=WIDTH, height=HEIGHT, sh_words=24):
     v, inst, read = stats["draw_count"], stats["instances"], stats["instances_read"]
-    tiles = ((width + 15) // 16) * ((height + 15) // 16)
+    cells = ((width + 31) // 32) * ((height + 31) // 32)
+    blocks = (v + 1023) // 1024
     return {
         # 32 B record per source splat, the SH record (96 B at SH3, device stride) of each
         # survivor, then a 4 B key, a 32 B projected record and a 16 B tile span per survivor
@@ -142,10 +143,10 @@ def stage_bytes(stats, bits, n=SPLATS, width=WIDTH, height=HEIGHT, sh_words=24):
         # one all-digit histogram read + per pass read key(+value) and write key+value; the
         # last pass skips the key write: 60 B/key at 32 bits, 28 B/key at 16 bits
         "sort": (60 if bits == 32 else 28) * v,
-        # count and emit each read order + span (20 B per survivor), emit writes (tile, value);
-        # the 16-bit tile sort reads the keys once for its histogram and moves 16 B per
-        # instance per pass (sorted keys written too); ranges read the keys, write 8 B per tile
-        "bin": 40 * v + 8 * inst + 4 * inst + 32 * inst + 4 * inst + 8 * tiles,
+        # direct cell lists: count and emit each read order + span (20 B per survivor); the
+        # per-block cell counts are written, read and turned into block starts (read again by
+        # the emission): 3 x 4 B per (block, cell); 8 B range per cell; 4 B written per entry
+        "bin": 40 * v + 12 * blocks * cells + 8 * cells + 4 * inst,
         # index + projected record per list entry read, RGBA8 image write
         "composite": 36 * read + width * height * 4,
     }
@@ -341,14 +342,14 @@ def run_ours(args):
         dominant = max(("cull", "sort", "bin", "composite"), key=lambda k: mean[k + "_ms"])
         peak, peak_kind = measured_peaks()
         achieved = bytes_by_stage[dominant] / (mean[dominant + "_ms"] / 1000.0) / 1e9
-        kernel_tag = {"cull": "visibility", "sort": "radix_sort", "bin": "binning",
+        kernel_tag = {"cull": "visibility", "sort": "radix_sort", "bin": "cell_lists",
                       "composite": "composite"}[dominant]
         profile = {"cull": "visibility_1m_sh3_1080p", "sort": "radix_sort_scatter_depth_1m_sh3_1080p",
-                   "bin": "binning_emit_1m_sh3_1080p", "composite": "composite_1m_sh3_1080p"}[dominant]
+                   "bin": "cell_lists_emit_1m_sh3_1080p", "composite": "composite_1m_sh3_1080p"}[dominant]
         traffic = traffic_from_profiles(profile) if args.bits == 16 else None
         passes = 2 if args.bits == 16 else 4
-        # visibility, depth sort (histogram + passes), bin count + emit, tile sort, ranges, composite
-        launches_per_frame = 1 + (1 + passes) + 2 + 3 + 1 + 1
+        # visibility, depth sort (histogram + passes), cell lists (count, scan, emit), composite
+        launches_per_frame = 1 + (1 + passes) + 3 + 1
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -360,7 +361,7 @@ def run_ours(args):
                          "algorithmic_bytes": bytes_by_stage[dominant],
                          "profile": f"profiles/{profile}.md"},
             "stages_ms": mean,
-            "stage_timing": "a second pass over the same frames with events around each stage",
+            "stage_timing": "a second pass over the same frames with events around each stage and fragment counting",
             "stage_gbs": {k: bytes_by_stage[k] / (mean[k + "_ms"] / 1000.0) / 1e9
                           for k in bytes_by_stage},
             "visible": last["draw_count"], "instances": last["instances"],
