@@ -246,6 +246,16 @@ sk_status sk_draw(sk_context* ctx, const sk_frame* frame);
 /* Waits for the last frame and copies its image (captureNextFrame). */
 sk_status sk_read_image(sk_context* ctx, void* host, size_t bytes, int32_t format);
 sk_status sk_wait_idle(sk_context* ctx);
+/* captureNextFrame (MetalSplatRenderer.mm:310-316): the next sk_draw also copies its image, in the
+ * context's own pixel format, into `host` (at least width x height x 4 or 16 bytes) on a copy
+ * stream of its own, so the copy overlaps the frames drawn after it; sk_wait_capture blocks until
+ * the image is there (a frame that is drawn again because its lists overflowed is copied
+ * again). From the first capture on, frames alternate between two device images. The host
+ * buffer must be pinned (sk_server_alloc_host, cudaHostAlloc) for the copy to overlap, and must
+ * stay untouched until the wait returns. One capture may wait for the next frame at a time. */
+sk_status sk_capture_next_frame(sk_context* ctx, void* host, size_t bytes, int32_t format,
+                                uint64_t* ticket);
+sk_status sk_wait_capture(sk_context* ctx, uint64_t ticket);
 sk_status sk_get_stats(sk_context* ctx, sk_stats* out);
 /* Switches the event timing of later frames (sk_config.time_stages' values); waits for the
  * frame in flight first. */

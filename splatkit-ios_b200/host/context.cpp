@@ -71,6 +71,12 @@ void PinnedBuffer::release() {
 // ---- context ------------------------------------------------------------------------------
 
 Context::~Context() {
+  if (copyStream) cudaStreamSynchronize(copyStream);
+  for (auto& c : captures)
+    if (c.copied) cudaEventDestroy(c.copied);
+  for (auto& e : imageFree)
+    if (e) cudaEventDestroy(e);
+  if (copyStream) cudaStreamDestroy(copyStream);
   if (done) cudaEventDestroy(done);
   if (stream) cudaStreamDestroy(stream);
 }
@@ -170,7 +176,9 @@ sk_status Context::reserveLod(FrameScratch& f, const World& w, cudaStream_t s) {
 
 sk_status Context::reserveView(uint32_t w, uint32_t h) {
   const size_t pixelBytes = imageFormat == SK_FORMAT_RGBA32F ? 16 : 4;
+  if (copyStream) cudaStreamSynchronize(copyStream);  // no capture copy reads an image freed here
   cudaError_t e = image.allocate(size_t{w} * h * pixelBytes);
+  if (e == cudaSuccess && twoImages) e = image2.allocate(size_t{w} * h * pixelBytes);
   if (e == cudaSuccess) e = frameCounters.allocate(sizeof(FrameCounters));
   if (e == cudaSuccess) e = camera.allocate(sizeof(Camera));
   if (e == cudaSuccess) e = hostCounters.allocate(sizeof(FrameCounters));
@@ -411,7 +419,7 @@ ViewTarget Context::plainView() {
   ViewTarget v;
   v.width = width;
   v.height = height;
-  v.image = image.ptr;
+  v.image = imageOf(imageSlot);
   v.counters = static_cast<FrameCounters*>(frameCounters.ptr);
   v.hostCounters = static_cast<FrameCounters*>(hostCounters.ptr);
   v.camera = static_cast<const Camera*>(camera.ptr);
@@ -424,9 +432,39 @@ sk_status Context::enqueuePlainFrame(const sk_frame& frame, uint32_t total) {
   cudaError_t e = cudaMemcpyAsync(camera.ptr, hostCamera.ptr, sizeof(Camera),
                                   cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return check(e, "camera upload");
+  // the image this frame draws into may still be on its way to a capture's host buffer
+  if (imageCopied[imageSlot]) {
+    e = cudaStreamWaitEvent(stream, imageFree[imageSlot], 0);
+    if (e != cudaSuccess) return check(e, "capture wait");
+  }
   sk_status st = enqueuePipeline(scratch, plainView(), frame, total, stream, timeStages);
   if (st != SK_OK) return st;
-  return check(cudaEventRecord(done, stream), "frame");
+  st = check(cudaEventRecord(done, stream), "frame");
+  if (st != SK_OK) return st;
+  // captures of this frame copy its image once it is drawn (again after a redraw)
+  for (auto& c : captures)
+    if (c.frame == submitted && (st = issueCapture(c)) != SK_OK) return st;
+  return SK_OK;
+}
+
+size_t Context::imageBytes() const {
+  return size_t{width} * height * (imageFormat == SK_FORMAT_RGBA32F ? 16 : 4);
+}
+
+sk_status Context::issueCapture(Capture& c) {
+  if (c.bytes < imageBytes()) {
+    c.tooSmall = true;
+    return SK_OK;
+  }
+  cudaError_t e = cudaStreamWaitEvent(copyStream, done, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c.host, imageOf(imageSlot), imageBytes(), cudaMemcpyDeviceToHost, copyStream);
+  if (e == cudaSuccess) e = cudaEventRecord(c.copied, copyStream);
+  if (e == cudaSuccess) e = cudaEventRecord(imageFree[imageSlot], copyStream);
+  if (e != cudaSuccess) return check(e, "capture copy");
+  imageCopied[imageSlot] = true;
+  c.issued = true;
+  return SK_OK;
 }
 
 // Reads the last frame's counters once it completed; grows the instance buffers and draws
@@ -776,14 +814,20 @@ sk_status sk_draw(sk_context* handle, const sk_frame* frame) {
   sk_status st = ctx->finishFrame(true);
   if (st == SK_E_DEVICE) return st;
   if (!ctx->world.splats.ptr) total = 0;
+  if (ctx->twoImages) ctx->imageSlot ^= 1u;
   ctx->lastFrame = *frame;
   ctx->lastTotal = total;
   ctx->lastRanges.assign(frame->ranges, frame->ranges + (frame->ranges ? frame->range_count : 0));
   ctx->lastFrame.ranges = ctx->lastRanges.data();
+  ++ctx->submitted;  // this frame's number, which pending captures are bound to
+  for (auto& c : ctx->captures)
+    if (c.frame == 0) c.frame = ctx->submitted;
   st = ctx->enqueuePlainFrame(ctx->lastFrame, total);
-  if (st != SK_OK) return st;
+  if (st != SK_OK) {
+    --ctx->submitted;
+    return st;
+  }
   ctx->frameInFlight = true;
-  ++ctx->submitted;
   return SK_OK;
 }
 
@@ -806,10 +850,12 @@ sk_status sk_read_image(sk_context* handle, void* host, size_t bytes, int32_t fo
   if (format == SK_FORMAT_RGBA32F && !deviceFloat)
     return ctx->fail(SK_E_INVALID, "the context renders 8-bit images");
   if ((format == SK_FORMAT_RGBA8 && !deviceFloat) || (format == SK_FORMAT_RGBA32F && deviceFloat))
-    return ctx->check(cudaMemcpy(host, ctx->image.ptr, need, cudaMemcpyDeviceToHost), "readback");
+    return ctx->check(cudaMemcpy(host, ctx->imageOf(ctx->imageSlot), need, cudaMemcpyDeviceToHost),
+                      "readback");
   // Conversions on the host.
   std::vector<uint8_t> staging(pixels * (deviceFloat ? 16 : 4));
-  cudaError_t e = cudaMemcpy(staging.data(), ctx->image.ptr, staging.size(), cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpy(staging.data(), ctx->imageOf(ctx->imageSlot), staging.size(),
+                             cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return ctx->check(e, "readback");
   uint8_t* out = static_cast<uint8_t*>(host);
   for (size_t i = 0; i < pixels; ++i) {
@@ -825,6 +871,61 @@ sk_status sk_read_image(sk_context* handle, void* host, size_t bytes, int32_t fo
     std::memcpy(out + i * 4, rgba, 4);
   }
   return SK_OK;
+}
+
+sk_status sk_capture_next_frame(sk_context* handle, void* host, size_t bytes, int32_t format,
+                                uint64_t* ticket) {
+  SK_CTX(handle);
+  if (!host || !ticket) return SK_E_INVALID;
+  const int32_t native = ctx->imageFormat == SK_FORMAT_RGBA32F ? SK_FORMAT_RGBA32F : SK_FORMAT_RGBA8;
+  if (format != native) return ctx->fail(SK_E_INVALID, "a capture copies the context's own pixel format");
+  if (bytes < ctx->imageBytes()) return ctx->fail(SK_E_INVALID, "capture buffer too small");
+  for (const auto& c : ctx->captures)
+    if (c.frame == 0) return ctx->fail(SK_E_INVALID, "a capture is already waiting for the next frame");
+  if (!ctx->copyStream) {
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->copyStream, cudaStreamNonBlocking);
+    for (auto& ev : ctx->imageFree)
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return ctx->check(e, "capture set-up");
+  }
+  if (!ctx->twoImages) {
+    const sk_status st = ctx->finishFrame(true);
+    if (st != SK_OK) return st;
+    ctx->twoImages = true;
+    const sk_status vs = ctx->reserveView(ctx->width, ctx->height);
+    if (vs != SK_OK) {
+      ctx->twoImages = false;
+      return vs;
+    }
+  }
+  Context::Capture c;
+  c.ticket = ctx->nextCapture++;
+  c.host = host;
+  c.bytes = bytes;
+  const cudaError_t e = cudaEventCreateWithFlags(&c.copied, cudaEventDisableTiming);
+  if (e != cudaSuccess) return ctx->check(e, "capture event");
+  ctx->captures.push_back(c);
+  *ticket = c.ticket;
+  return SK_OK;
+}
+
+sk_status sk_wait_capture(sk_context* handle, uint64_t ticket) {
+  SK_CTX(handle);
+  auto it = std::find_if(ctx->captures.begin(), ctx->captures.end(),
+                         [&](const Context::Capture& c) { return c.ticket == ticket; });
+  if (it == ctx->captures.end() || it->frame == 0)
+    return ctx->fail(SK_E_INVALID, "no such capture, or its frame is not drawn yet");
+  sk_status st = SK_OK;
+  if (ctx->frameInFlight && it->frame == ctx->submitted) st = ctx->finishFrame(true);  // may redraw
+  it = std::find_if(ctx->captures.begin(), ctx->captures.end(),
+                    [&](const Context::Capture& c) { return c.ticket == ticket; });
+  const cudaError_t e = cudaEventSynchronize(it->copied);
+  const bool tooSmall = it->tooSmall;
+  cudaEventDestroy(it->copied);
+  ctx->captures.erase(it);
+  if (e != cudaSuccess) return ctx->check(e, "capture wait");
+  if (tooSmall) return ctx->fail(SK_E_INVALID, "the target was resized past the capture buffer");
+  return st;
 }
 
 sk_status sk_set_binning(sk_context* handle, uint32_t mode) {

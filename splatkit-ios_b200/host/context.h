@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <deque>
 #include <string>
 #include <thread>
 #include <vector>
@@ -132,6 +133,27 @@ struct Context {
   PinnedBuffer hostCounters, hostCamera;
   cudaEvent_t done = nullptr;
   bool frameInFlight = false;
+  // Frame captures (captureNextFrame): once one is requested the frames alternate between two
+  // images, so the copy of one frame's image to the host (on copyStream) overlaps the drawing of
+  // the next; a frame waits for the copy that still reads its image before it draws.
+  struct Capture {
+    uint64_t ticket = 0, frame = 0;  // the frame: the submitted-frame count it was drawn as
+    void* host = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t copied = nullptr;
+    bool issued = false, tooSmall = false;  // tooSmall: the target grew past the buffer
+  };
+  DeviceBuffer image2;
+  bool twoImages = false;
+  uint32_t imageSlot = 0;  // image of the frame in flight or last drawn
+  cudaStream_t copyStream = nullptr;
+  cudaEvent_t imageFree[2] = {};
+  bool imageCopied[2] = {};
+  std::deque<Capture> captures;  // requested, in flight or landed but not waited for
+  uint64_t nextCapture = 1;
+  void* imageOf(uint32_t slot) { return slot ? image2.ptr : image.ptr; }
+  size_t imageBytes() const;
+  sk_status issueCapture(Capture& c);
   sk_frame lastFrame{};
   std::vector<sk_range> lastRanges;
   uint32_t lastTotal = 0;

@@ -201,6 +201,9 @@ _SIGNATURES = {
     "sk_get_stats": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_Stats)]),
     "sk_set_timing": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     "sk_set_binning": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    "sk_capture_next_frame": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                               ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
+    "sk_wait_capture": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64]),
     "sk_read_visible": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_void_p, ctypes.c_uint32,
                                          _u32p]),
     "sk_read_order": (ctypes.c_int32, [ctypes.c_void_p, _u32p, ctypes.c_uint32, _u32p]),
@@ -438,6 +441,7 @@ class Renderer:
             raise SplatError(st, "sk_create failed (is a CUDA device visible?)")
         self._h = handle
         self.width, self.height, self.image_format = width, height, image_format
+        self._captures = {}
 
     # lifetime
     def close(self):
@@ -557,6 +561,25 @@ class Renderer:
 
     def wait_idle(self):
         self._check(self._lib.sk_wait_idle(self._h), "wait")
+
+    def capture_next_frame(self, out: np.ndarray) -> int:
+        """captureNextFrame: the next draw's image is copied into `out` (the context's pixel
+        format; pinned memory lets the copy overlap later frames). Returns a ticket for
+        wait_capture; `out` must stay alive and untouched until then."""
+        fmt = self.image_format
+        need = self.width * self.height * (16 if fmt == FORMAT_RGBA32F else 4)
+        if not out.flags["C_CONTIGUOUS"] or out.nbytes < need:
+            raise SplatError(SK_E_INVALID, "capture buffer too small or not contiguous")
+        t = ctypes.c_uint64()
+        self._check(self._lib.sk_capture_next_frame(self._h, out.ctypes.data, out.nbytes, fmt,
+                                                    ctypes.byref(t)), "capture")
+        self._captures[t.value] = out
+        return t.value
+
+    def wait_capture(self, ticket: int) -> np.ndarray:
+        """Blocks until the captured frame's image is in its buffer; returns the buffer."""
+        self._check(self._lib.sk_wait_capture(self._h, ticket), "capture wait")
+        return self._captures.pop(ticket, None)
 
     def read_image(self, fmt: int = None, out: Optional[np.ndarray] = None) -> np.ndarray:
         fmt = self.image_format if fmt is None else fmt

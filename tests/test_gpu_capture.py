@@ -1,0 +1,120 @@
+"""captureNextFrame (sk_capture_next_frame / sk_wait_capture): captures taken one frame behind the
+draws, copied while the next frame renders, hold exactly the images sk_read_image gives for the
+same frames; a frame redrawn after an overflow of its lists is captured as redrawn; misuse is
+rejected."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import splatkit_b200 as sk
+from splatkit_b200 import camera as skcam
+from splatkit_b200 import synthetic
+
+
+def frames_for(cloud, w, h, steps):
+    out = []
+    for step in steps:
+        view, eye = skcam.orbit_view(step, radius=15.0)
+        proj = skcam.perspective(math.radians(60.0), w / h, 0.05, 200.0)
+        out.append(sk.Frame(view, proj, eye, [(0, cloud.count)], cloud.sh_degree))
+    return out
+
+
+def read_back(cloud, frames, w, h, fmt):
+    r = sk.Renderer(w, h, image_format=fmt)
+    r.upload_world(cloud, cloud.sh_degree)
+    out = []
+    for f in frames:
+        r.draw(f)
+        out.append(r.read_image(fmt).copy())
+    r.close()
+    return out
+
+
+def pinned_image(w, h, fmt):
+    if fmt == sk.FORMAT_RGBA32F:
+        return torch.empty((h, w, 4), dtype=torch.float32, pin_memory=True).numpy()
+    return torch.empty((h, w, 4), dtype=torch.uint8, pin_memory=True).numpy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmt", [sk.FORMAT_RGBA8, sk.FORMAT_RGBA32F])
+def test_captures_one_frame_behind_equal_read_image(cuda_device, fmt):
+    w, h = 640, 480
+    cloud = synthetic.random_cloud(200_000, seed=41, sh_degree=1)
+    frames = frames_for(cloud, w, h, range(0, 60, 7))
+    r = sk.Renderer(w, h, image_format=fmt)
+    r.upload_world(cloud, 1)
+    buffers = [pinned_image(w, h, fmt) for _ in range(2)]
+    captured, previous = [], None
+    for k, f in enumerate(frames):
+        ticket = r.capture_next_frame(buffers[k % 2])
+        r.draw(f)
+        if previous is not None:
+            captured.append(r.wait_capture(previous).copy())
+        previous = ticket
+    captured.append(r.wait_capture(previous).copy())
+    # a plain readback on the same renderer after captures: the last drawn frame
+    r.draw(frames[2])
+    last = r.read_image(fmt).copy()
+    r.close()
+    expected = read_back(cloud, frames, w, h, fmt)
+    for got, want in zip(captured, expected):
+        assert np.array_equal(got, want)
+    assert np.array_equal(last, expected[2])
+
+
+@pytest.mark.gpu
+def test_capture_of_a_redrawn_frame(cuda_device):
+    # boxes of many cells: the first draw overflows the first list reservation and is redrawn
+    w, h = 640, 480
+    cloud = synthetic.random_cloud(6_000, seed=31, sh_degree=1, log_scale_mean=1.0)
+    frames = frames_for(cloud, w, h, (3, 40))
+    r = sk.Renderer(w, h, image_format=sk.FORMAT_RGBA8)
+    r.upload_world(cloud, 1)
+    buf = pinned_image(w, h, sk.FORMAT_RGBA8)
+    got = []
+    for f in frames:
+        t = r.capture_next_frame(buf)
+        r.draw(f)
+        got.append(r.wait_capture(t).copy())
+    assert r.stats()["instances"] > 8 * cloud.count
+    r.close()
+    for g, want in zip(got, read_back(cloud, frames, w, h, sk.FORMAT_RGBA8)):
+        assert np.array_equal(g, want)
+
+
+@pytest.mark.gpu
+def test_capture_misuse_is_rejected(cuda_device):
+    w, h = 320, 240
+    cloud = synthetic.random_cloud(20_000, seed=5, sh_degree=0)
+    (frame,) = frames_for(cloud, w, h, (0,))
+    r = sk.Renderer(w, h, image_format=sk.FORMAT_RGBA8)
+    r.upload_world(cloud, 0)
+    lib = sk.library()
+    import ctypes
+    t = ctypes.c_uint64()
+    small = np.empty((h, w, 2), np.uint8)
+    assert lib.sk_capture_next_frame(r._h, small.ctypes.data, small.nbytes, sk.FORMAT_RGBA8,
+                                     ctypes.byref(t)) == sk.SK_E_INVALID
+    buf = np.empty((h, w, 4), np.uint8)
+    assert lib.sk_capture_next_frame(r._h, buf.ctypes.data, buf.nbytes, sk.FORMAT_RGBA32F,
+                                     ctypes.byref(t)) == sk.SK_E_INVALID
+    ticket = r.capture_next_frame(buf)
+    with pytest.raises(sk.SplatError):  # one capture waits for the next frame at a time
+        r.capture_next_frame(np.empty((h, w, 4), np.uint8))
+    with pytest.raises(sk.SplatError):  # its frame is not drawn yet
+        r.wait_capture(ticket)
+    r.resize(2 * w, 2 * h)  # the target outgrows the buffer before the frame is drawn
+    r.draw(frame)
+    with pytest.raises(sk.SplatError):
+        r.wait_capture(ticket)
+    assert lib.sk_wait_capture(r._h, 12345) == sk.SK_E_INVALID
+    # the renderer keeps working
+    r.draw(frame)
+    assert r.read_image(sk.FORMAT_RGBA8).shape == (2 * h, 2 * w, 4)
+    r.close()
