@@ -33,6 +33,19 @@ constexpr uint32_t kThreads = 256;
 constexpr uint32_t kItems = 4;
 constexpr uint32_t kTileSplats = kThreads * kItems;
 
+// Per block: i / 255 for the 8-bit colour and opacity channels (the same IEEE quotients the
+// division gives, computed once per block instead of four times per splat) and the camera's
+// near distance proj[14] / proj[10].
+__shared__ float blockUnorm8[256];
+__shared__ float blockZNear;
+
+// Fills the block constants; the camera must be in shared memory. Ends with a barrier.
+__device__ __forceinline__ void loadBlockConstants(const Camera& cam) {
+  blockUnorm8[threadIdx.x] = static_cast<float>(threadIdx.x) / 255.0f;
+  if (threadIdx.x == 0) blockZNear = cam.proj[14] / cam.proj[10];
+  __syncthreads();
+}
+
 __device__ __forceinline__ void mulPoint(const float* m, float x, float y, float z, float w,
                                          float* o) {
 #pragma unroll
@@ -115,7 +128,7 @@ __device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, 
   const uint32_t rgba8 = lo.w;
   const uint32_t cov0 = hi.x, cov1 = hi.y, cov2 = hi.z, lodAlpha = hi.w;
   if (!(cam.reveal[0] - py >= 0.0f)) return false;
-  const float ca = static_cast<float>(rgba8 >> 24) / 255.0f;
+  const float ca = blockUnorm8[rgba8 >> 24];
   const float alpha = lodAlpha != 0u ? asF(lodAlpha) : ca;
   if (alpha < kQuadMinAlpha) return false;
 
@@ -125,7 +138,7 @@ __device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, 
   float clip[4];
   mulPoint(cam.proj, v[0], v[1], v[2], v[3], clip);
   if (clip[2] < 0.0f || clip[2] > clip[3]) return false;
-  if (clip[3] <= cam.proj[14] / cam.proj[10]) return false;
+  if (clip[3] <= blockZNear) return false;
 
   // projectCovariance (SplatProjection.metalh:6-24)
   const float vz = v[2];
@@ -202,9 +215,8 @@ __device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, 
   const float depth = -v[2];
   if (!isfinite(depth)) return false;
 
-  float rgb[3] = {static_cast<float>(rgba8 & 0xffu) / 255.0f,
-                  static_cast<float>((rgba8 >> 8) & 0xffu) / 255.0f,
-                  static_cast<float>((rgba8 >> 16) & 0xffu) / 255.0f};
+  float rgb[3] = {blockUnorm8[rgba8 & 0xffu], blockUnorm8[(rgba8 >> 8) & 0xffu],
+                  blockUnorm8[(rgba8 >> 16) & 0xffu]};
   if constexpr (D >= 1) {
     ShWords<D> words;
     words.load(sh, index, shStride);
@@ -219,7 +231,7 @@ __device__ __forceinline__ bool projectSplat(const Camera& cam, const uint4 lo, 
   }
 
   if constexpr (kKey16) {
-    const float zNear = cam.proj[14] / cam.proj[10];
+    const float zNear = blockZNear;
     const uint32_t steps = asU(fmaxf(depth, zNear)) - asU(zNear);
     key = min(steps >> kDepthKeyShift, kDepthKeyMax);
   } else {
@@ -414,6 +426,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   __shared__ Camera cam;
   loadCamera(camera, &cam);
   const uint32_t tile = takeTile(a.counters);  // its barrier also publishes the camera
+  loadBlockConstants(cam);
   const uint32_t total = kIndexed ? min(*a.indexCount, a.total) : a.total;
   const uint32_t tiles = (total + kTileSplats - 1) / kTileSplats;
   if (tile < tiles) {
@@ -469,6 +482,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       reinterpret_cast<uint32_t*>(&view)[threadIdx.x] =
           __ldg(reinterpret_cast<const uint32_t*>(a.views + v) + threadIdx.x);
     __syncthreads();
+    loadBlockConstants(cam);
     const uint32_t chunk = item - view.itemStart;
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
     const uint32_t first = chunk * kTileSplats + warp * (32 * kItems) + lane;
