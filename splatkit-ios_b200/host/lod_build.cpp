@@ -12,9 +12,12 @@
 // has none in its worlds).
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "../../include/splatkit_b200.h"
@@ -68,41 +71,67 @@ std::array<float, 3> semiAxes(const float* cov) {
   return {std::sqrt(std::max(e[0], 0.0f)), std::sqrt(std::max(e[1], 0.0f)), std::sqrt(std::max(e[2], 0.0f))};
 }
 
-struct Nodes {
-  std::vector<float> positions, covariances, colors, alphas, sh, size;
-  std::vector<std::vector<uint32_t>> children;
-  size_t shStride = 0;
-
+// Node attributes, structure of arrays. `area` caches ellipsoidArea(semiAxes(covariance)), the
+// merge weight per unit opacity, so each node's eigenvalues are taken once. Node k's children
+// are kids[kidStart[k] .. kidStart[k] + kidCount[k]).
+struct Store {
+  std::vector<float> positions, covariances, colors, alphas, sh, size, area;
+  std::vector<uint32_t> kidStart, kidCount, kids;
   size_t count() const { return alphas.size(); }
+};
+
+// Where a node id lives: ids below `split` in `low`, the others at id - base in `high` (the
+// nodes this builder adds). A worker reads the shared leaves and writes its own store; the last,
+// sequential pass holds everything in one store.
+struct Nodes {
+  const Store* low;
+  Store* high;
+  uint32_t split, base;
+  size_t shStride;
+
+  const Store& at(uint32_t id, size_t& i) const {
+    if (id < split) {
+      i = id;
+      return *low;
+    }
+    i = id - base;
+    return *high;
+  }
 
   // LodTree.cpp:47-102: one splat matching the members' weighted spatial moments.
   uint32_t merge(const std::vector<uint32_t>& members) {
-    std::vector<float> weights(members.size());
+    const size_t m = members.size();
+    std::vector<float> weights(m);
+    std::vector<std::pair<const Store*, size_t>> ref(m);
     float total = 0.0f;
-    for (size_t k = 0; k < members.size(); ++k) {
-      const uint32_t i = members[k];
-      weights[k] = ellipsoidArea(semiAxes(&covariances[i * 6])) * alphas[i];
+    for (size_t k = 0; k < m; ++k) {
+      size_t i;
+      const Store& st = at(members[k], i);
+      ref[k] = {&st, i};
+      weights[k] = st.area[i] * st.alphas[i];
       total += weights[k];
     }
-    for (float& w : weights) w = total > 1e-30f ? w / total : 1.0f / members.size();
+    for (float& w : weights) w = total > 1e-30f ? w / total : 1.0f / m;
     float center[3] = {0, 0, 0}, rgb[3] = {0, 0, 0};
     std::vector<float> shSum(shStride, 0.0f);
-    for (size_t k = 0; k < members.size(); ++k) {
-      const uint32_t i = members[k];
+    for (size_t k = 0; k < m; ++k) {
+      const Store& st = *ref[k].first;
+      const size_t i = ref[k].second;
       for (int c = 0; c < 3; ++c) {
-        center[c] += weights[k] * positions[i * 3 + c];
-        rgb[c] += weights[k] * colors[i * 3 + c];
+        center[c] += weights[k] * st.positions[i * 3 + c];
+        rgb[c] += weights[k] * st.colors[i * 3 + c];
       }
-      for (size_t c = 0; c < shStride; ++c) shSum[c] += weights[k] * sh[i * shStride + c];
+      for (size_t c = 0; c < shStride; ++c) shSum[c] += weights[k] * st.sh[i * shStride + c];
     }
     for (float& channel : rgb) channel = std::clamp(channel, 0.0f, 1.0f);
     float cov[6] = {0, 0, 0, 0, 0, 0};
-    for (size_t k = 0; k < members.size(); ++k) {
-      const uint32_t i = members[k];
-      const float dx = positions[i * 3] - center[0];
-      const float dy = positions[i * 3 + 1] - center[1];
-      const float dz = positions[i * 3 + 2] - center[2];
-      const float* c = &covariances[i * 6];
+    for (size_t k = 0; k < m; ++k) {
+      const Store& st = *ref[k].first;
+      const size_t i = ref[k].second;
+      const float dx = st.positions[i * 3] - center[0];
+      const float dy = st.positions[i * 3 + 1] - center[1];
+      const float dz = st.positions[i * 3 + 2] - center[2];
+      const float* c = &st.covariances[i * 6];
       const float w = weights[k];
       cov[0] += w * (dx * dx + c[0]);
       cov[1] += w * (dx * dy + c[1]);
@@ -112,16 +141,21 @@ struct Nodes {
       cov[5] += w * (dz * dz + c[5]);
     }
     const auto axes = semiAxes(cov);
-    const float alpha = std::clamp(total / std::max(ellipsoidArea(axes), 1e-30f), 0.0f, 1000.0f);
-    const auto index = static_cast<uint32_t>(count());
-    positions.insert(positions.end(), center, center + 3);
-    covariances.insert(covariances.end(), cov, cov + 6);
-    colors.insert(colors.end(), rgb, rgb + 3);
-    alphas.push_back(alpha);
-    sh.insert(sh.end(), shSum.begin(), shSum.end());
-    size.push_back(2.0f * axes[0] * lodOpacityReach(alpha));
-    children.push_back(members);
-    return index;
+    const float area = ellipsoidArea(axes);
+    const float alpha = std::clamp(total / std::max(area, 1e-30f), 0.0f, 1000.0f);
+    Store& out = *high;
+    const auto id = static_cast<uint32_t>(base + out.count());
+    out.positions.insert(out.positions.end(), center, center + 3);
+    out.covariances.insert(out.covariances.end(), cov, cov + 6);
+    out.colors.insert(out.colors.end(), rgb, rgb + 3);
+    out.alphas.push_back(alpha);
+    out.sh.insert(out.sh.end(), shSum.begin(), shSum.end());
+    out.size.push_back(2.0f * axes[0] * lodOpacityReach(alpha));
+    out.area.push_back(area);
+    out.kidStart.push_back(static_cast<uint32_t>(out.kids.size()));
+    out.kidCount.push_back(static_cast<uint32_t>(m));
+    out.kids.insert(out.kids.end(), members.begin(), members.end());
+    return id;
   }
 };
 
@@ -142,12 +176,22 @@ uint64_t mortonKey(const float* position, const float* boundsMin, float extent, 
   return key;
 }
 
-// LodTree.cpp:162-196
+// A subtree built on its own: the sorted range, the level its build starts at, and its root.
+struct Task {
+  size_t begin, end;
+  uint32_t level;
+  uint32_t root = 0;
+  uint32_t worker = 0;
+};
+
+// LodTree.cpp:162-196. With `tasks` set, a call on a task's range returns the task's root
+// instead of building it (the subtrees were built beforehand, in parallel).
 struct OctreeBuilder {
   Nodes& nodes;
   const std::vector<Cell>& sorted;
   size_t clusterLeaves;
   uint32_t depth;
+  const std::vector<Task>* tasks = nullptr;
 
   uint32_t mergeLeaves(size_t begin, size_t end) {
     std::vector<uint32_t> members;
@@ -165,13 +209,80 @@ struct OctreeBuilder {
     return members;
   }
   uint32_t build(size_t begin, size_t end, uint32_t level) {
+    if (tasks) {
+      auto it = std::lower_bound(tasks->begin(), tasks->end(), begin,
+                                 [](const Task& t, size_t b) { return t.begin < b; });
+      if (it != tasks->end() && it->begin == begin && it->end == end && it->level == level)
+        return it->root;
+    }
     if (end - begin == 1) return sorted[begin].node;
     if (end - begin <= clusterLeaves || level == depth) return mergeLeaves(begin, end);
     const uint32_t shift = 3 * (depth - level - 1);
     if ((sorted[begin].key >> shift) == (sorted[end - 1].key >> shift)) return build(begin, end, level + 1);
     return nodes.merge(buildChildren(begin, end, level, shift));
   }
+
+  // The same descent without merging: every range of at most `limit` leaves the build reaches
+  // becomes a task.
+  void plan(size_t begin, size_t end, uint32_t level, size_t limit, std::vector<Task>& out) const {
+    if (end - begin <= limit || end - begin <= clusterLeaves || level == depth) {
+      out.push_back(Task{begin, end, level});
+      return;
+    }
+    const uint32_t shift = 3 * (depth - level - 1);
+    if ((sorted[begin].key >> shift) == (sorted[end - 1].key >> shift)) return plan(begin, end, level + 1, limit, out);
+    for (size_t first = begin; first < end;) {
+      size_t last = first + 1;
+      while (last < end && (sorted[last].key >> shift) == (sorted[first].key >> shift)) ++last;
+      plan(first, last, level + 1, limit, out);
+      first = last;
+    }
+  }
 };
+
+unsigned workerCount() { return std::max(1u, std::min(64u, std::thread::hardware_concurrency())); }
+
+// Runs fn(i) for i in [0, n) on the worker threads, in contiguous slices.
+template <typename Fn>
+void parallelFor(size_t n, Fn fn) {
+  const unsigned workers = static_cast<unsigned>(std::min<size_t>(workerCount(), std::max<size_t>(n / 4096, 1)));
+  if (workers <= 1) {
+    for (size_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (unsigned w = 0; w < workers; ++w)
+    pool.emplace_back([&, w] {
+      for (size_t i = n * w / workers, e = n * (w + 1) / workers; i < e; ++i) fn(i);
+    });
+  for (auto& t : pool) t.join();
+}
+
+// Sorts by (key, node): slices sorted in parallel, then merged pairwise. The order is total, so
+// the result is the one sequential sort gives.
+void parallelSort(std::vector<Cell>& cells) {
+  auto less = [](const Cell& a, const Cell& b) { return a.key == b.key ? a.node < b.node : a.key < b.key; };
+  const size_t n = cells.size();
+  const unsigned slices = static_cast<unsigned>(std::min<size_t>(workerCount(), std::max<size_t>(n / 65536, 1)));
+  std::vector<size_t> bounds(slices + 1);
+  for (unsigned s = 0; s <= slices; ++s) bounds[s] = n * s / slices;
+  {
+    std::vector<std::thread> pool;
+    for (unsigned s = 0; s < slices; ++s)
+      pool.emplace_back([&, s] { std::sort(cells.begin() + bounds[s], cells.begin() + bounds[s + 1], less); });
+    for (auto& t : pool) t.join();
+  }
+  for (size_t width = 1; width < slices; width *= 2) {
+    std::vector<std::thread> pool;
+    for (size_t s = 0; s + width < slices; s += 2 * width) {
+      const size_t lo = bounds[s], mid = bounds[s + width], hi = bounds[std::min<size_t>(s + 2 * width, slices)];
+      pool.emplace_back([&, lo, mid, hi] {
+        std::inplace_merge(cells.begin() + lo, cells.begin() + mid, cells.begin() + hi, less);
+      });
+    }
+    for (auto& t : pool) t.join();
+  }
+}
 
 }  // namespace
 
@@ -217,29 +328,93 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
       tree->boundsMax[c] = hi;
     }
   }
-  sk::Nodes nodes;
-  nodes.positions.assign(cloud->positions, cloud->positions + n * 3);
-  nodes.covariances.assign(cloud->covariances, cloud->covariances + n * 6);
-  nodes.colors.assign(cloud->colors, cloud->colors + n * 3);
-  nodes.alphas.assign(cloud->alphas, cloud->alphas + n);
-  if (shStride) nodes.sh.assign(cloud->sh, cloud->sh + n * shStride);
-  nodes.shStride = shStride;
-  nodes.size.resize(n);
-  nodes.children.resize(n);
-  for (size_t i = 0; i < n; ++i) nodes.size[i] = 2.0f * sk::semiAxes(&nodes.covariances[i * 6])[0];
+  // The leaves, with their size and merge area (eigenvalues per leaf, in parallel).
+  sk::Store store;
+  store.positions.assign(cloud->positions, cloud->positions + n * 3);
+  store.covariances.assign(cloud->covariances, cloud->covariances + n * 6);
+  store.colors.assign(cloud->colors, cloud->colors + n * 3);
+  store.alphas.assign(cloud->alphas, cloud->alphas + n);
+  if (shStride) store.sh.assign(cloud->sh, cloud->sh + n * shStride);
+  store.size.resize(n);
+  store.area.resize(n);
+  store.kidStart.assign(n, 0);
+  store.kidCount.assign(n, 0);
+  sk::parallelFor(n, [&](size_t i) {
+    const auto axes = sk::semiAxes(&store.covariances[i * 6]);
+    store.size[i] = 2.0f * axes[0];
+    store.area[i] = sk::ellipsoidArea(axes);
+  });
   // LodTree.cpp:145-156, 198-204: Morton order and the octree
   const uint32_t depth = std::clamp(octree_depth == 0 ? sk::kMaxOctreeDepth : octree_depth, 1u,
                                     sk::kMaxOctreeDepth);
   float extent = 1e-6f;
   for (int c = 0; c < 3; ++c) extent = std::max(extent, tree->boundsMax[c] - tree->boundsMin[c]);
   std::vector<sk::Cell> sorted(n);
-  for (uint32_t i = 0; i < n; ++i)
-    sorted[i] = {sk::mortonKey(&nodes.positions[i * 3], tree->boundsMin, extent, depth), i};
-  std::sort(sorted.begin(), sorted.end(), [](const sk::Cell& a, const sk::Cell& b) {
-    return a.key == b.key ? a.node < b.node : a.key < b.key;
+  sk::parallelFor(n, [&](size_t i) {
+    sorted[i] = {sk::mortonKey(&store.positions[i * 3], tree->boundsMin, extent, depth),
+                 static_cast<uint32_t>(i)};
   });
-  sk::OctreeBuilder builder{nodes, sorted, std::max<size_t>(cluster_leaves == 0 ? 32 : cluster_leaves, 2), depth};
+  sk::parallelSort(sorted);
+  const size_t clusterLeaves = std::max<size_t>(cluster_leaves == 0 ? 32 : cluster_leaves, 2);
+  // Subtrees of at most `limit` leaves are built in parallel, each worker into a store of its
+  // own (node ids from n on); the nodes above them are built last. Node creation order differs
+  // from a sequential build, but the breadth-first layout below depends only on the tree, so the
+  // file is the same.
+  const unsigned workers = sk::workerCount();
+  const auto leafCount = static_cast<uint32_t>(n);
+  sk::Nodes shared{&store, &store, 0, 0, shStride};
+  sk::OctreeBuilder planner{shared, sorted, clusterLeaves, depth};
+  std::vector<sk::Task> tasks;
+  planner.plan(0, n, 0, std::max<size_t>(n / (16 * workers), 256), tasks);
+  std::vector<sk::Store> own(workers);
+  {
+    std::vector<size_t> bySize(tasks.size());
+    for (size_t t = 0; t < tasks.size(); ++t) bySize[t] = t;
+    std::sort(bySize.begin(), bySize.end(), [&](size_t a, size_t b) {
+      return tasks[a].end - tasks[a].begin > tasks[b].end - tasks[b].begin;
+    });
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < workers; ++w)
+      pool.emplace_back([&, w] {
+        sk::Nodes mine{&store, &own[w], leafCount, leafCount, shStride};
+        sk::OctreeBuilder builder{mine, sorted, clusterLeaves, depth};
+        for (size_t k; (k = next.fetch_add(1)) < bySize.size();) {
+          sk::Task& t = tasks[bySize[k]];
+          t.root = builder.build(t.begin, t.end, t.level);
+          t.worker = w;
+        }
+      });
+    for (auto& t : pool) t.join();
+  }
+  // Workers' nodes after the leaves, in worker order; their ids (n + local) shifted to match.
+  std::vector<uint32_t> offset(workers, 0);
+  for (unsigned w = 1; w < workers; ++w) offset[w] = offset[w - 1] + static_cast<uint32_t>(own[w - 1].count());
+  for (unsigned w = 0; w < workers; ++w) {
+    sk::Store& o = own[w];
+    for (uint32_t& id : o.kids)
+      if (id >= leafCount) id += offset[w];
+    const auto kidBase = static_cast<uint32_t>(store.kids.size());
+    for (uint32_t& k : o.kidStart) k += kidBase;
+    store.kids.insert(store.kids.end(), o.kids.begin(), o.kids.end());
+    store.kidStart.insert(store.kidStart.end(), o.kidStart.begin(), o.kidStart.end());
+    store.kidCount.insert(store.kidCount.end(), o.kidCount.begin(), o.kidCount.end());
+    store.positions.insert(store.positions.end(), o.positions.begin(), o.positions.end());
+    store.covariances.insert(store.covariances.end(), o.covariances.begin(), o.covariances.end());
+    store.colors.insert(store.colors.end(), o.colors.begin(), o.colors.end());
+    store.alphas.insert(store.alphas.end(), o.alphas.begin(), o.alphas.end());
+    store.sh.insert(store.sh.end(), o.sh.begin(), o.sh.end());
+    store.size.insert(store.size.end(), o.size.begin(), o.size.end());
+    store.area.insert(store.area.end(), o.area.begin(), o.area.end());
+    o = sk::Store{};
+  }
+  for (auto& t : tasks)
+    if (t.root >= leafCount) t.root += offset[t.worker];
+  std::sort(tasks.begin(), tasks.end(), [](const sk::Task& a, const sk::Task& b) { return a.begin < b.begin; });
+  sk::Nodes top{&store, &store, 0, 0, shStride};
+  sk::OctreeBuilder builder{top, sorted, clusterLeaves, depth, &tasks};
   const uint32_t root = builder.build(0, sorted.size(), 0);
+  auto& nodes = store;
   // LodTree.cpp:209-243: breadth-first layout, attributes copied in layout order
   const size_t total = nodes.count();
   std::vector<uint32_t> order;
@@ -247,17 +422,18 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
   tree->layout.assign(total, sk::LodNode{});
   order.push_back(root);
   for (size_t head = 0; head < order.size(); ++head) {
-    const auto& kids = nodes.children[order[head]];
+    const uint32_t id = order[head];
+    const uint32_t first = nodes.kidStart[id], count = nodes.kidCount[id];
     tree->layout[head].childStart = static_cast<uint32_t>(order.size());
-    tree->layout[head].childCount = static_cast<uint32_t>(kids.size());
-    for (const uint32_t kid : kids) order.push_back(kid);
+    tree->layout[head].childCount = count;
+    order.insert(order.end(), nodes.kids.begin() + first, nodes.kids.begin() + first + count);
   }
   tree->positions.resize(total * 3);
   tree->covariances.resize(total * 6);
   tree->colors.resize(total * 3);
   tree->alphas.resize(total);
   tree->sh.resize(total * shStride);
-  for (size_t i = 0; i < total; ++i) {
+  sk::parallelFor(total, [&](size_t i) {
     const uint32_t old = order[i];
     std::copy_n(&nodes.positions[old * 3], 3, &tree->positions[i * 3]);
     std::copy_n(&nodes.positions[old * 3], 3, tree->layout[i].position);
@@ -266,7 +442,7 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
     std::copy_n(&nodes.colors[old * 3], 3, &tree->colors[i * 3]);
     tree->alphas[i] = nodes.alphas[old];
     if (shStride) std::copy_n(&nodes.sh[old * shStride], shStride, &tree->sh[i * shStride]);
-  }
+  });
   tree->leafCount = static_cast<uint32_t>(n);
   tree->shDegree = degree;
   if (build_selection) {

@@ -908,7 +908,7 @@ def _copy_out(ptr, dtype, shape):
     if not ptr or int(np.prod(shape)) == 0:
         return None
     count = int(np.prod(shape)) * np.dtype(dtype).itemsize
-    raw = ctypes.string_at(ptr, count)
+    raw = (ctypes.c_char * count).from_address(ptr)  # a view; the one copy is below
     return np.frombuffer(raw, dtype).reshape(shape).copy()
 
 

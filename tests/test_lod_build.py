@@ -1,4 +1,5 @@
-"""The host LOD tree builder (sk_build_lod_tree) and .lodsplat writer against the reference's own
+"""The host LOD tree builder (sk_build_lod_tree, subtrees built on all host threads) and .lodsplat
+writer against the reference's own
 builder and writer: the same tree, selection data and file, bit for bit (CPU only)."""
 from __future__ import annotations
 
@@ -23,6 +24,8 @@ CLOUDS = {
     "random_sh2": lambda: bounded(synthetic.random_cloud(5000, seed=11, sh_degree=2, half_extent=4.0)),
     "random_sh3": lambda: bounded(synthetic.random_cloud(3000, seed=12, sh_degree=3, half_extent=2.0)),
     "clustered": lambda: bounded(synthetic.clustered_cloud(12, 400, seed=13, half_extent=30.0)),
+    # enough leaves for hundreds of subtrees built on separate threads
+    "clustered_80k": lambda: bounded(synthetic.clustered_cloud(80, 1000, seed=14, half_extent=50.0)),
 }
 
 
