@@ -241,7 +241,9 @@ sk_status sk_set_part_styles(sk_context* ctx, const sk_part_style* palette, cons
                              uint32_t state_count);
 
 /* ---- the frame (SplatRenderer::draw, :134) ------------------------------------------- */
-/* Enqueues LOD cut, cull, sort, binning and composite; returns without waiting. */
+/* Enqueues LOD cut, cull, sort, binning and composite; returns without waiting. A flat world keeps
+ * two frames in flight (MetalFrameSlots.h:8): with both slots busy the call first finishes the
+ * older frame. A LOD world keeps one. */
 sk_status sk_draw(sk_context* ctx, const sk_frame* frame);
 /* Waits for the last frame and copies its image (captureNextFrame). */
 sk_status sk_read_image(sk_context* ctx, void* host, size_t bytes, int32_t format);

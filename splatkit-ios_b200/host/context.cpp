@@ -77,7 +77,11 @@ Context::~Context() {
   for (auto& e : imageFree)
     if (e) cudaEventDestroy(e);
   if (copyStream) cudaStreamDestroy(copyStream);
-  if (done) cudaEventDestroy(done);
+  for (auto& sl : slots) {
+    if (sl.done) cudaEventDestroy(sl.done);
+    for (auto& ev : sl.events)
+      if (ev) cudaEventDestroy(ev);
+  }
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -140,9 +144,6 @@ sk_status Context::reserveScratch(FrameScratch& f, uint32_t sources, uint32_t in
   if (e == cudaSuccess) e = cudaMemsetAsync(f.sortWorkspace.ptr, 0, f.sortWorkspace.bytes, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(f.tileSortWorkspace.ptr, 0, f.tileSortWorkspace.bytes, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(f.visStatus.ptr, 0, f.visStatus.bytes, s);
-  if (e == cudaSuccess && !f.events[0])
-    for (auto& ev : f.events)
-      if (e == cudaSuccess) e = cudaEventCreate(&ev);
   if (e != cudaSuccess) return check(e, "frame buffers");
   f.sources = sources;
   f.instanceCapacity = instances;
@@ -181,8 +182,10 @@ sk_status Context::reserveView(uint32_t w, uint32_t h) {
   if (e == cudaSuccess && twoImages) e = image2.allocate(size_t{w} * h * pixelBytes);
   if (e == cudaSuccess) e = frameCounters.allocate(sizeof(FrameCounters));
   if (e == cudaSuccess) e = camera.allocate(sizeof(Camera));
-  if (e == cudaSuccess) e = hostCounters.allocate(sizeof(FrameCounters));
-  if (e == cudaSuccess) e = hostCamera.allocate(sizeof(Camera));
+  for (auto& sl : slots) {
+    if (e == cudaSuccess) e = sl.hostCounters.allocate(sizeof(FrameCounters));
+    if (e == cudaSuccess) e = sl.hostCamera.allocate(sizeof(Camera));
+  }
   return check(e, "view buffers");
 }
 
@@ -232,7 +235,8 @@ sk_status Context::validateRanges(const sk_frame& frame, uint32_t* total) const 
 }
 
 sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, const sk_frame& frame,
-                                   uint32_t total, cudaStream_t s, uint32_t timing) {
+                                   uint32_t total, cudaStream_t s, uint32_t timing,
+                                   cudaEvent_t* events) {
   // Events between stages separate the chained launches, so frame-only timing records just
   // the outer pair.
   const bool timed = timing == 1;
@@ -249,7 +253,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
                       f.cellLists.bytes >= cellListBytes(f.sources, cells);
   cudaError_t e = cudaMemsetAsync(fc, 0, sizeof(FrameCounters), s);
   if (e == cudaSuccess && !direct) e = clearTileRanges(static_cast<uint2*>(f.ranges.ptr), cells, s);
-  if (timing != 0) cudaEventRecord(f.events[0], s);
+  if (timing != 0) cudaEventRecord(events[0], s);
 
   const bool lod = world.lod;
   if (lod && e == cudaSuccess) {
@@ -278,7 +282,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     a.report = fc->lod;
     e = launchLodSelect(view.camera, a, s);
   }
-  if (timed) cudaEventRecord(f.events[1], s);
+  if (timed) cudaEventRecord(events[1], s);
 
   if (e == cudaSuccess && !lod && frame.range_count > 1) {
     // Ranges and their starts (SplatVisibility.metal:30-37); pageable copies are staged at once.
@@ -320,7 +324,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
                            static_cast<const uint32_t*>(styleStateTable.ptr), styleStateCount};
     e = launchVisibility(view.camera, v, degree, key16, lod, s);
   }
-  if (timed) cudaEventRecord(f.events[2], s);
+  if (timed) cudaEventRecord(events[2], s);
   if (e == cudaSuccess) {
     SortArgs a{};
     a.keysIn = static_cast<const uint32_t*>(f.keys.ptr);
@@ -335,7 +339,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     a.error = error;
     e = launchSort(a, s);
   }
-  if (timed) cudaEventRecord(f.events[3], s);
+  if (timed) cudaEventRecord(events[3], s);
   if (e == cudaSuccess && direct) {
     // each cell's list written in place, front to back, with its range
     BinArgs b{};
@@ -391,7 +395,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
   if (e == cudaSuccess && !direct)
     e = launchTileRanges(static_cast<const uint32_t*>(f.instKeysSorted.ptr), &fc->instances,
                          f.instanceCapacity, static_cast<uint2*>(f.ranges.ptr), binsX * binsY, s);
-  if (timed) cudaEventRecord(f.events[4], s);
+  if (timed) cudaEventRecord(events[4], s);
   if (e == cudaSuccess) {
     CompositeArgs c{};
     c.projected = static_cast<const Projected*>(f.projected.ptr);
@@ -409,41 +413,45 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     c.loaded = &fc->loaded;
     e = launchComposite(c, s);
   }
-  if (timing != 0) cudaEventRecord(f.events[5], s);
+  if (timing != 0) cudaEventRecord(events[5], s);
   if (e == cudaSuccess && view.hostCounters)
     e = cudaMemcpyAsync(view.hostCounters, fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, s);
   return check(e, "frame");
 }
 
-ViewTarget Context::plainView() {
+ViewTarget Context::plainView(const Slot& slot) {
   ViewTarget v;
   v.width = width;
   v.height = height;
-  v.image = imageOf(imageSlot);
+  v.image = imageOf(slot.image);
   v.counters = static_cast<FrameCounters*>(frameCounters.ptr);
-  v.hostCounters = static_cast<FrameCounters*>(hostCounters.ptr);
+  v.hostCounters = static_cast<FrameCounters*>(slot.hostCounters.ptr);
   v.camera = static_cast<const Camera*>(camera.ptr);
   return v;
 }
 
-sk_status Context::enqueuePlainFrame(const sk_frame& frame, uint32_t total) {
-  // The previous frame has completed, so the pinned camera can be rewritten.
-  *static_cast<Camera*>(hostCamera.ptr) = cameraFor(frame, width, height);
-  cudaError_t e = cudaMemcpyAsync(camera.ptr, hostCamera.ptr, sizeof(Camera),
+// Enqueues the slot's frame. Its pinned camera is free: the frame that used the slot before
+// has finished. The device camera is rewritten after the previous frame's kernels, in stream
+// order.
+sk_status Context::enqueueSlot(uint32_t index) {
+  Slot& slot = slots[index];
+  *static_cast<Camera*>(slot.hostCamera.ptr) = cameraFor(slot.frame, width, height);
+  cudaError_t e = cudaMemcpyAsync(camera.ptr, slot.hostCamera.ptr, sizeof(Camera),
                                   cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return check(e, "camera upload");
   // the image this frame draws into may still be on its way to a capture's host buffer
-  if (imageCopied[imageSlot]) {
-    e = cudaStreamWaitEvent(stream, imageFree[imageSlot], 0);
+  if (imageCopied[slot.image]) {
+    e = cudaStreamWaitEvent(stream, imageFree[slot.image], 0);
     if (e != cudaSuccess) return check(e, "capture wait");
   }
-  sk_status st = enqueuePipeline(scratch, plainView(), frame, total, stream, timeStages);
+  sk_status st = enqueuePipeline(scratch, plainView(slot), slot.frame, slot.total, stream,
+                                 timeStages, slot.events);
   if (st != SK_OK) return st;
-  st = check(cudaEventRecord(done, stream), "frame");
+  st = check(cudaEventRecord(slot.done, stream), "frame");
   if (st != SK_OK) return st;
   // captures of this frame copy its image once it is drawn (again after a redraw)
   for (auto& c : captures)
-    if (c.frame == submitted && (st = issueCapture(c)) != SK_OK) return st;
+    if (c.frame == slot.number && (st = issueCapture(c, slot)) != SK_OK) return st;
   return SK_OK;
 }
 
@@ -451,53 +459,57 @@ size_t Context::imageBytes() const {
   return size_t{width} * height * (imageFormat == SK_FORMAT_RGBA32F ? 16 : 4);
 }
 
-sk_status Context::issueCapture(Capture& c) {
+sk_status Context::issueCapture(Capture& c, const Slot& slot) {
   if (c.bytes < imageBytes()) {
     c.tooSmall = true;
     return SK_OK;
   }
-  cudaError_t e = cudaStreamWaitEvent(copyStream, done, 0);
+  cudaError_t e = cudaStreamWaitEvent(copyStream, slot.done, 0);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(c.host, imageOf(imageSlot), imageBytes(), cudaMemcpyDeviceToHost, copyStream);
+    e = cudaMemcpyAsync(c.host, imageOf(slot.image), imageBytes(), cudaMemcpyDeviceToHost, copyStream);
   if (e == cudaSuccess) e = cudaEventRecord(c.copied, copyStream);
-  if (e == cudaSuccess) e = cudaEventRecord(imageFree[imageSlot], copyStream);
+  if (e == cudaSuccess) e = cudaEventRecord(imageFree[slot.image], copyStream);
   if (e != cudaSuccess) return check(e, "capture copy");
-  imageCopied[imageSlot] = true;
+  imageCopied[slot.image] = true;
   c.issued = true;
   return SK_OK;
 }
 
-// Reads the last frame's counters once it completed; grows the instance buffers and draws
-// again when the binning ran out of room.
-sk_status Context::finishFrame(bool wait) {
-  if (!frameInFlight) return SK_OK;
-  if (wait) {
-    const cudaError_t e = cudaEventSynchronize(done);
-    if (e != cudaSuccess) return check(e, "frame wait");
-  } else if (cudaEventQuery(done) != cudaSuccess) {
-    return SK_OK;
-  }
-  frameInFlight = false;
-  ++completed;
-  const FrameCounters c = *static_cast<const FrameCounters*>(hostCounters.ptr);
+sk_status Context::finishOldest() {
+  if (inFlight.empty()) return SK_OK;
+  Slot& slot = slots[inFlight.front()];
+  cudaError_t e = cudaEventSynchronize(slot.done);
+  if (e != cudaSuccess) return check(e, "frame wait");
+  const FrameCounters c = *static_cast<const FrameCounters*>(slot.hostCounters.ptr);
   if (c.overflow) {
-    const uint32_t need = static_cast<uint32_t>(std::min<uint64_t>(
-        uint64_t{c.instances} + c.instances / 4 + 1024, 0x7fffffffu));
+    // Every frame in flight drew with these list buffers (or after one that did, into the same
+    // image): wait for all of them, grow the buffers and draw them all again, in order.
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return check(e, "frame wait");
+    uint32_t most = c.instances;
+    for (const uint32_t k : inFlight) {
+      const auto* fc = static_cast<const FrameCounters*>(slots[k].hostCounters.ptr);
+      most = std::max(most, fc->instances);
+    }
+    const uint32_t need = static_cast<uint32_t>(
+        std::min<uint64_t>(uint64_t{most} + most / 4 + 1024, 0x7fffffffu));
     sk_status st = reserveScratch(scratch, scratch.sources, need, scratch.maxTiles, stream);
-    if (st != SK_OK) return st;
-    st = enqueuePlainFrame(lastFrame, lastTotal);
-    if (st != SK_OK) return st;
-    frameInFlight = true;
-    --completed;
-    return finishFrame(true);
+    for (size_t k = 0; st == SK_OK && k < inFlight.size(); ++k) st = enqueueSlot(inFlight[k]);
+    if (st != SK_OK) {
+      inFlight.clear();  // nothing of theirs is left running
+      return st;
+    }
+    return finishOldest();
   }
+  inFlight.pop_front();
+  ++completed;
   lastCounters = c;
   if (timeStages != 0) {
     float ms[5] = {0, 0, 0, 0, 0};
     if (timeStages == 1)
-      for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], scratch.events[i], scratch.events[i + 1]);
+      for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], slot.events[i], slot.events[i + 1]);
     float all = 0;
-    cudaEventElapsedTime(&all, scratch.events[0], scratch.events[5]);
+    cudaEventElapsedTime(&all, slot.events[0], slot.events[5]);
     stats.select_ms = ms[0], stats.cull_ms = ms[1], stats.sort_ms = ms[2];
     stats.bin_ms = ms[3], stats.composite_ms = ms[4], stats.gpu_ms = all;
   }
@@ -507,6 +519,27 @@ sk_status Context::finishFrame(bool wait) {
   }
   if (c.error) return fail(SK_E_TIMEOUT, "a bounded device wait or bounds check failed in the last frame");
   return SK_OK;
+}
+
+sk_status Context::finishFrame(bool wait) {
+  sk_status first = SK_OK;
+  while (!inFlight.empty()) {
+    if (!wait && cudaEventQuery(slots[inFlight.front()].done) != cudaSuccess) break;
+    const sk_status st = finishOldest();
+    if (st == SK_E_DEVICE) return st;
+    if (first == SK_OK) first = st;
+  }
+  return first;
+}
+
+sk_status Context::finishThrough(uint64_t number) {
+  sk_status first = SK_OK;
+  while (!inFlight.empty() && slots[inFlight.front()].number <= number) {
+    const sk_status st = finishOldest();
+    if (st == SK_E_DEVICE) return st;
+    if (first == SK_OK) first = st;
+  }
+  return first;
 }
 
 sk_status Context::uploadCloud(const sk_cloud_view& cloud, int maxSh, World& w) {
@@ -575,7 +608,11 @@ sk_status sk_create(const sk_config* config, sk_context** out) {
   sk_default_policy(&ctx->policy);
   ctx->threshold.reset(ctx->policy.lod_error_pixels);
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SK_E_DEVICE;
-  if (cudaEventCreateWithFlags(&ctx->done, cudaEventDisableTiming) != cudaSuccess) return SK_E_DEVICE;
+  for (auto& sl : ctx->slots) {
+    if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) return SK_E_DEVICE;
+    for (auto& ev : sl.events)
+      if (cudaEventCreate(&ev) != cudaSuccess) return SK_E_DEVICE;
+  }
   if (ctx->reserveView(ctx->width, ctx->height) != SK_OK) return SK_E_DEVICE;
   const uint32_t tiles = ((ctx->width + 15) / 16) * ((ctx->height + 15) / 16);
   if (ctx->reserveScratch(ctx->scratch, 1, 1024, tiles, ctx->stream) != SK_OK) return SK_E_DEVICE;
@@ -810,24 +847,33 @@ sk_status sk_draw(sk_context* handle, const sk_frame* frame) {
     if (ctx->validateRanges(*frame, &total) != SK_OK)
       return ctx->fail(SK_E_INVALID, "invalid visibility ranges");
   }
-  // One frame in flight on the plain path: the previous one completes first.
-  sk_status st = ctx->finishFrame(true);
-  if (st == SK_E_DEVICE) return st;
+  // Two frames in flight (one on a LOD world): the oldest finishes first when all slots are busy.
+  const size_t depth = ctx->world.lod ? 1 : sk::Context::kFrameSlots;
+  while (ctx->inFlight.size() >= depth) {
+    const sk_status st = ctx->finishOldest();
+    if (st == SK_E_DEVICE) return st;
+  }
   if (!ctx->world.splats.ptr) total = 0;
+  uint32_t index = 0;
+  while (std::find(ctx->inFlight.begin(), ctx->inFlight.end(), index) != ctx->inFlight.end()) ++index;
+  sk::Context::Slot& slot = ctx->slots[index];
   if (ctx->twoImages) ctx->imageSlot ^= 1u;
-  ctx->lastFrame = *frame;
-  ctx->lastTotal = total;
-  ctx->lastRanges.assign(frame->ranges, frame->ranges + (frame->ranges ? frame->range_count : 0));
-  ctx->lastFrame.ranges = ctx->lastRanges.data();
-  ++ctx->submitted;  // this frame's number, which pending captures are bound to
+  slot.frame = *frame;
+  slot.total = total;
+  slot.ranges.assign(frame->ranges, frame->ranges + (frame->ranges ? frame->range_count : 0));
+  slot.frame.ranges = slot.ranges.data();
+  slot.image = ctx->imageSlot;
+  slot.number = ++ctx->submitted;  // pending captures are bound to this number
   for (auto& c : ctx->captures)
-    if (c.frame == 0) c.frame = ctx->submitted;
-  st = ctx->enqueuePlainFrame(ctx->lastFrame, total);
+    if (c.frame == 0) c.frame = slot.number;
+  const sk_status st = ctx->enqueueSlot(index);
   if (st != SK_OK) {
+    for (auto& c : ctx->captures)
+      if (c.frame == slot.number) c.frame = 0;
     --ctx->submitted;
     return st;
   }
-  ctx->frameInFlight = true;
+  ctx->inFlight.push_back(index);
   return SK_OK;
 }
 
@@ -916,7 +962,7 @@ sk_status sk_wait_capture(sk_context* handle, uint64_t ticket) {
   if (it == ctx->captures.end() || it->frame == 0)
     return ctx->fail(SK_E_INVALID, "no such capture, or its frame is not drawn yet");
   sk_status st = SK_OK;
-  if (ctx->frameInFlight && it->frame == ctx->submitted) st = ctx->finishFrame(true);  // may redraw
+  st = ctx->finishThrough(it->frame);  // may draw it again
   it = std::find_if(ctx->captures.begin(), ctx->captures.end(),
                     [&](const Context::Capture& c) { return c.ticket == ticket; });
   const cudaError_t e = cudaEventSynchronize(it->copied);

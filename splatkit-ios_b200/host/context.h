@@ -87,14 +87,9 @@ struct FrameScratch {
   DeviceBuffer lodIndices, lodFrontier[2], lodCosts, lodOffsets, lodPackets, lodState, lodStatus,
       lodCounters;
   uint32_t lodFrontierCapacity = 0;
-  cudaEvent_t events[6] = {};
   FrameScratch() = default;
   FrameScratch(const FrameScratch&) = delete;
   FrameScratch& operator=(const FrameScratch&) = delete;
-  ~FrameScratch() {
-    for (auto& e : events)
-      if (e) cudaEventDestroy(e);
-  }
 };
 
 // Where one view's results go.
@@ -130,9 +125,22 @@ struct Context {
   FrameScratch scratch;
   // the plain renderer's own view: image, counters, camera
   DeviceBuffer image, frameCounters, camera;
-  PinnedBuffer hostCounters, hostCamera;
-  cudaEvent_t done = nullptr;
-  bool frameInFlight = false;
+  // Frame slots: like the reference's frame loop (MetalFrameSlots.h:8) a flat world keeps two
+  // frames in flight, so the host enqueues the next frame while the GPU draws the last; a
+  // slot holds what finishing (or drawing again) its frame needs. LOD worlds keep one, so the
+  // adaptive threshold sees every frame's cut before the next selection.
+  static constexpr uint32_t kFrameSlots = 2;
+  struct Slot {
+    PinnedBuffer hostCounters, hostCamera;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t events[6] = {};
+    sk_frame frame{};
+    std::vector<sk_range> ranges;
+    uint32_t total = 0, image = 0;
+    uint64_t number = 0;  // the submitted-frame count it was drawn as
+  };
+  Slot slots[kFrameSlots];
+  std::deque<uint32_t> inFlight;  // slots of the frames in flight, oldest first
   // Frame captures (captureNextFrame): once one is requested the frames alternate between two
   // images, so the copy of one frame's image to the host (on copyStream) overlaps the drawing of
   // the next; a frame waits for the copy that still reads its image before it draws.
@@ -153,10 +161,7 @@ struct Context {
   uint64_t nextCapture = 1;
   void* imageOf(uint32_t slot) { return slot ? image2.ptr : image.ptr; }
   size_t imageBytes() const;
-  sk_status issueCapture(Capture& c);
-  sk_frame lastFrame{};
-  std::vector<sk_range> lastRanges;
-  uint32_t lastTotal = 0;
+  sk_status issueCapture(Capture& c, const Slot& slot);
   FrameCounters lastCounters{};
   sk_stats stats{};
   uint64_t submitted = 0, completed = 0;
@@ -178,10 +183,17 @@ struct Context {
   sk_status validateRanges(const sk_frame& frame, uint32_t* total) const;
   // The whole frame pipeline for one view on stream s; nothing waits on the host.
   sk_status enqueuePipeline(FrameScratch& f, const ViewTarget& v, const sk_frame& frame,
-                            uint32_t total, cudaStream_t s, uint32_t timing);
-  ViewTarget plainView();
-  sk_status enqueuePlainFrame(const sk_frame& frame, uint32_t total);
+                            uint32_t total, cudaStream_t s, uint32_t timing, cudaEvent_t* events);
+  ViewTarget plainView(const Slot& slot);
+  sk_status enqueueSlot(uint32_t slot);
+  // Finishes the oldest frame in flight (waiting for it); grows the list buffers and draws
+  // every frame in flight again when one overflowed.
+  sk_status finishOldest();
+  // Finishes every frame in flight (with wait false, only those already complete); reports the
+  // first error but always drains what it waits for.
   sk_status finishFrame(bool wait);
+  // Finishes the frames in flight up to frame `number`.
+  sk_status finishThrough(uint64_t number);
   sk_status uploadCloud(const sk_cloud_view& cloud, int maxSh, World& w);
   uint32_t instanceGuess(uint32_t sources) const;
 };

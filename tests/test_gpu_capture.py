@@ -118,3 +118,28 @@ def test_capture_misuse_is_rejected(cuda_device):
     r.draw(frame)
     assert r.read_image(sk.FORMAT_RGBA8).shape == (2 * h, 2 * w, 4)
     r.close()
+
+
+@pytest.mark.gpu
+def test_two_frames_in_flight_with_an_overflow(cuda_device):
+    # three draws without a wait: the first overflows its lists while the second is queued, so
+    # both are drawn again before the third takes the first one's slot
+    w, h = 640, 480
+    cloud = synthetic.random_cloud(6_000, seed=31, sh_degree=1, log_scale_mean=1.0)
+    frames = frames_for(cloud, w, h, (3, 40, 41))
+    r = sk.Renderer(w, h, image_format=sk.FORMAT_RGBA8)
+    r.upload_world(cloud, 1)
+    buffers = [pinned_image(w, h, sk.FORMAT_RGBA8) for _ in frames]
+    tickets = []
+    for f, b in zip(frames, buffers):
+        tickets.append(r.capture_next_frame(b))
+        r.draw(f)
+    got = [r.wait_capture(t).copy() for t in tickets]
+    last = r.read_image(sk.FORMAT_RGBA8).copy()
+    stats = r.stats()
+    r.close()
+    want = read_back(cloud, frames, w, h, sk.FORMAT_RGBA8)
+    for g, expected in zip(got, want):
+        assert np.array_equal(g, expected)
+    assert np.array_equal(last, want[-1])
+    assert stats["submitted_frames"] == stats["completed_frames"] == len(frames)
