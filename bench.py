@@ -140,9 +140,10 @@ def stage_bytes(stats, bits, n=SPLATS, width=WIDTH, height=HEIGHT, sh_words=24):
         # 32 B record per source splat, the SH record (96 B at SH3, device stride) of each
         # survivor, then a 4 B key, a 32 B projected record and a 16 B tile span per survivor
         "cull": 32 * n + 4 * sh_words * v + 52 * v,
-        # one all-digit histogram read + per pass read key(+value) and write key+value; the
-        # last pass skips the key write: 60 B/key at 32 bits, 28 B/key at 16 bits
-        "sort": (60 if bits == 32 else 28) * v,
+        # per pass read key(+value) and write key+value, the last pass skipping the key write (the
+        # digit histogram is summed by the cull as it writes the keys): 56 B/key at 32 bits,
+        # 24 B/key at 16 bits
+        "sort": (56 if bits == 32 else 24) * v,
         # direct cell lists: count and emit each read order + span (20 B per survivor); the
         # per-block cell counts are written, read and turned into block starts (read again by
         # the emission): 3 x 4 B per (block, cell); 8 B range per cell; 4 B written per entry
@@ -364,8 +365,9 @@ def run_ours(args):
                    "bin": "cell_lists_emit_1m_sh3_1080p", "composite": "composite_1m_sh3_1080p"}[dominant]
         traffic = traffic_from_profiles(profile) if args.bits == 16 else None
         passes = 2 if args.bits == 16 else 4
-        # visibility, depth sort (histogram + passes), cell lists (count, scan, emit), composite
-        launches_per_frame = 1 + (1 + passes) + 3 + 1
+        # visibility (with the depth keys' digit histogram), the depth sort's scatter passes, cell
+        # lists (count, scan, emit), composite
+        launches_per_frame = 1 + passes + 3 + 1
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,

@@ -59,26 +59,7 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t v = (&h[0][0])[i];
     if (v) atomicAdd(&accum[i], v);
   }
-  if (finishTile(counters)) {
-    // Exclusive digit bases per pass; clear the accumulators for the next sort.
-    __shared__ uint32_t warpSums[kWarps];
-    for (uint32_t p = 0; p < passes; ++p) {
-      const uint32_t d = threadIdx.x;
-      const uint32_t v = __ldcg(&accum[p * kBins + d]);
-      uint32_t inc = v;
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
-        if (laneId() >= static_cast<uint32_t>(o)) inc += up;
-      }
-      if (laneId() == 31) warpSums[d >> 5] = inc;
-      __syncthreads();
-      uint32_t before = 0;
-      for (uint32_t w = 0; w < (d >> 5); ++w) before += warpSums[w];
-      bases[p * kBins + d] = before + inc - v;
-      accum[p * kBins + d] = 0;
-      __syncthreads();
-    }
-  }
+  if (finishTile(counters)) finishDigitHistograms(accum, bases, passes);
 }
 
 // ---- 2. onesweep scatter ----------------------------------------------------------------
@@ -232,6 +213,9 @@ inline size_t alignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 uint32_t sortTileKeys() { return kTileKeys; }
 
+uint32_t* sortDigitAccumulators(const SortArgs& a) { return a.histogram; }
+uint32_t* sortDigitBases(const SortArgs& a) { return a.histogram + kMaxPasses * kBins; }
+
 static uint32_t sortTiles(uint32_t capacity, uint32_t tileKeys = kTileKeys) {
   return max(1u, (capacity + tileKeys - 1) / tileKeys);
 }
@@ -279,10 +263,13 @@ cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
   if (tiles > a.statusTiles) return cudaErrorInvalidValue;  // the workspace was bound for larger tiles
   uint32_t* accum = a.histogram;
   uint32_t* bases = a.histogram + kMaxPasses * kBins;
-  const uint32_t histBlocks = min(sortTiles(a.capacity), 148u * 4u);
-  cudaError_t e = launchChained(histogramKernel, histBlocks, kThreads, stream, a.keysIn, a.count,
-                                a.capacity, passes, accum, bases, a.counters);
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  if (!a.basesReady) {
+    const uint32_t histBlocks = min(sortTiles(a.capacity), 148u * 4u);
+    e = launchChained(histogramKernel, histBlocks, kThreads, stream, a.keysIn, a.count, a.capacity,
+                      passes, accum, bases, a.counters);
+    if (e != cudaSuccess) return e;
+  }
   const uint32_t* kin = a.keysIn;
   const uint32_t* vin = a.valuesIn;
   for (uint32_t p = 0; p < passes; ++p) {

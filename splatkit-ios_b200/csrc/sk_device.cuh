@@ -198,4 +198,28 @@ __device__ __forceinline__ bool finishTile(uint32_t* counters) {
   return last != 0u;
 }
 
+// The end of a radix sort's digit histogram, run by the last block of the kernel that summed it
+// (256 threads): accum[p][d] (the counts of digit d of pass p over all keys) become the exclusive
+// digit bases bases[p][d], and the accumulators are cleared for the next sort.
+__device__ __forceinline__ void finishDigitHistograms(uint32_t* accum, uint32_t* bases,
+                                                      uint32_t passes) {
+  __shared__ uint32_t warpSums[8];
+  const uint32_t d = threadIdx.x, lane = laneId();
+  for (uint32_t p = 0; p < passes; ++p) {
+    const uint32_t v = __ldcg(&accum[p * 256 + d]);
+    uint32_t inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= static_cast<uint32_t>(o)) inc += up;
+    }
+    if (lane == 31) warpSums[d >> 5] = inc;
+    __syncthreads();
+    uint32_t before = 0;
+    for (uint32_t w = 0; w < (d >> 5); ++w) before += warpSums[w];
+    bases[p * 256 + d] = before + inc - v;
+    accum[p * 256 + d] = 0;
+    __syncthreads();
+  }
+}
+
 }  // namespace sk

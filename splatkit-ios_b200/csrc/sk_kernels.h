@@ -34,6 +34,11 @@ struct VisibilityArgs {
   uint32_t epoch;
   uint32_t* error;
   PartLabels parts;  // labels.labels null: no part styling
+  // the depth sort's digit histogram, summed over the survivors' keys as they are written (the
+  // last block turns it into digit bases); sortPasses 0: not summed
+  uint32_t* sortAccum;
+  uint32_t* sortBases;
+  uint32_t sortPasses;
 };
 uint32_t visibilityTileSplats();
 // `cam` is a device pointer: the kernels stage it in shared memory, so a captured graph can be
@@ -84,7 +89,13 @@ struct SortArgs {
   uint32_t* error;
   uint32_t tileKeys;    // keys per scatter tile: 2048, 4096 (0: the default) or 6144
   uint32_t statusTiles; // tiles the bound status region holds (set by the bind)
+  // 1: the kernel that wrote the keys already summed their digits and left the bases in the
+  // workspace (VisibilityArgs.sortPasses); the histogram pass is skipped
+  uint32_t basesReady;
 };
+// Where a bound workspace keeps the digit accumulators (zero between sorts) and the bases.
+uint32_t* sortDigitAccumulators(const SortArgs& args);
+uint32_t* sortDigitBases(const SortArgs& args);
 uint32_t sortTileKeys();
 size_t sortWorkspaceBytes(uint32_t capacity);
 // Carves the workspace into the SortArgs fields.

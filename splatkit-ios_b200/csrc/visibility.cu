@@ -403,13 +403,18 @@ __device__ __forceinline__ void compactTile(VisibilitySmem& s, uint64_t* status,
 
 // Coalesced copy-out: consecutive threads write consecutive survivors, with the tiles each
 // survivor's quad touches on a width x height target.
+// With digitPasses > 0 each key's 8-bit digits are counted into digits[pass][digit].
 __device__ __forceinline__ void copyOutTile(const VisibilitySmem& s, uint32_t* keys,
                                             Projected* projected, uint4* spans, float width,
-                                            float height, uint32_t tilesX, uint32_t tilesY) {
+                                            float height, uint32_t tilesX, uint32_t tilesY,
+                                            uint32_t (*digits)[256] = nullptr,
+                                            uint32_t digitPasses = 0) {
   const uint32_t count = s.tileCount, base = s.tileBase;
   for (uint32_t k = threadIdx.x; k < count; k += kThreads) {
     const uint32_t slot = s.slotOf[k];
-    keys[base + k] = s.key[slot];
+    const uint32_t key = s.key[slot];
+    keys[base + k] = key;
+    for (uint32_t p = 0; p < digitPasses; ++p) atomicAdd(&digits[p][(key >> (8 * p)) & 0xffu], 1u);
     const uint4 lo = s.rec[2 * slot], hi = s.rec[2 * slot + 1];
     uint4* o = reinterpret_cast<uint4*>(projected + base + k);
     o[0] = lo;
@@ -424,7 +429,9 @@ __global__ void __launch_bounds__(kThreads, 4)
   chainedKernelStart();
   __shared__ VisibilitySmem s;
   __shared__ Camera cam;
+  __shared__ uint32_t digits[4][256];
   loadCamera(camera, &cam);
+  for (uint32_t p = 0; p < a.sortPasses; ++p) digits[p][threadIdx.x] = 0;
   const uint32_t tile = takeTile(a.counters);  // its barrier also publishes the camera
   loadBlockConstants(cam);
   const uint32_t total = kIndexed ? min(*a.indexCount, a.total) : a.total;
@@ -445,9 +452,18 @@ __global__ void __launch_bounds__(kThreads, 4)
     compactTile(s, a.status, tile, a.epoch, a.error);
     if (tile == tiles - 1 && threadIdx.x == 0) *a.visibleCount = s.tileBase + s.tileCount;
     copyOutTile(s, a.keys, a.projected, a.spans, cam.screenSize[0], cam.screenSize[1], a.tilesX,
-                a.tilesY);
+                a.tilesY, digits, a.sortPasses);
   }
   if (tiles == 0 && tile == 0 && threadIdx.x == 0) *a.visibleCount = 0;
+  if (a.sortPasses) {
+    __syncthreads();
+    for (uint32_t p = 0; p < a.sortPasses; ++p) {
+      const uint32_t v = digits[p][threadIdx.x];
+      if (v) atomicAdd(&a.sortAccum[p * 256 + threadIdx.x], v);
+    }
+    if (finishTile(a.counters)) finishDigitHistograms(a.sortAccum, a.sortBases, a.sortPasses);
+    return;
+  }
   finishTile(a.counters);
 }
 

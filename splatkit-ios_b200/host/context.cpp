@@ -295,6 +295,9 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
       e = cudaMemcpyAsync(f.rangeStarts.ptr, starts.data(), starts.size() * 4,
                           cudaMemcpyHostToDevice, s);
   }
+  // The depth sort's workspace: the cull sums the digits of the keys it writes into it.
+  SortArgs depthSort{};
+  sortBindWorkspace(depthSort, f.sortWorkspace.ptr, f.sources);
   if (e == cudaSuccess) {
     VisibilityArgs v{};
     v.splats = static_cast<const GpuSplat*>(world.splats.ptr);
@@ -322,11 +325,14 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
       v.parts = PartLabels{static_cast<const uint16_t*>(labels.ptr),
                            static_cast<const PartStyle*>(stylePalette.ptr),
                            static_cast<const uint32_t*>(styleStateTable.ptr), styleStateCount};
+    v.sortAccum = sortDigitAccumulators(depthSort);
+    v.sortBases = sortDigitBases(depthSort);
+    v.sortPasses = key16 ? 2u : 4u;
     e = launchVisibility(view.camera, v, degree, key16, lod, s);
   }
   if (timed) cudaEventRecord(events[2], s);
   if (e == cudaSuccess) {
-    SortArgs a{};
+    SortArgs a = depthSort;
     a.keysIn = static_cast<const uint32_t*>(f.keys.ptr);
     a.valuesIn = nullptr;
     a.keysOut = nullptr;
@@ -334,7 +340,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     a.count = &fc->visible;
     a.capacity = f.sources;
     a.bits = key16 ? 16 : 32;
-    sortBindWorkspace(a, f.sortWorkspace.ptr, f.sources);
+    a.basesReady = 1;
     a.epoch = nextEpoch(4);
     a.error = error;
     e = launchSort(a, s);
