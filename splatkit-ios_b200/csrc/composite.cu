@@ -11,8 +11,8 @@
 //
 // A block of 128 threads owns a 16x16 tile; each thread owns two horizontally adjacent pixels and
 // each warp an 8x8-pixel quadrant. The tile reads the list of the 32x32 binning cell it lies in
-// (the splats touching the cell, front to back) in batches of 256 records: thread i
-// fetches records i and i + 128 (two 128-bit loads each), turns it into the coverage form (pixel centre, inverse
+// (the splats touching the cell, front to back) in batches of 128 records: thread i
+// fetches record i (two 128-bit loads), turns it into the coverage form (pixel centre, inverse
 // axes, radius, log cutoff, colour) in shared memory and marks which of the four quadrants its
 // quad overlaps (separating-axis test). Each warp compacts, by ballot, the batch entries that
 // reach it and sweeps only those, both of its pixels per entry. The coverage decision (quad bound and 1/255 cutoff)
@@ -29,7 +29,7 @@ namespace {
 
 constexpr uint32_t kThreads = kTileSize * kTileSize / 2;  // 128: two pixels per thread
 constexpr uint32_t kWarps = kThreads / 32;
-constexpr uint32_t kEntries = 2 * kThreads;  // list entries staged per batch (two per thread)
+constexpr uint32_t kEntries = kThreads;  // list entries staged per batch (one per thread)
 constexpr uint32_t kQuadrant = kTileSize / 2;  // each warp owns an 8x8 quadrant
 
 struct alignas(16) Splat2D {
