@@ -40,7 +40,21 @@ struct Work {
   uint32_t* blockCounts;  // blocks x cells
   uint32_t* blockStarts;  // blocks x cells: the block's first slot in each cell's list
   uint64_t* status;       // one look-back word per group of 32 cells
+  const uint32_t* rankRange;  // a batch view's ranks (CellLists), else null
+  uint32_t* entryBase;
 };
+
+// The ranks the lists are built from: [first, first + n) of the depth order.
+__device__ __forceinline__ void ranksOf(const BinArgs& a, const Work& w, uint32_t& first,
+                                        uint32_t& n) {
+  if (w.rankRange) {
+    first = w.rankRange[0];
+    n = min(w.rankRange[1] - first, a.capacity);
+  } else {
+    first = 0;
+    n = min(*a.count, a.capacity);
+  }
+}
 
 __host__ __device__ inline uint32_t cellWords(uint32_t cells) { return (cells + 1) / 2; }
 __host__ __device__ inline size_t align16(size_t n) { return (n + 15) & ~size_t{15}; }
@@ -51,7 +65,7 @@ __host__ __device__ inline uint32_t blocksFor(uint32_t capacity) {
 
 __host__ __device__ inline Work workOf(void* workspace, uint32_t blocks, uint32_t cells) {
   uint8_t* p = static_cast<uint8_t*>(workspace);
-  Work w;
+  Work w{};
   w.blockCounts = reinterpret_cast<uint32_t*>(p);
   p += align16(size_t{blocks} * cells * 4);
   w.blockStarts = reinterpret_cast<uint32_t*>(p);
@@ -69,7 +83,9 @@ __global__ void __launch_bounds__(kThreads)
     cellCountKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells) {
   chainedKernelStart();
   __shared__ uint32_t hist[kDirectMaxCells];
-  const uint32_t n = min(*a.count, a.capacity);
+  uint32_t first, n;
+  ranksOf(a, work, first, n);
+  const uint32_t* order = a.order + first;
   const uint32_t begin = blockIdx.x * kBlockRanks;
   if (begin >= n) return;  // rows of idle blocks are never read
   for (uint32_t c = threadIdx.x; c < cells; c += kThreads) hist[c] = 0;
@@ -79,7 +95,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (uint32_t r = 0; r < kItems; ++r) {
     const uint32_t i = begin + r * kThreads + threadIdx.x;
-    value[r] = i < n ? __ldg(a.order + i) : 0xffffffffu;
+    value[r] = i < n ? order[i] : 0xffffffffu;
   }
 #pragma unroll
   for (uint32_t r = 0; r < kItems; ++r)
@@ -102,7 +118,9 @@ __global__ void __launch_bounds__(kScanThreads, 1)
   __shared__ uint32_t part[kScanWarps][33];
   __shared__ uint32_t cellStart[32];
   const uint32_t group = takeTile(counters);
-  const uint32_t n = min(*a.count, a.capacity);
+  uint32_t first, n;
+  ranksOf(a, work, first, n);
+  const uint32_t viewBase = work.entryBase ? work.entryBase[0] : 0u;
   const uint32_t active = blocksFor(n);
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
   const uint32_t cell = group * 32 + lane;
@@ -144,14 +162,20 @@ __global__ void __launch_bounds__(kScanThreads, 1)
       if (lane == 0)
         storeStatus(work.status + group, makeStatus(epoch, kFlagPrefix, before + aggregate));
     }
-    const uint32_t start = before + inc - total;
+    const uint32_t start = viewBase + before + inc - total;
     cellStart[lane] = start;
     if (valid)
       ranges[cell] = make_uint2(min(start, a.instanceCapacity),
                                 min(start + total, a.instanceCapacity));
     if (group == gridDim.x - 1 && lane == 31) {
-      *a.instanceCount = before + aggregate;
-      *a.overflow = before + aggregate > a.instanceCapacity ? 1u : 0u;
+      const uint32_t entries = viewBase + before + aggregate;
+      *a.instanceCount = entries;
+      if (work.entryBase) {
+        work.entryBase[1] = entries;
+        if (entries > a.instanceCapacity) *a.overflow = 1u;
+      } else {
+        *a.overflow = entries > a.instanceCapacity ? 1u : 0u;
+      }
     }
   }
   __syncthreads();
@@ -183,7 +207,9 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ uint32_t stageValue[kWarps][kChunk];
   __shared__ uint32_t stageOffset[kWarps][kChunk];
   __shared__ uint32_t startItem[kWarps][32];
-  const uint32_t n = min(*a.count, a.capacity);
+  uint32_t first, n;
+  ranksOf(a, work, first, n);
+  const uint32_t* order = a.order + first;
   const uint32_t begin = blockIdx.x * kBlockRanks;
   if (begin >= n) return;
   const uint32_t words = cellWords(cells);
@@ -205,7 +231,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (uint32_t r = 0; r < kItems; ++r) {
     const uint32_t i = begin + warp * kChunk + r * 32 + lane;
-    value[r] = i < n ? __ldg(a.order + i) : 0xffffffffu;
+    value[r] = i < n ? order[i] : 0xffffffffu;
   }
 #pragma unroll
   for (uint32_t r = 0; r < kItems; ++r) {
@@ -306,21 +332,28 @@ size_t cellListBytes(uint32_t capacity, uint32_t cells) {
   return workBytes(blocksFor(std::max(capacity, 1u)), std::max(cells, 1u));
 }
 
+cudaError_t cellListsConfigure() {
+  static bool configured = false;
+  if (configured) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(cellEmitKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(emitDynamicBytes(kDirectMaxCells)));
+  if (e == cudaSuccess) configured = true;
+  return e;
+}
+
 cudaError_t launchCellLists(const BinArgs& a, const CellLists& lists, cudaStream_t stream) {
   const uint32_t cells = lists.cells;
   if (!cellListsFit(a.capacity, cells) || cells != a.tilesX * a.tilesY)
     return cudaErrorInvalidValue;
-  static bool configured = false;
-  if (!configured) {
-    const cudaError_t e =
-        cudaFuncSetAttribute(cellEmitKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(emitDynamicBytes(kDirectMaxCells)));
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  cudaError_t e = cellListsConfigure();
+  if (e != cudaSuccess) return e;
   const uint32_t blocks = blocksFor(a.capacity);
-  const Work work = workOf(lists.workspace, blocks, cells);
-  cudaError_t e = launchChained(cellCountKernel, blocks, kThreads, stream, a, work, cells);
+  Work work = workOf(lists.workspace, blocks, cells);
+  if (lists.status) work.status = lists.status;
+  work.rankRange = lists.rankRange;
+  work.entryBase = lists.entryBase;
+  e = launchChained(cellCountKernel, blocks, kThreads, stream, a, work, cells);
   if (e != cudaSuccess) return e;
   e = launchChained(cellScanKernel, cellGroups(cells), kScanThreads, stream, a, work, cells,
                     lists.ranges, lists.counters, lists.epoch, lists.error);

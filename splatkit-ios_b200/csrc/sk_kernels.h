@@ -153,11 +153,20 @@ struct CellLists {
   uint32_t* counters;   // two words, zero before the first launch (each launch restores them)
   uint32_t epoch;       // look-back epoch, fresh per launch
   uint32_t* error;      // SK_DEVERR_* bits
+  // One view of a batch (null for a plain frame): its ranks are [rankRange[0], rankRange[1]) of
+  // args.order (args.capacity bounds their count), its entries follow entryBase[0] earlier ones
+  // (the entry count after it is written to entryBase[1], args.overflow only set), and its
+  // look-back words are `status` (one per group of 32 cells, cleared before the batch).
+  const uint32_t* rankRange;
+  uint32_t* entryBase;
+  uint64_t* status;
 };
 // Whether a target of `cells` cells takes the direct path.
 bool cellListsFit(uint32_t capacity, uint32_t cells);
 size_t cellListBytes(uint32_t capacity, uint32_t cells);
 cudaError_t launchCellLists(const BinArgs& args, const CellLists& lists, cudaStream_t stream);
+// Sets the emission kernel's shared-memory limit (once; before any stream capture).
+cudaError_t cellListsConfigure();
 
 // ---- composite (composite.cu) ----------------------------------------------------------
 enum PixelFormat : int { kRgba8 = 0, kRgba32f = 1 };

@@ -185,6 +185,26 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
       std::max<uint64_t>(l.instances, sources * 4), 0x7fffffffu));
   sk_status st = reserve(l, static_cast<uint32_t>(sources), guess, items, tiles, count, pixels);
   if (st != SK_OK) return st;
+  // Every view's lists written in place when each has at most kDirectMaxCells cells.
+  uint32_t mostSources = 1, mostCells = 1;
+  for (const BatchView& t : l.table) {
+    mostSources = std::max(mostSources, t.count);
+    mostCells = std::max(mostCells, t.binsX * t.binsY);
+  }
+  l.directLists = mostCells <= kDirectMaxCells && cellListsConfigure() == cudaSuccess;
+  if (l.directLists) {
+    l.cellGroupsPerView = (mostCells + 31) / 32;
+    void* before[3] = {l.cellLists.ptr, l.cellStatus.ptr, l.entryBases.ptr};
+    cudaError_t e = l.cellLists.allocate(cellListBytes(mostSources, mostCells));
+    if (e == cudaSuccess) e = l.cellStatus.allocate(size_t{count} * l.cellGroupsPerView * 8);
+    if (e == cudaSuccess) e = l.entryBases.allocate(size_t{count + 1} * 4);
+    if (e != cudaSuccess) return check(e, "batch cell lists");
+    if (before[0] != l.cellLists.ptr || before[1] != l.cellStatus.ptr || before[2] != l.entryBases.ptr) {
+      if (l.graph) cudaGraphExecDestroy(l.graph);  // a captured graph points at the old buffers
+      l.graph = nullptr;
+      l.graphShape.clear();
+    }
+  }
   std::memcpy(l.hostViews.ptr, l.table.data(), size_t{count} * sizeof(BatchView));
   std::memcpy(l.hostCameras.ptr, l.cams.data(), size_t{count} * sizeof(Camera));
   return SK_OK;
@@ -200,7 +220,15 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
   const auto* views = static_cast<const BatchView*>(l.viewTable.ptr);
   const auto* viewFirst = static_cast<const uint32_t*>(l.viewFirst.ptr);
   cudaError_t e = cudaMemsetAsync(fc, 0, sizeof(FrameCounters), s);
-  if (e == cudaSuccess) e = clearTileRanges(static_cast<uint2*>(l.ranges.ptr), l.totalBins, s);
+  if (e == cudaSuccess && !l.directLists)
+    e = clearTileRanges(static_cast<uint2*>(l.ranges.ptr), l.totalBins, s);
+  if (e == cudaSuccess && l.directLists) {
+    // each view's entries start where the previous view's end; its cell groups' look-back words
+    // must read "not ready" (a replayed graph reuses its epochs)
+    e = cudaMemsetAsync(l.entryBases.ptr, 0, size_t{l.viewCount + 1} * 4, s);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(l.cellStatus.ptr, 0, size_t{l.viewCount} * l.cellGroupsPerView * 8, s);
+  }
   if (e == cudaSuccess && clearStatus) {
     e = cudaMemsetAsync(l.visStatus.ptr, 0, size_t{l.totalItems} * 8, s);
     SortArgs probe{};
@@ -244,7 +272,33 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     a.error = error;
     e = launchSort(a, s);
   }
-  if (e == cudaSuccess) {
+  for (uint32_t v = 0; e == cudaSuccess && l.directLists && v < l.viewCount; ++v) {
+    // view v's ranks are order[viewFirst[v] .. viewFirst[v + 1]) (views in order by the key's
+    // high bits), its cells binBase .. binBase + binsX * binsY of the batch
+    const BatchView& t = l.table[v];
+    BinArgs b{};
+    b.spans = static_cast<const uint4*>(l.spans.ptr);
+    b.order = static_cast<const uint32_t*>(l.order.ptr);
+    b.count = &fc->visible;
+    b.capacity = std::max(t.count, 1u);
+    b.width = t.width, b.height = t.height, b.tilesX = t.binsX, b.tilesY = t.binsY;
+    b.instanceValues = static_cast<uint32_t*>(l.instValuesSorted.ptr);
+    b.instanceCapacity = l.instances;
+    b.instanceCount = &fc->instances;
+    b.overflow = &fc->overflow;
+    CellLists cl{};
+    cl.cells = t.binsX * t.binsY;
+    cl.workspace = l.cellLists.ptr;
+    cl.ranges = static_cast<uint2*>(l.ranges.ptr) + t.binBase;
+    cl.counters = counters + 8;
+    cl.epoch = nextEpoch(1);
+    cl.error = error;
+    cl.rankRange = viewFirst + v;
+    cl.entryBase = static_cast<uint32_t*>(l.entryBases.ptr) + v;
+    cl.status = static_cast<uint64_t*>(l.cellStatus.ptr) + size_t{v} * l.cellGroupsPerView;
+    e = launchCellLists(b, cl, s);
+  }
+  if (e == cudaSuccess && !l.directLists) {
     BinArgs b{};
     b.spans = static_cast<const uint4*>(l.spans.ptr);
     b.order = static_cast<const uint32_t*>(l.order.ptr);
@@ -262,7 +316,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     b.balanced = tuning.balancedEmit ? 1u : 0u;
     e = launchBinning(b, s);
   }
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess && !l.directLists) {
     SortArgs a{};
     a.keysIn = static_cast<const uint32_t*>(l.instKeys.ptr);
     a.valuesIn = static_cast<const uint32_t*>(l.instValues.ptr);
@@ -277,7 +331,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     a.error = error;
     e = launchSort(a, s);
   }
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && !l.directLists)
     e = launchTileRanges(static_cast<const uint32_t*>(l.instKeysSorted.ptr), &fc->instances,
                          l.instances, static_cast<uint2*>(l.ranges.ptr), l.totalBins, s);
   if (e == cudaSuccess) {

@@ -41,6 +41,11 @@ struct BatchLane {
   DeviceBuffer keys, projected, spans, order, sortWorkspace, visStatus, binSums;
   DeviceBuffer instKeys, instValues, instKeysSorted, instValuesSorted, tileSortWorkspace;
   DeviceBuffer ranges, viewFirst, counters, frameCounters, viewTable, cameras, image;
+  // direct cell lists (every view at most kDirectMaxCells cells): one workspace reused view
+  // after view, per view the look-back words of its cell groups, and each view's first entry
+  DeviceBuffer cellLists, cellStatus, entryBases;
+  bool directLists = false;
+  uint32_t cellGroupsPerView = 0;
   // pinned host
   PinnedBuffer hostViews, hostCameras, hostCounters, hostViewFirst, hostImage;
   // the submission it holds
