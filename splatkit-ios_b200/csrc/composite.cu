@@ -126,8 +126,10 @@ __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const f
   const float2 u = __ffma2_rn(pair(w0.z), dx, pair(m01dy));
   const float2 v = __ffma2_rn(pair(w1.x), dx, pair(m11dy));
   const float2 q = __fmul2_rn(pair(0.5f), __ffma2_rn(u, u, __fmul2_rn(v, v)));
-  const bool c0 = p.T.x >= cutoff && fabsf(u.x) <= w1.z && fabsf(v.x) <= w1.z && q.x <= w1.w;
-  const bool c1 = p.T.y >= cutoff && fabsf(u.y) <= w1.z && fabsf(v.y) <= w1.z && q.y <= w1.w;
+  // |u|, |v| <= radius as one bound on the larger (a NaN u or v makes q NaN, so the q test
+  // still fails as the separate bounds would)
+  const bool c0 = p.T.x >= cutoff && fmaxf(fabsf(u.x), fabsf(v.x)) <= w1.z && q.x <= w1.w;
+  const bool c1 = p.T.y >= cutoff && fmaxf(fabsf(u.y), fabsf(v.y)) <= w1.z && q.y <= w1.w;
   if (!__any_sync(0xffffffffu, c0 || c1)) return;  // the whole quadrant misses this splat
   const float2 e = __ffma2_rn(q, pair(-1.4426950408889634f), pair(c.x));
   const float a0 = c0 ? fminf(exp2Approx(e.x), 1.0f) : 0.0f;
@@ -249,7 +251,7 @@ __global__ void __launch_bounds__(kThreads) compositeKernel(const __grid_constan
       for (uint32_t k0 = 0; k0 < count; k0 += 16) {
         if (__all_sync(0xffffffffu, finished())) break;
         const uint32_t k1 = min(count, k0 + 16);
-#pragma unroll 2
+#pragma unroll 4
         for (uint32_t k = k0; k < k1; ++k) {
           const Splat2D& s = sm.splat[sm.list[warp][k]];
           const float4 w0 = reinterpret_cast<const float4*>(&s)[0];
