@@ -60,7 +60,7 @@ __device__ __forceinline__ uint32_t coverageForm(const uint4 lo, const uint4 hi,
   s.m10 = -__fmul_rn(a1y, inv);
   s.m11 = __fmul_rn(a1x, inv);
   const float peak = highHalf(hi.y);
-  s.lcut = lnF32(__fmul_rn(255.0f, peak));
+  s.lcut = __fmul_rn(2.0f, lnF32(__fmul_rn(255.0f, peak)));  // 2 ln(255 peak), exact doubling
   s.lpeak = __log2f(peak);
   s.radius = asF(hi.z);
   s.r = lowHalf(hi.x);
@@ -116,7 +116,7 @@ __device__ __forceinline__ float exp2Approx(float x) {
 // Both pixels against one splat. px = the two pixel centres' x; m01dy, m11dy = m01 dy and
 // m11 dy, shared by the row. The coverage terms u, v, q are the oracle's FP32 sequence per pixel
 // (px - cx is px + (-cx) exactly); an uncovered or finished pixel takes alpha 0, which leaves
-// its colour and transmittance bit for bit as they were. alpha = min(1, 2^(log2 peak - q log2 e))
+// its colour and transmittance bit for bit as they were. alpha = min(1, 2^(log2 peak - q log2(e) / 2))
 // and T -= T alpha.
 template <bool kCount>
 __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const float4 w1,
@@ -125,13 +125,15 @@ __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const f
   const float2 dx = __fadd2_rn(px, pair(-w0.x));
   const float2 u = __ffma2_rn(pair(w0.z), dx, pair(m01dy));
   const float2 v = __ffma2_rn(pair(w1.x), dx, pair(m11dy));
-  const float2 q = __fmul2_rn(pair(0.5f), __ffma2_rn(u, u, __fmul2_rn(v, v)));
+  // q = u^2 + v^2 against 2 ln(255 peak): the oracle's (u^2 + v^2) / 2 <= ln(255 peak) with both
+  // sides doubled, which is exact, so every decision is the same
+  const float2 q = __ffma2_rn(u, u, __fmul2_rn(v, v));
   // |u|, |v| <= radius as one bound on the larger (a NaN u or v makes q NaN, so the q test
   // still fails as the separate bounds would)
   const bool c0 = p.T.x >= cutoff && fmaxf(fabsf(u.x), fabsf(v.x)) <= w1.z && q.x <= w1.w;
   const bool c1 = p.T.y >= cutoff && fmaxf(fabsf(u.y), fabsf(v.y)) <= w1.z && q.y <= w1.w;
   if (!__any_sync(0xffffffffu, c0 || c1)) return;  // the whole quadrant misses this splat
-  const float2 e = __ffma2_rn(q, pair(-1.4426950408889634f), pair(c.x));
+  const float2 e = __ffma2_rn(q, pair(-0.7213475204444817f), pair(c.x));  // -q log2(e) / 2
   const float a0 = c0 ? fminf(exp2Approx(e.x), 1.0f) : 0.0f;
   const float a1 = c1 ? fminf(exp2Approx(e.y), 1.0f) : 0.0f;
   const float2 alpha = make_float2(a0, a1);
