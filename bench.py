@@ -163,6 +163,28 @@ def traffic_from_profiles(stem):
     return None
 
 
+def instructions_from_profiles(stem):
+    """Warp instructions per launch from the committed ncu summary of this kernel, when present."""
+    path = ROOT / "profiles" / f"{stem}.md"
+    if path.exists():
+        m = re.search(r"warp instructions \(`smsp__inst_executed.sum`\) \| ([0-9.eE+]+)", path.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def issue_roofline(instructions, ms, sm_mhz, sms=148, schedulers=4):
+    """The dominant kernel against instruction issue, the bound that applies to it: warp
+    instructions per launch (its ncu summary) / live duration, against one warp instruction per
+    scheduler per clock at the sampled SM clock."""
+    if not instructions or not ms or not sm_mhz:
+        return None
+    achieved = instructions / (ms / 1000.0)
+    peak = sms * schedulers * sm_mhz * 1e6
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp inst/s",
+            "frac": achieved / peak, "instructions_per_launch": instructions}
+
+
 def measured_peaks():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -378,6 +400,8 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes": bytes_by_stage[dominant],
                          "profile": f"profiles/{profile}.md"},
+            "issue_roofline": issue_roofline(instructions_from_profiles(profile) if args.bits == 16 else None,
+                                             mean[dominant + "_ms"], clocks.summary().get("sm_mhz")),
             "stages_ms": mean,
             "stage_timing": "a second pass over the same frames with events around each stage and fragment counting",
             "stage_gbs": {k: bytes_by_stage[k] / (mean[k + "_ms"] / 1000.0) / 1e9
