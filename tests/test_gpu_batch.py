@@ -1,7 +1,8 @@
 """The batched multi-view path (sk_batch_*) against the plain per-frame path, view by view.
 
-A batch runs every stage once over all its views (several worlds, several target sizes) with
-the plain frame's arithmetic, so each view's image and survivor count must equal what sk_draw
+A batch runs every stage once over all its views (several worlds, several target sizes; the cell
+lists view after view, or for targets above 4096 cells one sort over all views) with the plain
+frame's arithmetic, so each view's image and survivor count must equal what sk_draw
 gives for that view with 16-bit depth keys — bit for bit, not just within tolerance.
 """
 from __future__ import annotations
@@ -75,6 +76,23 @@ def test_batch_of_two_worlds_and_five_sizes_equals_plain_frames(worlds):
         assert stats["views"] == 10 and stats["device_error"] == 0
         assert stats["visible"] == sum(batch.view_visible(ticket, i) for i in range(10))
         check_against_plain(batch, ticket, views)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graphs", [False, True])
+def test_batch_with_a_view_above_the_direct_cell_limit(worlds, graphs):
+    # 2560 x 2048 is 80 x 64 = 5120 binning cells, above the 4096 that lists are written in place
+    # for: the whole batch takes the sorted path (emission + stable sort of (cell, splat))
+    views = views_for(worlds, 3)
+    r, cloud = worlds[0]
+    view, eye = skcam.orbit_view(23, radius=15.0)
+    views.insert(1, sk.BatchView(r, sk.Frame(view, proj_for(2560, 2048), eye, [(0, cloud.count)], 3),
+                                 2560, 2048))
+    with sk.Batch(lanes=1, max_views=8, use_graphs=graphs) as batch:
+        for _ in range(2 if graphs else 1):  # with graphs: captured, then replayed
+            ticket = batch.submit(views)
+            batch.wait(ticket)
+            check_against_plain(batch, ticket, views)
 
 
 @pytest.mark.gpu
