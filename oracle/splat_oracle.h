@@ -117,7 +117,7 @@ uint32_t sko_lod_select(const sko_camera* cam, const sko_cluster* clusters, uint
                         uint32_t* stats6);
 
 // Front-to-back composite of `count` projected records in `order`, W x H, RGBA, row 0 on
-// top. precision 64: the FP64 evaluation the kernels are judged against; 32: the same in
+// top. precision 64: the FP64 evaluation the kernels are checked against; 32: the same in
 // FP32 (the CPU baseline). Coverage decisions (quad bound, 1/255 cutoff) use the FP32
 // formula the kernel uses, so both sides agree on each splat's support.
 // `opaque`: 1 puts the background under the remainder (alpha 1); 0 leaves coverage in alpha.
