@@ -165,13 +165,24 @@ struct Cell {
 };
 
 // LodTree.cpp:133-142
+// Bit k of a 21-bit value to bit 3k.
+uint64_t spreadBits3(uint32_t v) {
+  uint64_t x = v & 0x1fffffu;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+
 uint64_t mortonKey(const float* position, const float* boundsMin, float extent, uint32_t depth) {
   const uint32_t resolution = 1u << depth;
   uint64_t key = 0;
   for (uint32_t c = 0; c < 3; ++c) {
     const float unit = std::clamp((position[c] - boundsMin[c]) / extent, 0.0f, 1.0f);
     const uint32_t grid = std::min(static_cast<uint32_t>(unit * resolution), resolution - 1);
-    for (uint32_t bit = 0; bit < depth; ++bit) key |= uint64_t{(grid >> bit) & 1u} << (3 * bit + c);
+    key |= spreadBits3(grid) << c;  // grid < 2^depth: bit k of axis c lands at 3k + c
   }
   return key;
 }
@@ -390,6 +401,22 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
   // Workers' nodes after the leaves, in worker order; their ids (n + local) shifted to match.
   std::vector<uint32_t> offset(workers, 0);
   for (unsigned w = 1; w < workers; ++w) offset[w] = offset[w - 1] + static_cast<uint32_t>(own[w - 1].count());
+  {
+    // room for every worker's nodes and the few built last, so appending never moves the leaves
+    size_t interior = 0, kids = 0;
+    for (const auto& o : own) interior += o.count(), kids += o.kids.size();
+    const size_t nodesTotal = n + interior + tasks.size() + 64;
+    store.positions.reserve(nodesTotal * 3);
+    store.covariances.reserve(nodesTotal * 6);
+    store.colors.reserve(nodesTotal * 3);
+    store.alphas.reserve(nodesTotal);
+    if (shStride) store.sh.reserve(nodesTotal * shStride);
+    store.size.reserve(nodesTotal);
+    store.area.reserve(nodesTotal);
+    store.kidStart.reserve(nodesTotal);
+    store.kidCount.reserve(nodesTotal);
+    store.kids.reserve(kids + n + 64 * clusterLeaves);
+  }
   for (unsigned w = 0; w < workers; ++w) {
     sk::Store& o = own[w];
     for (uint32_t& id : o.kids)

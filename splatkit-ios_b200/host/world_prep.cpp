@@ -184,8 +184,17 @@ void buildSelection(const CloudRef& cloud, const LodNode* layout, uint32_t nodeC
     clusters.resize(order.size());
     clusters[head] = cluster;
   }
-  // Bottom up: bounds, merge error, colour variance, opacity, leaf count.
-  for (size_t k = clusters.size(); k-- > 0;) {
+  // Bottom up: bounds, merge error, colour variance, opacity, leaf count. A cluster reads only
+  // its own node and its children, which sit in the next BFS level, so the levels are done
+  // deepest first and the clusters of one level on all host threads.
+  std::vector<uint32_t> level(clusters.size(), 0);
+  std::vector<size_t> levelStart{0};
+  for (size_t k = 0; k < clusters.size(); ++k) {
+    if (k > 0 && level[k] != level[k - 1]) levelStart.push_back(k);
+    for (uint32_t j = 0; j < clusters[k].childCount; ++j) level[clusters[k].childStart + j] = level[k] + 1;
+  }
+  levelStart.push_back(clusters.size());
+  auto finish = [&](size_t k) {
     LodCluster& cluster = clusters[k];
     const float* parent = &cloud.positions[cluster.node * 3];
     const float* parentCov = &cloud.covariances[cluster.node * 6];
@@ -236,6 +245,21 @@ void buildSelection(const CloudRef& cloud, const LodNode* layout, uint32_t nodeC
         std::abs(std::min(cloud.alphas[cluster.node], 1.0f) - (1.0f - coincidentTransmittance));
     cluster.error = std::max(cluster.error, cluster.radius * peakDifference);
     cluster.colorVariance = weightSum > 0 ? weightedVariance / weightSum : 0;
+  };
+  const int threads = std::max(1, static_cast<int>(std::thread::hardware_concurrency()));
+  for (size_t l = levelStart.size() - 1; l-- > 0;) {
+    const size_t first = levelStart[l], count = levelStart[l + 1] - first;
+    const int workers = std::max(1, std::min<int>(threads, static_cast<int>(count / 2048)));
+    if (workers == 1) {
+      for (size_t k = 0; k < count; ++k) finish(first + k);
+      continue;
+    }
+    std::vector<std::thread> pool;
+    for (int w = 0; w < workers; ++w)
+      pool.emplace_back([&, w] {
+        for (size_t k = count * w / workers, e = count * (w + 1) / workers; k < e; ++k) finish(first + k);
+      });
+    for (auto& t : pool) t.join();
   }
 }
 
