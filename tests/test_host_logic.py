@@ -145,3 +145,17 @@ def test_policy_validation_matches_reference(reference):
              (1.0, 0, 0.5, 1.0, 32, (0, 1.5, 0), False)]
     for *args, expected in cases:
         assert reference.valid_render_policy(*args) == expected
+
+
+def test_frame_entry_points_reject_a_missing_context():
+    # argument checks come before any device work, so they hold without a GPU
+    import ctypes
+    lib = sk.library()
+    t = ctypes.c_uint64()
+    buf = np.zeros(16, np.uint8)
+    assert lib.sk_set_timing(None, 1) == sk.SK_E_INVALID
+    assert lib.sk_set_binning(None, 0) == sk.SK_E_INVALID
+    assert lib.sk_capture_next_frame(None, buf.ctypes.data, buf.nbytes, sk.FORMAT_RGBA8,
+                                     ctypes.byref(t)) == sk.SK_E_INVALID
+    assert lib.sk_wait_capture(None, 1) == sk.SK_E_INVALID
+    assert lib.sk_draw(None, None) == sk.SK_E_INVALID
