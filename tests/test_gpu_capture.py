@@ -1,7 +1,7 @@
 """captureNextFrame (sk_capture_next_frame / sk_wait_capture): captures taken one frame behind the
 draws, copied while the next frame renders, hold exactly the images sk_read_image gives for the
 same frames; a frame redrawn after an overflow of its lists is captured as redrawn; misuse is
-rejected."""
+rejected; the timing modes draw the same pixels."""
 from __future__ import annotations
 
 import math
@@ -143,3 +143,28 @@ def test_two_frames_in_flight_with_an_overflow(cuda_device):
         assert np.array_equal(g, expected)
     assert np.array_equal(last, want[-1])
     assert stats["submitted_frames"] == stats["completed_frames"] == len(frames)
+
+
+@pytest.mark.gpu
+def test_timing_modes_draw_the_same_image(cuda_device):
+    # sk_set_timing: 1 per-stage events and fragment counts, 2 the frame's own pair, 0 nothing;
+    # none of them changes a pixel
+    w, h = 640, 480
+    cloud = synthetic.random_cloud(100_000, seed=8, sh_degree=1)
+    (frame,) = frames_for(cloud, w, h, (12,))
+    r = sk.Renderer(w, h, image_format=sk.FORMAT_RGBA8)
+    r.upload_world(cloud, 1)
+    images, stats = {}, {}
+    for mode in (True, "frame", False):
+        r.set_timing(mode)
+        r.draw(frame)
+        images[mode] = r.read_image(sk.FORMAT_RGBA8).copy()
+        stats[mode] = r.stats()
+    r.close()
+    assert np.array_equal(images[True], images["frame"])
+    assert np.array_equal(images[True], images[False])
+    assert stats[True]["gpu_ms"] > 0 and stats[True]["composite_ms"] > 0
+    assert stats[True]["fragments"] > 0
+    assert stats["frame"]["gpu_ms"] > 0 and stats["frame"]["composite_ms"] == 0
+    for mode in (True, "frame", False):
+        assert stats[mode]["draw_count"] == stats[True]["draw_count"]
