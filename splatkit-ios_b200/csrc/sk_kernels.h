@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "sk_layout.h"
 
@@ -217,5 +218,28 @@ struct LodArgs {
 };
 uint32_t lodTileClusters();
 cudaError_t launchLodSelect(const Camera* cam, const LodArgs& args, cudaStream_t stream);
+
+// ---- LOD tree build (tree_build.cu) -----------------------------------------------------
+// The octree of sk_build_lod_tree built on the device from host arrays; the nodes come back in
+// the breadth-first layout (node 0 the root), childStart/childCount per node (0/0 for a leaf).
+struct LodBuildInput {
+  const float* positions;    // host, 3 per splat
+  const float* covariances;  // 6
+  const float* colors;       // 3
+  const float* alphas;
+  const float* sh;           // shStride per splat (nullptr when shStride is 0)
+  uint32_t count;
+  uint32_t shStride;
+  float boundsMin[3];
+  float extent;  // the largest side of the bounds (at least 1e-6)
+  uint32_t depth;          // 1 .. 21
+  uint32_t clusterLeaves;  // >= 2
+};
+struct LodBuildOutput {
+  uint32_t count = 0;
+  std::vector<float> positions, covariances, colors, alphas, sh, size;
+  std::vector<uint32_t> childStart, childCount;
+};
+cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out);
 
 }  // namespace sk

@@ -309,6 +309,38 @@ struct BuiltTree {
   float boundsMin[3] = {0, 0, 0}, boundsMax[3] = {0, 0, 0};
 };
 
+namespace {
+
+// The build's bounds: the caller's (a loader's cloud bounds), else the positions' own box.
+void treeBounds(const sk_cloud_view* cloud, const float* bounds_min, const float* bounds_max,
+                BuiltTree& tree) {
+  const size_t n = cloud->count;
+  for (int c = 0; c < 3; ++c) {
+    if (bounds_min && bounds_max) {
+      tree.boundsMin[c] = bounds_min[c];
+      tree.boundsMax[c] = bounds_max[c];
+    } else {
+      float lo = cloud->positions[c], hi = lo;
+      for (size_t i = 1; i < n; ++i) {
+        lo = std::min(lo, cloud->positions[i * 3 + c]);
+        hi = std::max(hi, cloud->positions[i * 3 + c]);
+      }
+      tree.boundsMin[c] = lo;
+      tree.boundsMax[c] = hi;
+    }
+  }
+}
+
+// The selection data of a laid-out tree (buildLodSelectionData).
+void attachSelection(BuiltTree& tree) {
+  const size_t shStride = static_cast<size_t>((tree.shDegree + 1) * (tree.shDegree + 1) - 1) * 3;
+  const auto total = static_cast<uint32_t>(tree.layout.size());
+  host::CloudRef ref{tree.positions.data(), tree.covariances.data(), tree.colors.data(),
+                     tree.alphas.data(), shStride ? tree.sh.data() : nullptr, total, tree.shDegree};
+  host::buildSelection(ref, tree.layout.data(), total, tree.clusters, tree.leaves);
+}
+
+}  // namespace
 }  // namespace sk
 
 extern "C" {
@@ -324,21 +356,7 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
   const int degree = cloud->sh ? std::max(0, std::min(cloud->sh_degree, 3)) : 0;
   const size_t shStride = static_cast<size_t>((degree + 1) * (degree + 1) - 1) * 3;
   auto tree = std::make_unique<sk::BuiltTree>();
-  // bounds: the caller's (a loader's cloud bounds), else the positions' own box
-  for (int c = 0; c < 3; ++c) {
-    if (bounds_min && bounds_max) {
-      tree->boundsMin[c] = bounds_min[c];
-      tree->boundsMax[c] = bounds_max[c];
-    } else {
-      float lo = cloud->positions[c], hi = lo;
-      for (size_t i = 1; i < n; ++i) {
-        lo = std::min(lo, cloud->positions[i * 3 + c]);
-        hi = std::max(hi, cloud->positions[i * 3 + c]);
-      }
-      tree->boundsMin[c] = lo;
-      tree->boundsMax[c] = hi;
-    }
-  }
+  sk::treeBounds(cloud, bounds_min, bounds_max, *tree);
   // The leaves, with their size and merge area (eigenvalues per leaf, in parallel).
   sk::Store store;
   store.positions.assign(cloud->positions, cloud->positions + n * 3);
@@ -472,13 +490,57 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
   });
   tree->leafCount = static_cast<uint32_t>(n);
   tree->shDegree = degree;
-  if (build_selection) {
-    sk::host::CloudRef ref{tree->positions.data(), tree->covariances.data(), tree->colors.data(),
-                           tree->alphas.data(), shStride ? tree->sh.data() : nullptr,
-                           static_cast<uint32_t>(total), degree};
-    sk::host::buildSelection(ref, tree->layout.data(), static_cast<uint32_t>(total), tree->clusters,
-                             tree->leaves);
+  if (build_selection) sk::attachSelection(*tree);
+  *out = reinterpret_cast<sk_lod_tree*>(tree.release());
+  return SK_OK;
+}
+
+sk_status sk_build_lod_tree_device(const sk_cloud_view* cloud, const float* bounds_min,
+                                   const float* bounds_max, uint32_t octree_depth,
+                                   uint32_t cluster_leaves, int32_t build_selection,
+                                   sk_lod_tree** out) {
+  if (!cloud || !out || cloud->count == 0 || !cloud->positions || !cloud->covariances ||
+      !cloud->colors || !cloud->alphas)
+    return SK_E_INVALID;
+  *out = nullptr;
+  const int degree = cloud->sh ? std::max(0, std::min(cloud->sh_degree, 3)) : 0;
+  const auto shStride = static_cast<uint32_t>(((degree + 1) * (degree + 1) - 1) * 3);
+  auto tree = std::make_unique<sk::BuiltTree>();
+  sk::treeBounds(cloud, bounds_min, bounds_max, *tree);
+  sk::LodBuildInput in{};
+  in.positions = cloud->positions;
+  in.covariances = cloud->covariances;
+  in.colors = cloud->colors;
+  in.alphas = cloud->alphas;
+  in.sh = shStride ? cloud->sh : nullptr;
+  in.count = cloud->count;
+  in.shStride = shStride;
+  in.extent = 1e-6f;
+  for (int c = 0; c < 3; ++c) {
+    in.boundsMin[c] = tree->boundsMin[c];
+    in.extent = std::max(in.extent, tree->boundsMax[c] - tree->boundsMin[c]);
   }
+  in.depth = std::clamp(octree_depth == 0 ? sk::kMaxOctreeDepth : octree_depth, 1u, sk::kMaxOctreeDepth);
+  in.clusterLeaves = std::max(cluster_leaves == 0 ? 32u : cluster_leaves, 2u);
+  sk::LodBuildOutput built;
+  if (sk::buildLodTreeGpu(in, built) != cudaSuccess) return SK_E_DEVICE;
+  const uint32_t total = built.count;
+  tree->positions = std::move(built.positions);
+  tree->covariances = std::move(built.covariances);
+  tree->colors = std::move(built.colors);
+  tree->alphas = std::move(built.alphas);
+  tree->sh = std::move(built.sh);
+  tree->layout.assign(total, sk::LodNode{});
+  for (uint32_t i = 0; i < total; ++i) {
+    sk::LodNode& node = tree->layout[i];
+    std::copy_n(&tree->positions[size_t{i} * 3], 3, node.position);
+    node.size = built.size[i];
+    node.childStart = built.childStart[i];
+    node.childCount = built.childCount[i];
+  }
+  tree->leafCount = cloud->count;
+  tree->shDegree = degree;
+  if (build_selection) sk::attachSelection(*tree);
   *out = reinterpret_cast<sk_lod_tree*>(tree.release());
   return SK_OK;
 }

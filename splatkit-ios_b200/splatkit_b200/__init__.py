@@ -251,6 +251,8 @@ _SIGNATURES = {
     "sk_write_lodsplat": (ctypes.c_int32, [ctypes.POINTER(_LodView), _f32p, _f32p, ctypes.c_char_p]),
     "sk_build_lod_tree": (ctypes.c_int32, [ctypes.POINTER(_Cloud), _f32p, _f32p, ctypes.c_uint32, ctypes.c_uint32,
                                            ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "sk_build_lod_tree_device": (ctypes.c_int32, [ctypes.POINTER(_Cloud), _f32p, _f32p, ctypes.c_uint32,
+                                                  ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     "sk_lod_tree_view": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_LodView), _f32p, _f32p]),
     "sk_lod_tree_free": (None, [ctypes.c_void_p]),
     "sk_upload_labels": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32]),
@@ -913,20 +915,22 @@ def _copy_out(ptr, dtype, shape):
 
 
 def build_lod_tree(cloud: Cloud, bounds_min=None, bounds_max=None, octree_depth: int = 0,
-                   cluster_leaves: int = 0, selection: bool = True) -> LodTree:
-    """buildLodTree on the host (sk_build_lod_tree): bounds default to the cloud's, else the
-    positions' own box."""
+                   cluster_leaves: int = 0, selection: bool = True, device: bool = False) -> LodTree:
+    """buildLodTree: bounds default to the cloud's, else the positions' own box. On the host
+    (sk_build_lod_tree, bit for bit the reference's tree) or, with device=True, on the current GPU
+    (sk_build_lod_tree_device: the same layout, attributes within a few ulp)."""
     lib = library()
+    entry = "sk_build_lod_tree_device" if device else "sk_build_lod_tree"
     lo = bounds_min if bounds_min is not None else cloud.bounds_min
     hi = bounds_max if bounds_max is not None else cloud.bounds_max
     lo = None if lo is None else np.ascontiguousarray(lo, np.float32)
     hi = None if hi is None else np.ascontiguousarray(hi, np.float32)
     v = cloud.view()
     handle = ctypes.c_void_p()
-    st = lib.sk_build_lod_tree(ctypes.byref(v), _ptr(lo), _ptr(hi), octree_depth, cluster_leaves,
-                               1 if selection else 0, ctypes.byref(handle))
+    st = getattr(lib, entry)(ctypes.byref(v), _ptr(lo), _ptr(hi), octree_depth, cluster_leaves,
+                             1 if selection else 0, ctypes.byref(handle))
     if st != SK_OK:
-        raise SplatError(st, "sk_build_lod_tree")
+        raise SplatError(st, entry)
     try:
         t = _LodView()
         bmin, bmax = np.zeros(3, np.float32), np.zeros(3, np.float32)

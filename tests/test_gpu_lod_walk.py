@@ -56,3 +56,21 @@ def test_walk_cuts_and_orders_match_the_oracle(oracle, walk_tree):
         assert projected.tobytes() == oproj.tobytes(), f"frame {i}"
         assert np.array_equal(order, oracle.stable_argsort(okeys)), f"frame {i}"
     r.close()
+
+
+@pytest.mark.gpu
+def test_device_tree_build_has_the_host_layout(walk_tree):
+    """The same 6M-leaf tree built on the GPU (sk_build_lod_tree_device): the layout is the host
+    builder's exactly, attributes to a few ulp."""
+    cloud = synthetic.clustered_cloud(2000, 3000, seed=0)
+    pos = np.asarray(cloud.positions, np.float32)
+    cloud.bounds_min, cloud.bounds_max = pos.min(axis=0), pos.max(axis=0)
+    gpu = sk.build_lod_tree(cloud, device=True)
+    host = walk_tree
+    assert gpu.leaf_count == host.leaf_count and len(gpu.layout) == len(host.layout)
+    np.testing.assert_array_equal(gpu.layout["child_start"], host.layout["child_start"])
+    np.testing.assert_array_equal(gpu.layout["child_count"], host.layout["child_count"])
+    np.testing.assert_allclose(gpu.nodes.positions, host.nodes.positions, rtol=1e-4, atol=1e-3)
+    np.testing.assert_allclose(gpu.layout["size"], host.layout["size"], rtol=1e-3, atol=1e-5)
+    np.testing.assert_array_equal(gpu.clusters["leaf_count"], host.clusters["leaf_count"])
+    np.testing.assert_array_equal(gpu.leaves, host.leaves)
