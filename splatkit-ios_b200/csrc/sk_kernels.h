@@ -237,8 +237,8 @@ struct LodBuildInput {
 };
 struct LodBuildOutput {
   uint32_t count = 0;
-  std::vector<float> positions, covariances, colors, alphas, sh, size;
-  std::vector<uint32_t> childStart, childCount;
+  std::vector<float> positions, covariances, colors, alphas, sh;
+  std::vector<LodNode> layout;
 };
 cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out);
 

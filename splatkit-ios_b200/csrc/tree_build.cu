@@ -279,8 +279,8 @@ struct NodeArrays {
   float* colors;       // 3
   float* alphas;
   float* sh;           // shStride
-  float* size;
-  float* area;
+  float* area;         // merge weight per unit opacity
+  LodNode* layout;     // position, size, child range
 };
 
 // 4. one level, deepest first: leaves copy their splat, the others merge their children
@@ -303,8 +303,10 @@ __global__ void mergeKernel(uint32_t m, uint32_t levelBase, const uint32_t* chil
     for (int c = 0; c < 3; ++c) out.colors[size_t{node} * 3 + c] = inColors[size_t{s} * 3 + c];
     out.alphas[node] = inAlphas[s];
     for (uint32_t c = 0; c < shStride; ++c) out.sh[size_t{node} * shStride + c] = inSh[size_t{s} * shStride + c];
-    out.size[node] = leafSize[s];
     out.area[node] = leafArea[s];
+    out.layout[node] = LodNode{{inPositions[size_t{s} * 3], inPositions[size_t{s} * 3 + 1],
+                                inPositions[size_t{s} * 3 + 2]},
+                               leafSize[s], childStart[node], 0u};
     return;
   }
   const uint32_t first = childStart[node];
@@ -352,24 +354,23 @@ __global__ void mergeKernel(uint32_t m, uint32_t levelBase, const uint32_t* chil
   for (int c = 0; c < 6; ++c) out.covariances[size_t{node} * 6 + c] = cov[c];
   for (int c = 0; c < 3; ++c) out.colors[size_t{node} * 3 + c] = rgb[c];
   out.alphas[node] = alpha;
-  out.size[node] = 2.0f * axes[0] * lodOpacityReach(alpha);
   out.area[node] = a;
+  out.layout[node] = LodNode{{center[0], center[1], center[2]},
+                             2.0f * axes[0] * lodOpacityReach(alpha), first, cnt};
 }
 
 uint32_t blocksOf(uint32_t n, uint32_t per) { return std::max(1u, (n + per - 1) / per); }
 
-struct Buffers {
-  std::vector<void*> all;
-  cudaError_t error = cudaSuccess;
+// Carves one device allocation into the build's arrays (256-byte aligned); a first pass with no
+// base only sums the sizes.
+struct Arena {
+  uint8_t* base = nullptr;
+  size_t bytes = 0;
   template <typename T>
   T* get(size_t count) {
-    void* p = nullptr;
-    if (error == cudaSuccess) error = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
-    if (error == cudaSuccess) all.push_back(p);
-    return static_cast<T*>(p);
-  }
-  ~Buffers() {
-    for (void* p : all) cudaFree(p);
+    const size_t at = (bytes + 255) & ~size_t{255};
+    bytes = at + std::max<size_t>(count, 1) * sizeof(T);
+    return base ? reinterpret_cast<T*>(base + at) : nullptr;
   }
 };
 
@@ -382,43 +383,55 @@ cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out) {
   cudaStream_t s = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e != cudaSuccess) return e;
+  uint8_t* memory = nullptr;
   {
-    Buffers b;
-    float* positions = b.get<float>(size_t{n} * 3);
-    float* covariances = b.get<float>(size_t{n} * 6);
-    float* colors = b.get<float>(size_t{n} * 3);
-    float* alphas = b.get<float>(n);
-    float* sh = b.get<float>(std::max<size_t>(size_t{n} * shStride, 1));
-    float* leafSize = b.get<float>(n);
-    float* leafArea = b.get<float>(n);
-    uint32_t* keyLo = b.get<uint32_t>(n);
-    uint32_t* keyHi = b.get<uint32_t>(n);
-    uint32_t* orderLo = b.get<uint32_t>(n);
-    uint32_t* hiByLo = b.get<uint32_t>(n);
-    uint32_t* sortedIndex = b.get<uint32_t>(n);
-    uint32_t* sortedLo = b.get<uint32_t>(n);
-    uint32_t* sortedHi = b.get<uint32_t>(n);
-    uint32_t* sortCount = b.get<uint32_t>(1);
-    uint32_t* sortError = b.get<uint32_t>(1);
-    void* sortWork = b.get<uint8_t>(sortWorkspaceBytes(n));
-    const uint32_t maxNodes = 2 * n;
-    Element* levelA = b.get<Element>(n);
-    Element* levelB = b.get<Element>(n);
-    uint32_t* counts = b.get<uint32_t>(n);
-    uint32_t* offsets = b.get<uint32_t>(n);
-    uint32_t* blockTotals = b.get<uint32_t>(blocksOf(n, 1024));
-    uint32_t* grand = b.get<uint32_t>(1);
-    uint32_t* childStart = b.get<uint32_t>(maxNodes);
-    uint32_t* childCount = b.get<uint32_t>(maxNodes);
-    uint32_t* leafOf = b.get<uint32_t>(maxNodes);
-    NodeArrays nodes{b.get<float>(size_t{maxNodes} * 3), b.get<float>(size_t{maxNodes} * 6),
-                     b.get<float>(size_t{maxNodes} * 3), b.get<float>(maxNodes),
-                     b.get<float>(std::max<size_t>(size_t{maxNodes} * shStride, 1)),
-                     b.get<float>(maxNodes), b.get<float>(maxNodes)};
-    if ((e = b.error) != cudaSuccess) {
+    Arena b;
+    float *positions, *covariances, *colors, *alphas, *sh, *leafSize, *leafArea;
+    uint32_t *keyLo, *keyHi, *orderLo, *hiByLo, *sortedIndex, *sortedLo, *sortedHi, *sortCount,
+        *sortError, *counts, *offsets, *blockTotals, *grand, *childStart, *childCount, *leafOf;
+    void* sortWork;
+    Element *levelA, *levelB;
+    NodeArrays nodes;
+    const uint32_t maxNodes = 2 * n;  // every interior node has two children or more
+    auto carve = [&] {
+      positions = b.get<float>(size_t{n} * 3);
+      covariances = b.get<float>(size_t{n} * 6);
+      colors = b.get<float>(size_t{n} * 3);
+      alphas = b.get<float>(n);
+      sh = b.get<float>(size_t{n} * shStride);
+      leafSize = b.get<float>(n);
+      leafArea = b.get<float>(n);
+      keyLo = b.get<uint32_t>(n);
+      keyHi = b.get<uint32_t>(n);
+      orderLo = b.get<uint32_t>(n);
+      hiByLo = b.get<uint32_t>(n);
+      sortedIndex = b.get<uint32_t>(n);
+      sortedLo = b.get<uint32_t>(n);
+      sortedHi = b.get<uint32_t>(n);
+      sortCount = b.get<uint32_t>(1);
+      sortError = b.get<uint32_t>(1);
+      sortWork = b.get<uint8_t>(sortWorkspaceBytes(n));
+      levelA = b.get<Element>(n);
+      levelB = b.get<Element>(n);
+      counts = b.get<uint32_t>(n);
+      offsets = b.get<uint32_t>(n);
+      blockTotals = b.get<uint32_t>(blocksOf(n, 1024));
+      grand = b.get<uint32_t>(1);
+      childStart = b.get<uint32_t>(maxNodes);
+      childCount = b.get<uint32_t>(maxNodes);
+      leafOf = b.get<uint32_t>(maxNodes);
+      nodes = NodeArrays{b.get<float>(size_t{maxNodes} * 3), b.get<float>(size_t{maxNodes} * 6),
+                         b.get<float>(size_t{maxNodes} * 3), b.get<float>(maxNodes),
+                         b.get<float>(size_t{maxNodes} * shStride), b.get<float>(maxNodes),
+                         b.get<LodNode>(maxNodes)};
+    };
+    carve();
+    if ((e = cudaMalloc(&memory, b.bytes)) != cudaSuccess) {
       cudaStreamDestroy(s);
       return e;
     }
+    b = Arena{memory, 0};
+    carve();
     auto up = [&](void* dst, const void* src, size_t bytes) {
       if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
     };
@@ -521,9 +534,7 @@ cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out) {
       out.colors.resize(size_t{total} * 3);
       out.alphas.resize(total);
       out.sh.resize(size_t{total} * shStride);
-      out.size.resize(total);
-      out.childStart.resize(total);
-      out.childCount.resize(total);
+      out.layout.resize(total);
       auto down = [&](void* dst, const void* src, size_t bytes) {
         if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
       };
@@ -532,13 +543,12 @@ cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out) {
       down(out.colors.data(), nodes.colors, size_t{total} * 12);
       down(out.alphas.data(), nodes.alphas, size_t{total} * 4);
       if (shStride) down(out.sh.data(), nodes.sh, size_t{total} * shStride * 4);
-      down(out.size.data(), nodes.size, size_t{total} * 4);
-      down(out.childStart.data(), childStart, size_t{total} * 4);
-      down(out.childCount.data(), childCount, size_t{total} * 4);
+      down(out.layout.data(), nodes.layout, size_t{total} * sizeof(LodNode));
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     }
     if (e != cudaSuccess) cudaStreamSynchronize(s);
   }
+  cudaFree(memory);
   cudaStreamDestroy(s);
   return e;
 }

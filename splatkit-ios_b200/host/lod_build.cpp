@@ -524,20 +524,12 @@ sk_status sk_build_lod_tree_device(const sk_cloud_view* cloud, const float* boun
   in.clusterLeaves = std::max(cluster_leaves == 0 ? 32u : cluster_leaves, 2u);
   sk::LodBuildOutput built;
   if (sk::buildLodTreeGpu(in, built) != cudaSuccess) return SK_E_DEVICE;
-  const uint32_t total = built.count;
   tree->positions = std::move(built.positions);
   tree->covariances = std::move(built.covariances);
   tree->colors = std::move(built.colors);
   tree->alphas = std::move(built.alphas);
   tree->sh = std::move(built.sh);
-  tree->layout.assign(total, sk::LodNode{});
-  for (uint32_t i = 0; i < total; ++i) {
-    sk::LodNode& node = tree->layout[i];
-    std::copy_n(&tree->positions[size_t{i} * 3], 3, node.position);
-    node.size = built.size[i];
-    node.childStart = built.childStart[i];
-    node.childCount = built.childCount[i];
-  }
+  tree->layout = std::move(built.layout);
   tree->leafCount = cloud->count;
   tree->shDegree = degree;
   if (build_selection) sk::attachSelection(*tree);
