@@ -518,6 +518,14 @@ def measure_lod_walk():
     t0 = time.perf_counter()
     tree = sk.build_lod_tree(cloud)
     build_s = time.perf_counter() - t0
+    # the same tree built on the GPU (after one small build that loads the module)
+    sk.build_lod_tree(synthetic.random_cloud(1000, seed=1), device=True)
+    t0 = time.perf_counter()
+    device_tree = sk.build_lod_tree(cloud, device=True)
+    device_build_s = time.perf_counter() - t0
+    same_layout = bool(np.array_equal(device_tree.layout["child_start"], tree.layout["child_start"]) and
+                       np.array_equal(device_tree.layout["child_count"], tree.layout["child_count"]))
+    del device_tree
     r = sk.Renderer(WIDTH, HEIGHT, image_format=sk.FORMAT_RGBA8, time_stages=True)
     r.apply_render_policy(sk.Policy(lod_error_pixels=1.5, sort_depth_bits=16))
     r.upload_lod_world(tree, 0, 4_000_000)
@@ -544,7 +552,10 @@ def measure_lod_walk():
                         f"{len(tree.layout)} nodes, 1.5 px cut, 300-frame walk at 1920x1080",
             "frames_per_s": 300 / (sum(gpu_ms) / 1000.0), "mean_gpu_ms": float(np.mean(gpu_ms)),
             "mean_select_ms": float(np.mean(select_ms)), "mean_cut_splats": float(np.mean(cut)),
-            "tree_build_s": build_s}
+            "tree_build_s": build_s, "tree_build_device_s": device_build_s,
+            "tree_build_device_same_layout": same_layout,
+            "tree_build_how": "Python build_lod_tree with selection data, node arrays copied out; host: "
+                              "all host threads; device: keys, sort, levels and merges on the GPU"}
 
 
 # ---- serving: Poisson requests over 8 resident scenes -----------------------------------------
