@@ -227,8 +227,8 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
 /* The same tree built on the GPU (current device): Morton keys and a radix sort on the device,
  * then the octree breadth first, one pass per level, and the merges deepest level first. The
  * layout (child ranges) is sk_build_lod_tree's exactly; node attributes agree to a few ulp (the
- * eigen-solve's acos/cos and the surface formula's powf are the device's). SK_E_DEVICE on a CUDA
- * error. */
+ * eigen-solve's acos/cos and the surface formula's powf are the device's). SK_E_LIMIT above
+ * 2^31 - 1 splats; SK_E_DEVICE on a CUDA error (out of device memory included). */
 sk_status sk_build_lod_tree_device(const sk_cloud_view* cloud, const float* bounds_min,
                                    const float* bounds_max, uint32_t octree_depth,
                                    uint32_t cluster_leaves, int32_t build_selection,

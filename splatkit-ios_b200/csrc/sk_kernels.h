@@ -240,6 +240,7 @@ struct LodBuildOutput {
   std::vector<float> positions, covariances, colors, alphas, sh;
   std::vector<LodNode> layout;
 };
+constexpr uint32_t kMaxLodBuildLeaves = 0x7fffffffu;
 cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out);
 
 }  // namespace sk

@@ -1,7 +1,9 @@
 // The LOD tree build on the GPU: the same octree as the host builder (host/lod_build.cpp, which
-// restates splat-core/src/lod/LodTree.cpp:17-344), built breadth first, one kernel per level.
+// restates splat-core/src/lod/LodTree.cpp:17-344), built breadth first, one round of kernels
+// (classify, scan, expand) per tree level.
 //
-//   1. per leaf: semi-axes and merge area (ellipsoid surface), node size, Morton key (63 bits);
+//   1. per leaf: semi-axes and merge area (ellipsoid surface), node size, Morton key (3 bits per
+//      octree level, at most 63);
 //   2. the leaves sorted by (key, index): two stable 32-bit radix argsorts (low word, then high);
 //   3. level by level from the root: every element of the level is a sorted range. A range of one
 //      splat is that leaf; a range of at most clusterLeaves splats, at the depth limit, or of one
@@ -379,7 +381,7 @@ struct Arena {
 cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out) {
   const uint32_t n = in.count;
   const size_t shStride = in.shStride;
-  if (n == 0) return cudaErrorInvalidValue;
+  if (n == 0 || n > kMaxLodBuildLeaves) return cudaErrorInvalidValue;  // 2n - 1 nodes fit 32 bits
   cudaStream_t s = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e != cudaSuccess) return e;

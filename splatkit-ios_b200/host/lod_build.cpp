@@ -503,6 +503,7 @@ sk_status sk_build_lod_tree_device(const sk_cloud_view* cloud, const float* boun
       !cloud->colors || !cloud->alphas)
     return SK_E_INVALID;
   *out = nullptr;
+  if (cloud->count > sk::kMaxLodBuildLeaves) return SK_E_LIMIT;
   const int degree = cloud->sh ? std::max(0, std::min(cloud->sh_degree, 3)) : 0;
   const auto shStride = static_cast<uint32_t>(((degree + 1) * (degree + 1) - 1) * 3);
   auto tree = std::make_unique<sk::BuiltTree>();

@@ -159,3 +159,15 @@ def test_frame_entry_points_reject_a_missing_context():
                                      ctypes.byref(t)) == sk.SK_E_INVALID
     assert lib.sk_wait_capture(None, 1) == sk.SK_E_INVALID
     assert lib.sk_draw(None, None) == sk.SK_E_INVALID
+
+
+def test_device_tree_build_rejects_bad_clouds_before_device_work():
+    import ctypes
+    lib = sk.library()
+    handle = ctypes.c_void_p()
+    assert lib.sk_build_lod_tree_device(None, None, None, 0, 0, 1, ctypes.byref(handle)) == sk.SK_E_INVALID
+    empty = sk.Cloud(np.zeros((0, 3), np.float32), np.zeros((0, 6), np.float32),
+                     np.zeros((0, 3), np.float32), np.zeros(0, np.float32))
+    v = empty.view()
+    assert lib.sk_build_lod_tree_device(ctypes.byref(v), None, None, 0, 0, 1, ctypes.byref(handle)) == sk.SK_E_INVALID
+    assert not handle.value
