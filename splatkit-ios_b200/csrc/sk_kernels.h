@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "sk_layout.h"
@@ -235,10 +237,34 @@ struct LodBuildInput {
   uint32_t depth;          // 1 .. 21
   uint32_t clusterLeaves;  // >= 2
 };
+// Host arrays that a resize leaves uninitialised (a default-initialising allocator): the arrays
+// of a built tree are filled by a bulk copy or a parallel loop right after they are sized, so
+// zeroing hundreds of MB on one thread first would only add time.
+template <typename T>
+struct UninitAllocator : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = UninitAllocator<U>;
+  };
+  UninitAllocator() = default;
+  template <typename U>
+  UninitAllocator(const UninitAllocator<U>&) noexcept {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+template <typename T>
+using HostArray = std::vector<T, UninitAllocator<T>>;
+
 struct LodBuildOutput {
   uint32_t count = 0;
-  std::vector<float> positions, covariances, colors, alphas, sh;
-  std::vector<LodNode> layout;
+  HostArray<float> positions, covariances, colors, alphas, sh;
+  HostArray<LodNode> layout;
 };
 constexpr uint32_t kMaxLodBuildLeaves = 0x7fffffffu;
 cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out);

@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <thread>
 #include <vector>
 
 #include "sk_device.cuh"
@@ -363,6 +364,24 @@ __global__ void mergeKernel(uint32_t m, uint32_t levelBase, const uint32_t* chil
 
 uint32_t blocksOf(uint32_t n, uint32_t per) { return std::max(1u, (n + per - 1) / per); }
 
+// Touches every 4 KB page of a fresh host array on several threads, so the page faults of the
+// download that follows are taken in parallel instead of inside the driver's one copy thread.
+void touchPages(void* data, size_t bytes) {
+  constexpr size_t kPage = 4096;
+  auto* bytesOf = static_cast<volatile unsigned char*>(data);
+  const size_t pages = (bytes + kPage - 1) / kPage;
+  const unsigned workers = static_cast<unsigned>(
+      std::min<size_t>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())),
+                       std::max<size_t>(pages / 4096, 1)));
+  auto touch = [=](size_t first, size_t last) {
+    for (size_t pg = first; pg < last; ++pg) bytesOf[pg * kPage] = 0;
+  };
+  if (workers <= 1) return touch(0, pages);
+  std::vector<std::thread> pool;
+  for (unsigned w = 0; w < workers; ++w) pool.emplace_back(touch, pages * w / workers, pages * (w + 1) / workers);
+  for (auto& t : pool) t.join();
+}
+
 // Carves one device allocation into the build's arrays (256-byte aligned); a first pass with no
 // base only sums the sizes.
 struct Arena {
@@ -538,7 +557,10 @@ cudaError_t buildLodTreeGpu(const LodBuildInput& in, LodBuildOutput& out) {
       out.sh.resize(size_t{total} * shStride);
       out.layout.resize(total);
       auto down = [&](void* dst, const void* src, size_t bytes) {
-        if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && bytes) {
+          touchPages(dst, bytes);
+          e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        }
       };
       down(out.positions.data(), nodes.positions, size_t{total} * 12);
       down(out.covariances.data(), nodes.covariances, size_t{total} * 24);

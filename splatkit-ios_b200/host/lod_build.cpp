@@ -300,8 +300,8 @@ void parallelSort(std::vector<Cell>& cells) {
 // The tree of a build: the nodes as a cloud in layout order plus the layout (and optionally
 // the selection data), owned until sk_lod_tree_free.
 struct BuiltTree {
-  std::vector<float> positions, covariances, colors, alphas, sh;
-  std::vector<LodNode> layout;
+  HostArray<float> positions, covariances, colors, alphas, sh;
+  HostArray<LodNode> layout;
   std::vector<LodCluster> clusters;
   std::vector<uint32_t> leaves;
   uint32_t leafCount = 0;
