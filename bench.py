@@ -504,6 +504,28 @@ def measure_batch(renderer):
 
 
 # ---- LOD walk: 6M leaves in 2000 clusters, 300 frames at 1920x1080 ----------------------------
+def tree_build_call_seconds(sk, cloud, entry, reps=3):
+    """Median time of one C-ABI tree build (with selection data) through `entry`, the tree freed
+    after each call: the build alone, without the Python copies of the result."""
+    import ctypes
+    lib = sk.library()
+    view = cloud.view()
+    lo = np.ascontiguousarray(cloud.bounds_min, np.float32)
+    hi = np.ascontiguousarray(cloud.bounds_max, np.float32)
+    f32p = ctypes.POINTER(ctypes.c_float)
+    times = []
+    for _ in range(reps):
+        handle = ctypes.c_void_p()
+        t0 = time.perf_counter()
+        st = getattr(lib, entry)(ctypes.byref(view), lo.ctypes.data_as(f32p), hi.ctypes.data_as(f32p),
+                                 0, 0, 1, ctypes.byref(handle))
+        times.append(time.perf_counter() - t0)
+        if st != sk.SK_OK:
+            raise sk.SplatError(st, entry)
+        lib.sk_lod_tree_free(handle)
+    return float(np.median(times))
+
+
 def measure_lod_walk():
     """The LOD workload: 2000 anisotropic clusters of 3000 splats (centres in a 200 m box), the
     tree built on the host by the project's builder (the reference builder's tree), cut at
@@ -526,6 +548,8 @@ def measure_lod_walk():
     same_layout = bool(np.array_equal(device_tree.layout["child_start"], tree.layout["child_start"]) and
                        np.array_equal(device_tree.layout["child_count"], tree.layout["child_count"]))
     del device_tree
+    c_call_s = {"host": tree_build_call_seconds(sk, cloud, "sk_build_lod_tree"),
+                "device": tree_build_call_seconds(sk, cloud, "sk_build_lod_tree_device")}
     r = sk.Renderer(WIDTH, HEIGHT, image_format=sk.FORMAT_RGBA8, time_stages=True)
     r.apply_render_policy(sk.Policy(lod_error_pixels=1.5, sort_depth_bits=16))
     r.upload_lod_world(tree, 0, 4_000_000)
@@ -554,8 +578,10 @@ def measure_lod_walk():
             "mean_select_ms": float(np.mean(select_ms)), "mean_cut_splats": float(np.mean(cut)),
             "tree_build_s": build_s, "tree_build_device_s": device_build_s,
             "tree_build_device_same_layout": same_layout,
-            "tree_build_how": "Python build_lod_tree with selection data, node arrays copied out; host: "
-                              "all host threads; device: keys, sort, levels and merges on the GPU"}
+            "tree_build_c_call_s": c_call_s,
+            "tree_build_how": "tree_build_s / tree_build_device_s: Python build_lod_tree with selection data, "
+                              "node arrays copied out; tree_build_c_call_s: the C-ABI call alone (median of 3); "
+                              "host: all host threads; device: keys, sort, levels and merges on the GPU"}
 
 
 # ---- serving: Poisson requests over 8 resident scenes -----------------------------------------
