@@ -906,12 +906,34 @@ def lodsplat_decode(data: bytes, max_sh_degree: int = 3) -> LodTree:
     return LodTree(cloud, layout, hd["leaf_count"], clusters, leaves)
 
 
-def _copy_out(ptr, dtype, shape):
+class _TreeMemory:
+    """Owns one built tree (sk_lod_tree); the numpy views of its arrays keep it alive, and it is
+    freed with the last of them."""
+
+    def __init__(self, lib, handle: int):
+        self._free = lib.sk_lod_tree_free
+        self.handle = handle
+
+    def __del__(self):
+        if self.handle:
+            self._free(self.handle)
+            self.handle = None
+
+
+class _TreeArray:
+    """The array interface of one array of a built tree (no copy), holding the tree."""
+
+    def __init__(self, owner: _TreeMemory, ptr: int, dtype, shape):
+        self._owner = owner
+        dt = np.dtype(dtype)
+        self.__array_interface__ = {"version": 3, "data": (ptr, False), "shape": tuple(shape),
+                                    "typestr": dt.str, "descr": dt.descr}
+
+
+def _tree_array(owner: _TreeMemory, ptr, dtype, shape) -> Optional[np.ndarray]:
     if not ptr or int(np.prod(shape)) == 0:
         return None
-    count = int(np.prod(shape)) * np.dtype(dtype).itemsize
-    raw = (ctypes.c_char * count).from_address(ptr)  # a view; the one copy is below
-    return np.frombuffer(raw, dtype).reshape(shape).copy()
+    return np.asarray(_TreeArray(owner, int(ptr), dtype, shape))
 
 
 def build_lod_tree(cloud: Cloud, bounds_min=None, bounds_max=None, octree_depth: int = 0,
@@ -931,26 +953,24 @@ def build_lod_tree(cloud: Cloud, bounds_min=None, bounds_max=None, octree_depth:
                              1 if selection else 0, ctypes.byref(handle))
     if st != SK_OK:
         raise SplatError(st, entry)
-    try:
-        t = _LodView()
-        bmin, bmax = np.zeros(3, np.float32), np.zeros(3, np.float32)
-        lib.sk_lod_tree_view(handle, ctypes.byref(t), _ptr(bmin), _ptr(bmax))
-        n, d = t.node_count, t.nodes.sh_degree
-        coeffs = 3 * ((d + 1) ** 2 - 1)
-        nodes = Cloud(_copy_out(ctypes.cast(t.nodes.positions, ctypes.c_void_p).value, np.float32, (n, 3)),
-                      _copy_out(ctypes.cast(t.nodes.covariances, ctypes.c_void_p).value, np.float32, (n, 6)),
-                      _copy_out(ctypes.cast(t.nodes.colors, ctypes.c_void_p).value, np.float32, (n, 3)),
-                      _copy_out(ctypes.cast(t.nodes.alphas, ctypes.c_void_p).value, np.float32, (n,)),
-                      sh_degree=d,
-                      sh=_copy_out(ctypes.cast(t.nodes.sh, ctypes.c_void_p).value, np.float32, (n, coeffs))
-                      if coeffs else None,
-                      bounds_min=bmin, bounds_max=bmax)
-        layout = _copy_out(t.layout, LOD_NODE_DTYPE, (n,))
-        clusters = _copy_out(t.clusters, LOD_CLUSTER_DTYPE, (t.cluster_count,))
-        leaves = _copy_out(ctypes.cast(t.leaves, ctypes.c_void_p).value, np.uint32, (t.leaf_ref_count,))
-        return LodTree(nodes, layout, t.leaf_count, clusters, leaves)
-    finally:
-        lib.sk_lod_tree_free(handle)
+    owner = _TreeMemory(lib, handle.value)  # the arrays below are views of the tree's own memory
+    t = _LodView()
+    bmin, bmax = np.zeros(3, np.float32), np.zeros(3, np.float32)
+    lib.sk_lod_tree_view(handle, ctypes.byref(t), _ptr(bmin), _ptr(bmax))
+    n, d = t.node_count, t.nodes.sh_degree
+    coeffs = 3 * ((d + 1) ** 2 - 1)
+    addr = lambda p: ctypes.cast(p, ctypes.c_void_p).value
+    nodes = Cloud(_tree_array(owner, addr(t.nodes.positions), np.float32, (n, 3)),
+                  _tree_array(owner, addr(t.nodes.covariances), np.float32, (n, 6)),
+                  _tree_array(owner, addr(t.nodes.colors), np.float32, (n, 3)),
+                  _tree_array(owner, addr(t.nodes.alphas), np.float32, (n,)),
+                  sh_degree=d,
+                  sh=_tree_array(owner, addr(t.nodes.sh), np.float32, (n, coeffs)) if coeffs else None,
+                  bounds_min=bmin, bounds_max=bmax)
+    layout = _tree_array(owner, t.layout, LOD_NODE_DTYPE, (n,))
+    clusters = _tree_array(owner, t.clusters, LOD_CLUSTER_DTYPE, (t.cluster_count,))
+    leaves = _tree_array(owner, addr(t.leaves), np.uint32, (t.leaf_ref_count,))
+    return LodTree(nodes, layout, t.leaf_count, clusters, leaves)
 
 
 def write_lodsplat(tree: LodTree, path):
