@@ -579,8 +579,8 @@ def measure_lod_walk():
             "tree_build_s": build_s, "tree_build_device_s": device_build_s,
             "tree_build_device_same_layout": same_layout,
             "tree_build_c_call_s": c_call_s,
-            "tree_build_how": "tree_build_s / tree_build_device_s: Python build_lod_tree with selection data, "
-                              "node arrays copied out; tree_build_c_call_s: the C-ABI call alone (median of 3); "
+            "tree_build_how": "tree_build_s / tree_build_device_s: Python build_lod_tree with selection data "
+                              "(node arrays returned as views); tree_build_c_call_s: the C-ABI call alone (median of 3); "
                               "host: all host threads; device: keys, sort, levels and merges on the GPU"}
 
 
