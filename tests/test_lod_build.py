@@ -65,3 +65,21 @@ def test_written_file_is_the_reference_file(reference, tmp_path, selection):
     with pytest.raises(sk.SplatError):  # never overwrites
         sk.write_lodsplat(ours, tmp_path / "ours.lodsplat")
     assert ref["depth"] == sk.lodsplat_header((tmp_path / "ours.lodsplat").read_bytes())["depth"]
+
+
+def test_tree_arrays_are_views_that_keep_the_tree_alive():
+    import gc
+    import weakref
+    cloud = CLOUDS["random_sh2"]()
+    tree = sk.build_lod_tree(cloud)
+    expected = tree.nodes.positions.copy()
+    owner = weakref.ref(tree.layout.base._owner)
+    assert not tree.nodes.positions.flags["OWNDATA"]
+    positions = tree.nodes.positions
+    del tree
+    gc.collect()
+    assert owner() is not None  # one view is left
+    np.testing.assert_array_equal(positions, expected)
+    del positions
+    gc.collect()
+    assert owner() is None  # freed with the last view
