@@ -158,15 +158,109 @@ void packSh(const CloudRef& c, int degree, size_t offset, size_t count, uint32_t
   });
 }
 
+namespace {
+
+// Runs fn(w, begin, end) over `workers` contiguous slices of [0, n) on host threads.
+template <typename Fn>
+void forSlices(size_t n, int workers, Fn fn) {
+  if (workers <= 1) return fn(0, size_t{0}, n);
+  std::vector<std::thread> pool;
+  for (int w = 0; w < workers; ++w) pool.emplace_back(fn, w, n * w / workers, n * (w + 1) / workers);
+  for (auto& t : pool) t.join();
+}
+
+// The clusters and leaf references of a breadth-first layout without walking it: the
+// breadth-first order of the interior nodes alone is their layout order, so cluster k is the
+// k-th interior node, its interior children are the clusters ranked from the interior count
+// before its first child, and its leaf children follow the leaf children of clusters 0..k-1.
+// The same arrays the walk below gives. Returns false, leaving both empty, when the child ranges
+// are not consecutive from node 1 on or a node comes before its parent (not a breadth-first
+// layout).
+bool selectionFromBreadthFirst(const LodNode* layout, uint32_t nodeCount, int threads,
+                               std::vector<LodCluster>& clusters, std::vector<uint32_t>& leaves) {
+  const int workers = std::max(1, std::min<int>(threads, static_cast<int>(nodeCount / 65536)));
+  // per slice: interiors and children, then each node's exclusive counts
+  std::vector<uint64_t> sliceInteriors(workers + 1, 0), sliceChildren(workers + 1, 0);
+  forSlices(nodeCount, workers, [&](int w, size_t b, size_t e) {
+    uint64_t interiors = 0, children = 0;
+    for (size_t i = b; i < e; ++i) {
+      interiors += layout[i].childCount != 0;
+      children += layout[i].childCount;
+    }
+    sliceInteriors[w + 1] = interiors;
+    sliceChildren[w + 1] = children;
+  });
+  for (int w = 0; w < workers; ++w) {
+    sliceInteriors[w + 1] += sliceInteriors[w];
+    sliceChildren[w + 1] += sliceChildren[w];
+  }
+  if (sliceChildren[workers] + 1 != nodeCount) return false;
+  // each node's interior rank, and the interior nodes in order
+  const auto count = static_cast<uint32_t>(sliceInteriors[workers]);
+  std::vector<uint32_t> rank(size_t{nodeCount} + 1), nodeOf(count);
+  std::vector<char> bad(workers, 0);
+  forSlices(nodeCount, workers, [&](int w, size_t b, size_t e) {
+    uint64_t interiors = sliceInteriors[w], next = 1 + sliceChildren[w];
+    for (size_t i = b; i < e; ++i) {
+      rank[i] = static_cast<uint32_t>(interiors);
+      if (i >= next) bad[w] = 1;  // every node after the one whose range holds it
+      if (layout[i].childCount) {
+        if (layout[i].childStart != next) bad[w] = 1;
+        nodeOf[interiors++] = static_cast<uint32_t>(i);
+        next += layout[i].childCount;
+      }
+    }
+  });
+  rank[nodeCount] = count;
+  for (char b : bad)
+    if (b) return false;
+  // each cluster's children and leaves
+  clusters.assign(count, LodCluster{});
+  const int clusterWorkers = std::max(1, std::min<int>(threads, static_cast<int>(count / 16384)));
+  std::vector<uint64_t> sliceLeaves(clusterWorkers + 1, 0);
+  forSlices(count, clusterWorkers, [&](int w, size_t b, size_t e) {
+    uint64_t leafTotal = 0;
+    for (size_t k = b; k < e; ++k) {
+      const LodNode& node = layout[nodeOf[k]];
+      LodCluster& c = clusters[k];
+      c.node = nodeOf[k];
+      c.childStart = rank[node.childStart];
+      c.childCount = rank[node.childStart + node.childCount] - c.childStart;
+      c.leafCount = node.childCount - c.childCount;
+      leafTotal += c.leafCount;
+    }
+    sliceLeaves[w + 1] = leafTotal;
+  });
+  for (int w = 0; w < clusterWorkers; ++w) sliceLeaves[w + 1] += sliceLeaves[w];
+  leaves.resize(sliceLeaves[clusterWorkers]);
+  forSlices(count, clusterWorkers, [&](int w, size_t b, size_t e) {
+    auto at = static_cast<uint32_t>(sliceLeaves[w]);
+    for (size_t k = b; k < e; ++k) {
+      LodCluster& c = clusters[k];
+      c.leafStart = at;
+      const LodNode& node = layout[c.node];
+      for (uint32_t j = 0; j < node.childCount; ++j)
+        if (layout[node.childStart + j].childCount == 0) leaves[at++] = node.childStart + j;
+    }
+  });
+  return true;
+}
+
+}  // namespace
+
 void buildSelection(const CloudRef& cloud, const LodNode* layout, uint32_t nodeCount,
                     std::vector<LodCluster>& clusters, std::vector<uint32_t>& leaves) {
   clusters.clear();
   leaves.clear();
   if (nodeCount == 0) return;
-  // Interiors in BFS order; each cluster's interior children are consecutive clusters.
+  const int threads = std::max(1, static_cast<int>(std::thread::hardware_concurrency()));
+  const bool laidOut = layout[0].childCount != 0 &&
+                       selectionFromBreadthFirst(layout, nodeCount, threads, clusters, leaves);
+  // Otherwise interiors in BFS order by a walk; each cluster's interior children are
+  // consecutive clusters.
   std::vector<uint32_t> order{0};
-  clusters.resize(1);
-  for (size_t head = 0; head < order.size(); ++head) {
+  if (!laidOut) clusters.resize(1);
+  for (size_t head = 0; !laidOut && head < order.size(); ++head) {
     const uint32_t index = order[head];
     const LodNode& node = layout[index];
     LodCluster cluster{};
@@ -246,7 +340,6 @@ void buildSelection(const CloudRef& cloud, const LodNode* layout, uint32_t nodeC
     cluster.error = std::max(cluster.error, cluster.radius * peakDifference);
     cluster.colorVariance = weightSum > 0 ? weightedVariance / weightSum : 0;
   };
-  const int threads = std::max(1, static_cast<int>(std::thread::hardware_concurrency()));
   for (size_t l = levelStart.size() - 1; l-- > 0;) {
     const size_t first = levelStart[l], count = levelStart[l + 1] - first;
     const int workers = std::max(1, std::min<int>(threads, static_cast<int>(count / 2048)));

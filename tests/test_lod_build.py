@@ -83,3 +83,13 @@ def test_tree_arrays_are_views_that_keep_the_tree_alive():
     del positions
     gc.collect()
     assert owner() is None  # freed with the last view
+
+
+def test_selection_of_a_tree_split_over_host_threads_is_the_reference_selection(reference):
+    """~540k nodes: the selection structure is ranked in several host-thread slices of the layout
+    (and of the clusters); clusters, leaf references and layout stay the reference's bit for bit."""
+    cloud = bounded(synthetic.clustered_cloud(160, 3000, seed=15, half_extent=60.0))
+    ours = sk.build_lod_tree(cloud)
+    ref = reference.build_lod_tree(cloud)
+    assert len(ours.layout) > 4 * 65536 and len(ours.clusters) > 2 * 16384
+    assert_tree_equals(ours, ref)
