@@ -280,14 +280,15 @@ void buildSelection(const CloudRef& cloud, const LodNode* layout, uint32_t nodeC
   }
   // Bottom up: bounds, merge error, colour variance, opacity, leaf count. A cluster reads only
   // its own node and its children, which sit in the next BFS level, so the levels are done
-  // deepest first and the clusters of one level on all host threads.
-  std::vector<uint32_t> level(clusters.size(), 0);
+  // deepest first and the clusters of one level on all host threads. Clusters are in BFS order,
+  // so the level after [a, b) is [b, the end of cluster b-1's children).
   std::vector<size_t> levelStart{0};
-  for (size_t k = 0; k < clusters.size(); ++k) {
-    if (k > 0 && level[k] != level[k - 1]) levelStart.push_back(k);
-    for (uint32_t j = 0; j < clusters[k].childCount; ++j) level[clusters[k].childStart + j] = level[k] + 1;
+  for (size_t a = 0, b = clusters.empty() ? 0 : 1; a < b;) {
+    levelStart.push_back(b);
+    const size_t next = size_t{clusters[b - 1].childStart} + clusters[b - 1].childCount;
+    a = b;
+    b = std::max(next, b);
   }
-  levelStart.push_back(clusters.size());
   auto finish = [&](size_t k) {
     LodCluster& cluster = clusters[k];
     const float* parent = &cloud.positions[cluster.node * 3];
