@@ -75,8 +75,8 @@ std::array<float, 3> semiAxes(const float* cov) {
 // merge weight per unit opacity, so each node's eigenvalues are taken once. Node k's children
 // are kids[kidStart[k] .. kidStart[k] + kidCount[k]).
 struct Store {
-  std::vector<float> positions, covariances, colors, alphas, sh, size, area;
-  std::vector<uint32_t> kidStart, kidCount, kids;
+  HostArray<float> positions, covariances, colors, alphas, sh, size, area;
+  HostArray<uint32_t> kidStart, kidCount, kids;
   size_t count() const { return alphas.size(); }
 };
 
@@ -357,18 +357,32 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
   const size_t shStride = static_cast<size_t>((degree + 1) * (degree + 1) - 1) * 3;
   auto tree = std::make_unique<sk::BuiltTree>();
   sk::treeBounds(cloud, bounds_min, bounds_max, *tree);
-  // The leaves, with their size and merge area (eigenvalues per leaf, in parallel).
+  // The leaves, with their size and merge area (eigenvalues per leaf), copied and solved on all
+  // host threads. The arrays are reserved for every node of the tree (at most 2n - 1), so the
+  // interior nodes appended later never move the leaves; untouched capacity costs no memory.
   sk::Store store;
-  store.positions.assign(cloud->positions, cloud->positions + n * 3);
-  store.covariances.assign(cloud->covariances, cloud->covariances + n * 6);
-  store.colors.assign(cloud->colors, cloud->colors + n * 3);
-  store.alphas.assign(cloud->alphas, cloud->alphas + n);
-  if (shStride) store.sh.assign(cloud->sh, cloud->sh + n * shStride);
-  store.size.resize(n);
-  store.area.resize(n);
-  store.kidStart.assign(n, 0);
-  store.kidCount.assign(n, 0);
+  const size_t nodeBound = 2 * n;
+  auto sized = [&](auto& array, size_t perNode) {
+    array.reserve(nodeBound * perNode);
+    array.resize(n * perNode);
+  };
+  sized(store.positions, 3);
+  sized(store.covariances, 6);
+  sized(store.colors, 3);
+  sized(store.alphas, 1);
+  sized(store.sh, shStride);
+  sized(store.size, 1);
+  sized(store.area, 1);
+  sized(store.kidStart, 1);
+  sized(store.kidCount, 1);
   sk::parallelFor(n, [&](size_t i) {
+    std::copy_n(cloud->positions + i * 3, 3, &store.positions[i * 3]);
+    std::copy_n(cloud->covariances + i * 6, 6, &store.covariances[i * 6]);
+    std::copy_n(cloud->colors + i * 3, 3, &store.colors[i * 3]);
+    store.alphas[i] = cloud->alphas[i];
+    if (shStride) std::copy_n(cloud->sh + i * shStride, shStride, &store.sh[i * shStride]);
+    store.kidStart[i] = 0;
+    store.kidCount[i] = 0;
     const auto axes = sk::semiAxes(&store.covariances[i * 6]);
     store.size[i] = 2.0f * axes[0];
     store.area[i] = sk::ellipsoidArea(axes);
@@ -461,18 +475,41 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
   const uint32_t root = builder.build(0, sorted.size(), 0);
   auto& nodes = store;
   // LodTree.cpp:209-243: breadth-first layout, attributes copied in layout order
+  // The queue of the breadth-first walk, one level at a time on all host threads: a level's
+  // nodes count their children, the counts are summed per slice, and each node writes its
+  // children at the queue's tail plus the children of the nodes before it in the level (the
+  // position a sequential walk gives them).
   const size_t total = nodes.count();
-  std::vector<uint32_t> order;
-  order.reserve(total);
-  tree->layout.assign(total, sk::LodNode{});
-  order.push_back(root);
-  for (size_t head = 0; head < order.size(); ++head) {
-    const uint32_t id = order[head];
-    const uint32_t first = nodes.kidStart[id], count = nodes.kidCount[id];
-    tree->layout[head].childStart = static_cast<uint32_t>(order.size());
-    tree->layout[head].childCount = count;
-    order.insert(order.end(), nodes.kids.begin() + first, nodes.kids.begin() + first + count);
+  sk::HostArray<uint32_t> order(total);  // node ids in layout order; every node appears once
+  tree->layout.resize(total);            // every field is written below
+  order[0] = root;
+  size_t levelEnd = 1;
+  for (size_t levelBegin = 0; levelBegin < levelEnd;) {
+    const size_t width = levelEnd - levelBegin;
+    const int slices = static_cast<int>(std::min<size_t>(workers, std::max<size_t>(width / 16384, 1)));
+    std::vector<uint64_t> sliceKids(slices + 1, 0);
+    sk::host::forSlices(width, slices, [&](int w, size_t b, size_t e) {
+      uint64_t kids = 0;
+      for (size_t k = levelBegin + b; k < levelBegin + e; ++k) kids += nodes.kidCount[order[k]];
+      sliceKids[w + 1] = kids;
+    });
+    for (int w = 0; w < slices; ++w) sliceKids[w + 1] += sliceKids[w];
+    if (sliceKids[slices] > total - levelEnd) return SK_E_INVALID;  // a node reached twice: not a tree
+    sk::host::forSlices(width, slices, [&](int w, size_t b, size_t e) {
+      size_t tail = levelEnd + sliceKids[w];
+      for (size_t head = levelBegin + b; head < levelBegin + e; ++head) {
+        const uint32_t id = order[head];
+        const uint32_t first = nodes.kidStart[id], count = nodes.kidCount[id];
+        tree->layout[head].childStart = static_cast<uint32_t>(tail);
+        tree->layout[head].childCount = count;
+        std::copy_n(nodes.kids.data() + first, count, order.data() + tail);
+        tail += count;
+      }
+    });
+    levelBegin = levelEnd;
+    levelEnd += sliceKids[slices];
   }
+  if (levelEnd != total) return SK_E_INVALID;  // a node the walk never reached
   tree->positions.resize(total * 3);
   tree->covariances.resize(total * 6);
   tree->colors.resize(total * 3);

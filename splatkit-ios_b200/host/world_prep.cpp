@@ -160,15 +160,6 @@ void packSh(const CloudRef& c, int degree, size_t offset, size_t count, uint32_t
 
 namespace {
 
-// Runs fn(w, begin, end) over `workers` contiguous slices of [0, n) on host threads.
-template <typename Fn>
-void forSlices(size_t n, int workers, Fn fn) {
-  if (workers <= 1) return fn(0, size_t{0}, n);
-  std::vector<std::thread> pool;
-  for (int w = 0; w < workers; ++w) pool.emplace_back(fn, w, n * w / workers, n * (w + 1) / workers);
-  for (auto& t : pool) t.join();
-}
-
 // The clusters and leaf references of a breadth-first layout without walking it: the
 // breadth-first order of the interior nodes alone is their layout order, so cluster k is the
 // k-th interior node, its interior children are the clusters ranked from the interior count

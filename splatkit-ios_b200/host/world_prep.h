@@ -10,6 +10,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -31,6 +32,15 @@ uint16_t floatToHalf(float v);
 float halfToFloat(uint16_t h);
 
 // Harmonics coefficients per channel, bands 1..degree.
+// Runs fn(w, begin, end) over `workers` contiguous slices of [0, n) on host threads.
+template <typename Fn>
+void forSlices(size_t n, int workers, Fn fn) {
+  if (workers <= 1) return fn(0, size_t{0}, n);
+  std::vector<std::thread> pool;
+  for (int w = 0; w < workers; ++w) pool.emplace_back(fn, w, n * w / workers, n * (w + 1) / workers);
+  for (auto& t : pool) t.join();
+}
+
 inline uint32_t shCoefficients(int degree) {
   return degree <= 0 ? 0u : static_cast<uint32_t>((degree + 1) * (degree + 1) - 1);
 }
