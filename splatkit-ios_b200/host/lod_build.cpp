@@ -199,7 +199,7 @@ struct Task {
 // instead of building it (the subtrees were built beforehand, in parallel).
 struct OctreeBuilder {
   Nodes& nodes;
-  const std::vector<Cell>& sorted;
+  const HostArray<Cell>& sorted;
   size_t clusterLeaves;
   uint32_t depth;
   const std::vector<Task>* tasks = nullptr;
@@ -271,7 +271,7 @@ void parallelFor(size_t n, Fn fn) {
 
 // Sorts by (key, node): slices sorted in parallel, then merged pairwise. The order is total, so
 // the result is the one sequential sort gives.
-void parallelSort(std::vector<Cell>& cells) {
+void sliceMergeSort(HostArray<Cell>& cells) {
   auto less = [](const Cell& a, const Cell& b) { return a.key == b.key ? a.node < b.node : a.key < b.key; };
   const size_t n = cells.size();
   const unsigned slices = static_cast<unsigned>(std::min<size_t>(workerCount(), std::max<size_t>(n / 65536, 1)));
@@ -293,6 +293,53 @@ void parallelSort(std::vector<Cell>& cells) {
     }
     for (auto& t : pool) t.join();
   }
+}
+
+// Sorts by (key, node), keys below 2^keyBits: the cells are scattered by their top 12 key bits
+// into buckets in key order (counts per thread, then a parallel scatter), and the buckets are
+// sorted on all threads. The order is total, so the result is the one sequential sort gives. A
+// bucket holding more than half the cells (a tiny or degenerate cloud) falls back to
+// sliceMergeSort.
+void parallelSort(HostArray<Cell>& cells, uint32_t keyBits) {
+  constexpr uint32_t kBucketBits = 12, kBuckets = 1u << kBucketBits;
+  const size_t n = cells.size();
+  const unsigned workers = static_cast<unsigned>(std::min<size_t>(workerCount(), std::max<size_t>(n / 65536, 1)));
+  if (workers <= 1) return sliceMergeSort(cells);
+  const uint32_t shift = keyBits > kBucketBits ? keyBits - kBucketBits : 0;
+  auto bucketOf = [shift](const Cell& c) { return static_cast<uint32_t>(std::min<uint64_t>(c.key >> shift, kBuckets - 1)); };
+  std::vector<uint32_t> counts(size_t{workers} * kBuckets, 0);
+  host::forSlices(n, static_cast<int>(workers), [&](int w, size_t b, size_t e) {
+    uint32_t* mine = &counts[size_t(w) * kBuckets];
+    for (size_t i = b; i < e; ++i) ++mine[bucketOf(cells[i])];
+  });
+  // bucket starts, then each slice's first position in every bucket (bucket-major order)
+  std::vector<size_t> bucketStart(kBuckets + 1, 0), at(size_t{workers} * kBuckets);
+  size_t largest = 0;
+  for (uint32_t k = 0; k < kBuckets; ++k) {
+    size_t run = bucketStart[k];
+    for (unsigned w = 0; w < workers; ++w) {
+      at[size_t(w) * kBuckets + k] = run;
+      run += counts[size_t(w) * kBuckets + k];
+    }
+    bucketStart[k + 1] = run;
+    largest = std::max(largest, run - bucketStart[k]);
+  }
+  if (largest > n / 2) return sliceMergeSort(cells);
+  HostArray<Cell> out(n);  // every element is written by the scatter
+  host::forSlices(n, static_cast<int>(workers), [&](int w, size_t b, size_t e) {
+    size_t* mine = &at[size_t(w) * kBuckets];
+    for (size_t i = b; i < e; ++i) out[mine[bucketOf(cells[i])]++] = cells[i];
+  });
+  auto less = [](const Cell& a, const Cell& b) { return a.key == b.key ? a.node < b.node : a.key < b.key; };
+  std::atomic<uint32_t> next{0};
+  std::vector<std::thread> pool;
+  for (unsigned w = 0; w < workers; ++w)
+    pool.emplace_back([&] {
+      for (uint32_t k; (k = next.fetch_add(1)) < kBuckets;)
+        std::sort(out.begin() + bucketStart[k], out.begin() + bucketStart[k + 1], less);
+    });
+  for (auto& t : pool) t.join();
+  cells.swap(out);
 }
 
 }  // namespace
@@ -392,12 +439,12 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
                                     sk::kMaxOctreeDepth);
   float extent = 1e-6f;
   for (int c = 0; c < 3; ++c) extent = std::max(extent, tree->boundsMax[c] - tree->boundsMin[c]);
-  std::vector<sk::Cell> sorted(n);
+  sk::HostArray<sk::Cell> sorted(n);  // every element is written below
   sk::parallelFor(n, [&](size_t i) {
     sorted[i] = {sk::mortonKey(&store.positions[i * 3], tree->boundsMin, extent, depth),
                  static_cast<uint32_t>(i)};
   });
-  sk::parallelSort(sorted);
+  sk::parallelSort(sorted, 3 * depth);
   const size_t clusterLeaves = std::max<size_t>(cluster_leaves == 0 ? 32 : cluster_leaves, 2);
   // Subtrees of at most `limit` leaves are built in parallel, each worker into a store of its
   // own (node ids from n on); the nodes above them are built last. Node creation order differs
