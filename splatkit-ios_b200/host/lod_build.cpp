@@ -496,24 +496,43 @@ sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
     store.kidCount.reserve(nodesTotal);
     store.kids.reserve(kids + n + 64 * clusterLeaves);
   }
-  for (unsigned w = 0; w < workers; ++w) {
+  // Each worker's block has a known place (nodes from n + offset[w], child ids from
+  // kidOffset[w]), so the blocks are copied in parallel, one thread per worker store.
+  std::vector<size_t> kidOffset(workers + 1, store.kids.size());
+  for (unsigned w = 0; w < workers; ++w) kidOffset[w + 1] = kidOffset[w] + own[w].kids.size();
+  const size_t merged = n + offset[workers - 1] + own[workers - 1].count();
+  store.positions.resize(merged * 3);
+  store.covariances.resize(merged * 6);
+  store.colors.resize(merged * 3);
+  store.alphas.resize(merged);
+  store.sh.resize(merged * shStride);
+  store.size.resize(merged);
+  store.area.resize(merged);
+  store.kidStart.resize(merged);
+  store.kidCount.resize(merged);
+  store.kids.resize(kidOffset[workers]);
+  sk::host::forSlices(workers, static_cast<int>(workers), [&](int w, size_t, size_t) {
     sk::Store& o = own[w];
-    for (uint32_t& id : o.kids)
-      if (id >= leafCount) id += offset[w];
-    const auto kidBase = static_cast<uint32_t>(store.kids.size());
-    for (uint32_t& k : o.kidStart) k += kidBase;
-    store.kids.insert(store.kids.end(), o.kids.begin(), o.kids.end());
-    store.kidStart.insert(store.kidStart.end(), o.kidStart.begin(), o.kidStart.end());
-    store.kidCount.insert(store.kidCount.end(), o.kidCount.begin(), o.kidCount.end());
-    store.positions.insert(store.positions.end(), o.positions.begin(), o.positions.end());
-    store.covariances.insert(store.covariances.end(), o.covariances.begin(), o.covariances.end());
-    store.colors.insert(store.colors.end(), o.colors.begin(), o.colors.end());
-    store.alphas.insert(store.alphas.end(), o.alphas.begin(), o.alphas.end());
-    store.sh.insert(store.sh.end(), o.sh.begin(), o.sh.end());
-    store.size.insert(store.size.end(), o.size.begin(), o.size.end());
-    store.area.insert(store.area.end(), o.area.begin(), o.area.end());
+    const size_t base = n + offset[w], m = o.count();
+    const uint32_t shift = offset[w];
+    const auto kidBase = static_cast<uint32_t>(kidOffset[w]);
+    for (size_t j = 0; j < o.kids.size(); ++j) {
+      const uint32_t id = o.kids[j];
+      store.kids[kidOffset[w] + j] = id >= leafCount ? id + shift : id;
+    }
+    for (size_t j = 0; j < m; ++j) {
+      store.kidStart[base + j] = o.kidStart[j] + kidBase;
+      store.kidCount[base + j] = o.kidCount[j];
+    }
+    std::copy_n(o.positions.data(), m * 3, store.positions.data() + base * 3);
+    std::copy_n(o.covariances.data(), m * 6, store.covariances.data() + base * 6);
+    std::copy_n(o.colors.data(), m * 3, store.colors.data() + base * 3);
+    std::copy_n(o.alphas.data(), m, store.alphas.data() + base);
+    if (shStride) std::copy_n(o.sh.data(), m * shStride, store.sh.data() + base * shStride);
+    std::copy_n(o.size.data(), m, store.size.data() + base);
+    std::copy_n(o.area.data(), m, store.area.data() + base);
     o = sk::Store{};
-  }
+  });
   for (auto& t : tasks)
     if (t.root >= leafCount) t.root += offset[t.worker];
   std::sort(tasks.begin(), tasks.end(), [](const sk::Task& a, const sk::Task& b) { return a.begin < b.begin; });
