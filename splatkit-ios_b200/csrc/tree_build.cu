@@ -1,5 +1,5 @@
 // The LOD tree build on the GPU: the same octree as the host builder (host/lod_build.cpp, which
-// restates splat-core/src/lod/LodTree.cpp:17-344), built breadth first, one round of kernels
+// restates splat-core/src/lod/LodTree.cpp:17-344), built breadth first, one set of kernels
 // (classify, scan, expand) per tree level.
 //
 //   1. per leaf: semi-axes and merge area (ellipsoid surface), node size, Morton key (3 bits per
