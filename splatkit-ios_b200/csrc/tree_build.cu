@@ -140,6 +140,22 @@ __device__ uint32_t lowerBound(const uint32_t* lo, const uint32_t* hi, uint32_t 
   return b;
 }
 
+// Calls run(start, stop) for each non-empty run of one octant digit at the element's level, in
+// key order (at most 8: the element's keys share every digit above it).
+template <typename Run>
+__device__ __forceinline__ void forOctantRuns(const Element& el, const uint32_t* keyLo,
+                                              const uint32_t* keyHi, uint32_t depth, Run run) {
+  const uint32_t shift = 3 * (depth - el.level - 1);
+  const uint64_t prefix = sortedKey(keyLo, keyHi, el.begin) >> shift;
+  const uint64_t last = sortedKey(keyLo, keyHi, el.end - 1) >> shift;
+  uint32_t start = el.begin;
+  for (uint64_t d = prefix; d <= last; ++d) {
+    const uint32_t stop = lowerBound(keyLo, keyHi, start, el.end, shift, d + 1);
+    if (stop > start) run(start, stop);
+    start = stop;
+  }
+}
+
 // 3a. the kind of every element of the level and its number of children (LodTree.cpp:182-196)
 __global__ void classifyKernel(uint32_t m, Element* elements, const uint32_t* keyLo,
                                const uint32_t* keyHi, uint32_t clusterLeaves, uint32_t depth,
@@ -163,15 +179,7 @@ __global__ void classifyKernel(uint32_t m, Element* elements, const uint32_t* ke
       const uint32_t hb = 63 - __clzll(static_cast<long long>(x));
       el.level = max(el.level, depth - 1 - hb / 3);
       el.kind = 2;
-      const uint32_t shift = 3 * (depth - el.level - 1);
-      const uint64_t prefix = sortedKey(keyLo, keyHi, el.begin) >> shift;
-      const uint64_t last = sortedKey(keyLo, keyHi, el.end - 1) >> shift;
-      uint32_t start = el.begin;
-      for (uint64_t d = prefix; d <= last; ++d) {  // at most 8 octants
-        const uint32_t stop = lowerBound(keyLo, keyHi, start, el.end, shift, d + 1);
-        count += stop > start ? 1u : 0u;
-        start = stop;
-      }
+      forOctantRuns(el, keyLo, keyHi, depth, [&](uint32_t, uint32_t) { ++count; });
     }
   }
   elements[i] = el;
@@ -195,15 +203,9 @@ __global__ void expandKernel(uint32_t m, const Element* elements, const uint32_t
     for (uint32_t j = el.begin; j < el.end; ++j)
       next[out + written++] = Element{j, j + 1, el.level + 1, 0};
   } else if (el.kind == 2) {
-    const uint32_t shift = 3 * (depth - el.level - 1);
-    const uint64_t prefix = sortedKey(keyLo, keyHi, el.begin) >> shift;
-    const uint64_t last = sortedKey(keyLo, keyHi, el.end - 1) >> shift;
-    uint32_t start = el.begin;
-    for (uint64_t d = prefix; d <= last; ++d) {
-      const uint32_t stop = lowerBound(keyLo, keyHi, start, el.end, shift, d + 1);
-      if (stop > start) next[out + written++] = Element{start, stop, el.level + 1, 0};
-      start = stop;
-    }
+    forOctantRuns(el, keyLo, keyHi, depth, [&](uint32_t start, uint32_t stop) {
+      next[out + written++] = Element{start, stop, el.level + 1, 0};
+    });
   }
   childCount[node] = written;
 }
