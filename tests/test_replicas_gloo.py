@@ -1,6 +1,7 @@
 """The bench's replica plumbing on two CPU ranks (gloo): the job time is the slowest rank's, the
 aggregate rate counts every rank's frames, ranks draw different frames, and the reference arm
-runs on rank 0 only. Frames are independent, so there is no data-path collective to test."""
+runs on rank 0 only, and the HBM peak is read from the peaks file when it is there. Frames are
+independent, so there is no data-path collective to test."""
 from __future__ import annotations
 
 import os
@@ -66,3 +67,15 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     args = bench.parse(["--impl", "reference", "--steps", "1", "--warmup", "0"])
     bench.run_reference(args)  # returns at once on a non-zero rank
     assert capsys.readouterr().out == ""
+
+
+def test_peaks_file_is_read_when_present_and_readable(tmp_path, monkeypatch):
+    import bench
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    assert bench.measured_peaks() == (6650.0, "fallback")  # absent
+    for text, expected in [('{"hbm_gbs": 7100.5}', (7100.5, "measured")),
+                           ('{"hbm_gbs": {"value": 7000}}', (7000.0, "measured")),
+                           ('{"bf16_tflops": 1590}', (6650.0, "fallback")),
+                           ("not json", (6650.0, "fallback"))]:
+        (tmp_path / "MEASURED_PEAKS.json").write_text(text)
+        assert bench.measured_peaks() == expected
