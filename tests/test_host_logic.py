@@ -171,3 +171,10 @@ def test_device_tree_build_rejects_bad_clouds_before_device_work():
     v = empty.view()
     assert lib.sk_build_lod_tree_device(ctypes.byref(v), None, None, 0, 0, 1, ctypes.byref(handle)) == sk.SK_E_INVALID
     assert not handle.value
+    # a count above 2^31 - 1 (2n - 1 nodes would not fit 32 bits) is refused before any array is read
+    one = sk.Cloud(np.zeros((1, 3), np.float32), np.zeros((1, 6), np.float32),
+                   np.zeros((1, 3), np.float32), np.zeros(1, np.float32))
+    v = one.view()
+    v.count = 0x80000000
+    assert lib.sk_build_lod_tree_device(ctypes.byref(v), None, None, 0, 0, 1, ctypes.byref(handle)) == sk.SK_E_LIMIT
+    assert not handle.value
