@@ -26,7 +26,20 @@ CLOUDS = {
     "clustered": lambda: bounded(synthetic.clustered_cloud(12, 400, seed=13, half_extent=30.0)),
     # enough leaves for hundreds of subtrees built on separate threads
     "clustered_80k": lambda: bounded(synthetic.clustered_cloud(80, 1000, seed=14, half_extent=50.0)),
+    # edge cases: a root that is its one splat, a root of two, every splat repeated (one Morton
+    # key per run, merged at the depth limit). Bounds given, as a loader gives them: the
+    # reference builder takes the cloud's bounds as they are (zero when unset), this build the
+    # positions' own box when none are passed.
+    "one": lambda: bounded(synthetic.random_cloud(1, seed=24, sh_degree=2)),
+    "two": lambda: bounded(synthetic.random_cloud(2, seed=25, sh_degree=2)),
+    "duplicates": lambda: bounded(repeated(synthetic.random_cloud(300, seed=23, sh_degree=1, half_extent=3.0), 40)),
 }
+
+
+def repeated(cloud, copies: int):
+    rep = lambda a: None if a is None else np.repeat(np.asarray(a), copies, axis=0)
+    return sk.Cloud(rep(cloud.positions), rep(cloud.covariances), rep(cloud.colors), rep(cloud.alphas),
+                    sh_degree=cloud.sh_degree, sh=rep(cloud.sh))
 
 
 def assert_tree_equals(ours: sk.LodTree, ref: dict):
