@@ -227,7 +227,7 @@ def aggregate_rate(steps, world, seconds):
 
 
 def cpu_frame(cloud_packed, sh_packed, sh_stride, view, proj, eye, bits, threads, width=WIDTH,
-              height=HEIGHT, pixel_rows=None):
+              height=HEIGHT):
     from oracle.oracle import Oracle
 
     o = Oracle()
@@ -244,19 +244,34 @@ def cpu_frame(cloud_packed, sh_packed, sh_stride, view, proj, eye, bits, threads
             "visible": len(keys)}
 
 
+def reference_packed_scene():
+    """The workload's cloud packed by the reference's own packSplatRange / packShRange
+    (splatkit-engine/src/rendering/GpuLayout.cpp:92-137, compiled into oracle/_ref): the CPU arm
+    maps no library of the product. None when oracle/_ref is not built."""
+    from oracle import oracle as oracle_mod
+    from splatkit_b200 import synthetic  # numpy only: the product library stays unloaded
+
+    if not oracle_mod.reference_available():
+        return None
+    ref = oracle_mod.Reference()
+    cloud = synthetic.random_cloud(SPLATS, seed=0, sh_degree=SH_DEGREE)
+    return ref.pack_splats(cloud), ref.pack_sh(cloud, SH_DEGREE), ref.sh_stride(SH_DEGREE)
+
+
 def run_reference(args):
-    """The reference arm: the oracle port of the frame path on the host cores."""
+    """The reference arm: the reference has no CPU frame path (its frame runs only as Metal
+    shaders), so it is the oracle port of the frame path (cull, LSD radix sort, FP32 composite) on
+    every host core, fed the reference's own packed records."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import splatkit_b200 as sk
-    from splatkit_b200 import synthetic
-
     threads = os.cpu_count() or 1
-    cloud = synthetic.random_cloud(SPLATS, seed=0, sh_degree=SH_DEGREE)
-    packed = sk.pack_splats(cloud)
-    sh = sk.pack_sh(cloud, SH_DEGREE)
-    stride = sk.sh_device_stride(SH_DEGREE)
+    scene = reference_packed_scene()
+    if scene is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's C++ "
+                          "packing) is not built"}), flush=True)
+        return
+    packed, sh, stride = scene
     for step in range(args.warmup):
         cpu_frame(packed, sh, stride, *frame_inputs(step), args.bits, threads)
     times = []
@@ -272,7 +287,8 @@ def run_reference(args):
             "config": workload_config(args.bits),
             "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
                              "sample": "every step is one full frame of the workload: cull "
-                                       "1M splats, LSD radix sort, FP32 composite 1920x1080"},
+                                       "1M splats (records packed by the reference's C++), LSD "
+                                       "radix sort, FP32 composite 1920x1080"},
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -348,6 +364,12 @@ def run_ours(args):
             stages[k].append(s[k])
         stage_stats.append(s)  # fragments are counted in this pass only
     torch.cuda.synchronize()
+
+    # the other depth-key width on the same frames (the workload compares 16- and 32-bit keys):
+    # frame-timed, then per stage; the headline line's own width is restored afterwards
+    other_bits = 32 if args.bits == 16 else 16
+    other = time_key_width(r, frame, flush, other_bits, min(args.steps, 100), args.warmup)
+    r.apply_render_policy(sk.Policy(sort_depth_bits=args.bits))
 
     # e2e: the public calls with every frame's image landing in pinned host memory, host-timed.
     # captureNextFrame form: each step requests the capture of its frame and draws it, then waits
@@ -430,8 +452,9 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "gpu_launches": launches_per_frame * args.steps,
         }
+        line[f"bits{other_bits}"] = other
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(cloud, args.bits)
+            line["cpu_baseline"] = cpu_baseline(args.bits, args.warmup - 1, args.warmup)
         if world == 1 and not args.no_batch and args.bits == 16:
             line["batch64"] = measure_batch(r)
         if world == 1 and not args.no_lod and args.bits == 16:
@@ -442,6 +465,47 @@ def run_ours(args):
     r.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def time_key_width(r, frame, flush, bits, steps, warmup):
+    """Frames/s, per-stage device ms and GB/s, and sort keys/s of the workload with `bits`-bit
+    depth keys: the same orbit frames as the headline loop, L2 flushed before each."""
+    import torch
+
+    import splatkit_b200 as sk
+
+    r.apply_render_policy(sk.Policy(sort_depth_bits=bits))
+    for step in range(3):
+        frame(step)
+        r.wait_idle()
+    stage_names = ("cull_ms", "sort_ms", "bin_ms", "composite_ms")
+    per_frame, stats_list, stages = [], [], {k: [] for k in stage_names}
+    for timing in ("frame", True):
+        r.set_timing(timing)
+        for step in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            frame(warmup + step)
+            r.wait_idle()
+            s = r.stats()
+            if timing == "frame":
+                per_frame.append(s["gpu_ms"])
+                stats_list.append(s)
+            else:
+                for k in stage_names:
+                    stages[k].append(s[k])
+    mean = {k: float(np.mean(v)) for k, v in stages.items()}
+    bytes_by_stage = {k: float(np.mean([stage_bytes(s, bits)[k] for s in stats_list]))
+                      for k in ("cull", "sort", "bin", "composite")}
+    visible = float(np.mean([s["draw_count"] for s in stats_list]))
+    return {"key_bits": bits, "steps": steps, "value": steps / (sum(per_frame) / 1000.0),
+            "unit": "frames/s", "ms_per_step": float(np.mean(per_frame)), "stages_ms": mean,
+            "stage_gbs": {k: bytes_by_stage[k] / (mean[k + "_ms"] / 1000.0) / 1e9
+                          for k in bytes_by_stage},
+            "sort_algorithmic_bytes": bytes_by_stage["sort"],
+            "sort_keys_per_s": visible / (mean["sort_ms"] / 1000.0),
+            "how": "device time per frame (frame events), then a second pass with per-stage "
+                   "events; L2 flushed before every frame"}
 
 
 # ---- batched multi-view: 64 views of the 1M SH3 scene, mixed resolutions ----------------------
@@ -687,17 +751,26 @@ def measure_serve():
     return out
 
 
-def cpu_baseline(cloud, bits):
-    import splatkit_b200 as sk
+CPU_BASELINE_FRAMES = 8
 
+
+def cpu_baseline(bits, warmup, first):
+    """The oracle port of the frame path on every host core over the same orbit frames the timed
+    loop starts with (one untimed warm-up frame first), records packed by the reference's C++."""
     threads = os.cpu_count() or 1
-    packed = sk.pack_splats(cloud)
-    sh = sk.pack_sh(cloud, SH_DEGREE)
-    t = cpu_frame(packed, sh, sk.sh_device_stride(SH_DEGREE), *frame_inputs(0), bits, threads)
-    return {"value": 1.0 / t["total"], "unit": "frames/s", "cores": threads, "kind": "port",
-            "sample": "one full frame of the workload (cull 1M, radix sort, FP32 composite "
-                      "1920x1080) on the oracle port",
-            "stages_s": {k: t[k] for k in ("cull", "sort", "composite")}}
+    scene = reference_packed_scene()
+    if scene is None:
+        return None
+    packed, sh, stride = scene
+    cpu_frame(packed, sh, stride, *frame_inputs(warmup), bits, threads)
+    runs = [cpu_frame(packed, sh, stride, *frame_inputs(first + k), bits, threads)
+            for k in range(CPU_BASELINE_FRAMES)]
+    total = sum(t["total"] for t in runs)
+    return {"value": CPU_BASELINE_FRAMES / total, "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"{CPU_BASELINE_FRAMES} full frames of the workload (orbit frames {first}.."
+                      f"{first + CPU_BASELINE_FRAMES - 1}: cull 1M, LSD radix sort, FP32 composite "
+                      "1920x1080) on the oracle port, after one warm-up frame",
+            "stages_s": {k: float(np.mean([t[k] for t in runs])) for k in ("cull", "sort", "composite")}}
 
 
 def main():

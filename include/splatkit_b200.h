@@ -452,9 +452,11 @@ sk_status sk_radix_argsort_device(const uint32_t* d_keys, const uint32_t* d_coun
  *
  * Setup: the first call on each device (the device current on the calling thread) looks up the
  * array's device address, which may load the module; make that first call before any stream
- * capture. There is one array per device: calls on one device whose sorts may overlap in time
- * (different streams without an event between them, or several host threads) race on it and
- * give wrong orders. Keep them ordered on one stream. */
+ * capture. The address is kept for the life of the process: after cudaDeviceReset (or anything
+ * else that destroys the device's primary context) the module reloads elsewhere, so do not call
+ * this entry point on that device again. There is one array per device: calls on one device
+ * whose sorts may overlap in time (different streams without an event between them, or several
+ * host threads) race on it and give wrong orders. Keep them ordered on one stream. */
 #define SK_NOALLOC_SORT_MAX_KEYS (1u << 20)
 sk_status sk_radix_argsort_noalloc(const uint32_t* d_keys, const uint32_t* d_count,
                                    uint32_t capacity, int32_t bits, uint32_t* d_order,

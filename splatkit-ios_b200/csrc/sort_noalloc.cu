@@ -33,7 +33,10 @@ constexpr size_t kNoAllocScratchBytes = 3 * roundUp256(kNoAllocKeys * 4) + round
 // Zero when the module loads. The histogram accumulators and the tile counters must be zero
 // when a sort starts: every completed sort leaves them at zero, and each call clears them again
 // before it sorts (two small memsets on the caller's stream), so a sort cut short by an error
-// cannot poison the next one. The status words need no clearing: each call uses new epochs.
+// cannot poison the next one. The status words need no clearing while the 30-bit epochs are
+// new: each call takes four (one per pass). When the epoch counter wraps, after 2^28 calls, the
+// call that wraps it zeroes the status words first (a flag of 0 never matches), so a word left
+// by a sort 2^28 calls earlier cannot pass for one of the new epochs.
 static __device__ __align__(256) unsigned char gSortScratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
@@ -80,10 +83,14 @@ extern "C" sk_status sk_radix_argsort_noalloc(const uint32_t* d_keys, const uint
   // The layout of the largest sort, whatever the capacity: the status words then always sit
   // at the same place and the region never holds anything but status words.
   sk::sortBindWorkspace(a, scratch, SK_NOALLOC_SORT_MAX_KEYS);
-  a.epoch = sk::gEpoch.fetch_add(4) & 0x3fffffffu;
+  const uint32_t raw = sk::gEpoch.fetch_add(4);
+  a.epoch = raw & 0x3fffffffu;
   a.error = d_error;
   const auto s = static_cast<cudaStream_t>(stream);
-  cudaError_t e = sk::sortResetWorkspace(a, s);
+  cudaError_t e = cudaSuccess;
+  if (a.epoch == 1 && raw != 1)  // the counter wrapped: the old status words could match again
+    e = cudaMemsetAsync(a.status, 0, static_cast<size_t>(a.statusTiles) * 256 * 8, s);
+  if (e == cudaSuccess) e = sk::sortResetWorkspace(a, s);
   if (e == cudaSuccess) e = sk::launchSort(a, s);
   return e == cudaSuccess ? SK_OK : SK_E_DEVICE;
 }

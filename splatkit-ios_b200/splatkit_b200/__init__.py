@@ -921,12 +921,13 @@ class _TreeMemory:
 
 
 class _TreeArray:
-    """The array interface of one array of a built tree (no copy), holding the tree."""
+    """The array interface of one array of a built tree (no copy, read only: the memory belongs
+    to the library), holding the tree."""
 
     def __init__(self, owner: _TreeMemory, ptr: int, dtype, shape):
         self._owner = owner
         dt = np.dtype(dtype)
-        self.__array_interface__ = {"version": 3, "data": (ptr, False), "shape": tuple(shape),
+        self.__array_interface__ = {"version": 3, "data": (ptr, True), "shape": tuple(shape),
                                     "typestr": dt.str, "descr": dt.descr}
 
 
@@ -956,7 +957,9 @@ def build_lod_tree(cloud: Cloud, bounds_min=None, bounds_max=None, octree_depth:
     owner = _TreeMemory(lib, handle.value)  # the arrays below are views of the tree's own memory
     t = _LodView()
     bmin, bmax = np.zeros(3, np.float32), np.zeros(3, np.float32)
-    lib.sk_lod_tree_view(handle, ctypes.byref(t), _ptr(bmin), _ptr(bmax))
+    st = lib.sk_lod_tree_view(handle, ctypes.byref(t), _ptr(bmin), _ptr(bmax))
+    if st != SK_OK:
+        raise SplatError(st, "sk_lod_tree_view")
     n, d = t.node_count, t.nodes.sh_degree
     coeffs = 3 * ((d + 1) ** 2 - 1)
     addr = lambda p: ctypes.cast(p, ctypes.c_void_p).value

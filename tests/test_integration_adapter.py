@@ -2,7 +2,8 @@
 the reference engine's own SplatRenderer interface and links against the library (CPU only).
 
 It needs the reference's headers, which exist only where the reference tree is mounted; the test
-skips elsewhere. SPLATKIT_REFERENCE overrides the location of its `packages` directory.
+skips elsewhere. The location of its `packages` directory is SPLATKIT_REFERENCE, else the one the
+oracle build recorded in oracle/_ref/reference_packages when it compiled the reference's C++.
 """
 from __future__ import annotations
 
@@ -14,7 +15,17 @@ from pathlib import Path
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
-PACKAGES = Path(os.environ.get("SPLATKIT_REFERENCE", "/root/reference/packages"))
+
+
+def _packages() -> Path:
+    env = os.environ.get("SPLATKIT_REFERENCE")
+    if env:
+        return Path(env)
+    recorded = ROOT / "oracle" / "_ref" / "reference_packages"
+    return Path(recorded.read_text().strip()) if recorded.exists() else Path("reference-not-found")
+
+
+PACKAGES = _packages()
 LIB_DIR = ROOT / "splatkit-ios_b200"
 
 MAIN = r"""
