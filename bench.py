@@ -601,7 +601,7 @@ def tree_build_call_seconds(sk, cloud, entry, reps=3):
 
 def measure_lod_walk():
     """The LOD workload: 2000 anisotropic clusters of 3000 splats (centres in a 200 m box), the
-    tree built on the host by the project's builder (the reference builder's tree), cut at
+    tree built on the GPU by the project's builder (the reference builder's layout), cut at
     1.5 px along a 300-frame walk (eye height 1.7 m, x from -90 to 90 m, looking +x)."""
     import splatkit_b200 as sk
     from splatkit_b200 import camera as skcam
@@ -610,19 +610,11 @@ def measure_lod_walk():
     cloud = synthetic.clustered_cloud(2000, 3000, seed=0)
     pos = np.asarray(cloud.positions, np.float32)
     cloud.bounds_min, cloud.bounds_max = pos.min(axis=0), pos.max(axis=0)
+    sk.build_lod_tree(synthetic.random_cloud(1000, seed=1))  # loads the module
     t0 = time.perf_counter()
     tree = sk.build_lod_tree(cloud)
     build_s = time.perf_counter() - t0
-    # the same tree built on the GPU (after one small build that loads the module)
-    sk.build_lod_tree(synthetic.random_cloud(1000, seed=1), device=True)
-    t0 = time.perf_counter()
-    device_tree = sk.build_lod_tree(cloud, device=True)
-    device_build_s = time.perf_counter() - t0
-    same_layout = bool(np.array_equal(device_tree.layout["child_start"], tree.layout["child_start"]) and
-                       np.array_equal(device_tree.layout["child_count"], tree.layout["child_count"]))
-    del device_tree
-    c_call_s = {"host": tree_build_call_seconds(sk, cloud, "sk_build_lod_tree"),
-                "device": tree_build_call_seconds(sk, cloud, "sk_build_lod_tree_device")}
+    c_call_s = tree_build_call_seconds(sk, cloud, "sk_build_lod_tree_device")
     r = sk.Renderer(WIDTH, HEIGHT, image_format=sk.FORMAT_RGBA8, time_stages=True)
     r.apply_render_policy(sk.Policy(lod_error_pixels=1.5, sort_depth_bits=16))
     r.upload_lod_world(tree, 0, 4_000_000)
@@ -645,16 +637,15 @@ def measure_lod_walk():
         select_ms.append(s["select_ms"])
         cut.append(s["selected_count"])
     r.close()
-    return {"workload": "6M leaves (2000 clusters x 3000), host-built tree of "
+    return {"workload": "6M leaves (2000 clusters x 3000), GPU-built tree of "
                         f"{len(tree.layout)} nodes, 1.5 px cut, 300-frame walk at 1920x1080",
             "frames_per_s": 300 / (sum(gpu_ms) / 1000.0), "mean_gpu_ms": float(np.mean(gpu_ms)),
             "mean_select_ms": float(np.mean(select_ms)), "mean_cut_splats": float(np.mean(cut)),
-            "tree_build_s": build_s, "tree_build_device_s": device_build_s,
-            "tree_build_device_same_layout": same_layout,
-            "tree_build_c_call_s": c_call_s,
-            "tree_build_how": "tree_build_s / tree_build_device_s: Python build_lod_tree with selection data "
-                              "(node arrays returned as views); tree_build_c_call_s: the C-ABI call alone (median of 3); "
-                              "host: all host threads; device: keys, sort, levels and merges on the GPU"}
+            "tree_build_s": build_s, "tree_build_c_call_s": c_call_s,
+            "tree_build_how": "tree_build_s: Python build_lod_tree with selection data (node arrays "
+                              "returned as views); tree_build_c_call_s: the C-ABI call alone "
+                              "(median of 3): keys, sort, levels and merges on the GPU, selection "
+                              "data on the host threads"}
 
 
 # ---- serving: Poisson requests over 8 resident scenes -----------------------------------------

@@ -214,21 +214,17 @@ sk_status sk_upload_lodsplat_file(sk_context* ctx, const char* path, int32_t max
 sk_status sk_write_lodsplat(const sk_lod_view* tree, const float* bounds_min,
                             const float* bounds_max, const char* path);
 
-/* buildLodTree (splat-core/src/lod/LodTree.cpp:308-330, LodTree.h:58-75) on the host: the
- * cloud's splats become the leaves of an octree of merged nodes, laid out breadth first; the
- * same tree bit for bit as the reference's builder given the same bounds. octree_depth 0: 21;
+/* buildLodTree (splat-core/src/lod/LodTree.cpp:308-330, LodTree.h:58-75), built on the GPU
+ * (current device): the cloud's splats become the leaves of an octree of merged nodes, laid out
+ * breadth first. Morton keys and a radix sort on the device, then the octree one pass per level,
+ * and the merges deepest level first. Given the same bounds the layout (child ranges) is the
+ * reference builder's exactly; node attributes agree to a few ulp (the eigen-solve's acos/cos and
+ * the surface formula's powf are the device's, not the host library's). octree_depth 0: 21;
  * cluster_leaves 0: 32. bounds NULL: the positions' own box. build_selection: also build the
  * selection data (buildLodSelectionData). The tree is read through sk_lod_tree_view (pointers
- * valid until sk_lod_tree_free). */
+ * valid until sk_lod_tree_free). SK_E_LIMIT above 2^31 - 1 splats; SK_E_DEVICE on a CUDA error
+ * (out of device memory included). */
 typedef struct sk_lod_tree sk_lod_tree;
-sk_status sk_build_lod_tree(const sk_cloud_view* cloud, const float* bounds_min,
-                            const float* bounds_max, uint32_t octree_depth, uint32_t cluster_leaves,
-                            int32_t build_selection, sk_lod_tree** out);
-/* The same tree built on the GPU (current device): Morton keys and a radix sort on the device,
- * then the octree breadth first, one pass per level, and the merges deepest level first. The
- * layout (child ranges) is sk_build_lod_tree's exactly; node attributes agree to a few ulp (the
- * eigen-solve's acos/cos and the surface formula's powf are the device's). SK_E_LIMIT above
- * 2^31 - 1 splats; SK_E_DEVICE on a CUDA error (out of device memory included). */
 sk_status sk_build_lod_tree_device(const sk_cloud_view* cloud, const float* bounds_min,
                                    const float* bounds_max, uint32_t octree_depth,
                                    uint32_t cluster_leaves, int32_t build_selection,
@@ -472,8 +468,8 @@ sk_status sk_pack_splats(const sk_cloud_view* cloud, uint32_t offset, uint32_t c
 /* packShRange float16 (GpuLayout.cpp:92-113) at `stride` words per splat (>= packed stride). */
 sk_status sk_pack_sh(const sk_cloud_view* cloud, int32_t degree, uint32_t offset, uint32_t count,
                      uint32_t* out, uint32_t stride);
-/* buildLodSelectionData (splat-core/src/lod/LodSelection.cpp:47-133). Pass null outputs to
- * learn the counts first. */
+/* buildLodSelectionData (splat-core/src/lod/LodSelection.cpp:47-133) of a breadth-first laid-out
+ * tree (SK_E_INVALID otherwise). Pass null outputs to learn the counts first. */
 sk_status sk_build_lod_selection(const sk_lod_view* tree, sk_lod_cluster* clusters,
                                  uint32_t cluster_capacity, uint32_t* cluster_count,
                                  uint32_t* leaves, uint32_t leaf_capacity, uint32_t* leaf_count);

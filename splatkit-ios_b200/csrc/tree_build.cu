@@ -1,6 +1,6 @@
-// The LOD tree build on the GPU: the same octree as the host builder (host/lod_build.cpp, which
-// restates splat-core/src/lod/LodTree.cpp:17-344), built breadth first, one set of kernels
-// (classify, scan, expand) per tree level.
+// The LOD tree build on the GPU: the octree of the reference's builder
+// (splat-core/src/lod/LodTree.cpp:17-344), built breadth first, one set of kernels (classify,
+// scan, expand) per tree level.
 //
 //   1. per leaf: semi-axes and merge area (ellipsoid surface), node size, Morton key (3 bits per
 //      octree level, at most 63);
@@ -12,12 +12,14 @@
 //      children are the next level's elements in order, so the levels laid out one after the
 //      other are the reference's breadth-first layout (LodTree.cpp:209-243);
 //   4. deepest level first, each node merges its children's weighted moments (LodTree.cpp:47-102)
-//      in the host's order of float operations.
-// The structure (child ranges) is the host builder's exactly. The attributes match to a few ulp:
-// the eigen-solve's acos and cos and the surface formula's powf are CUDA's, not the host
-// library's.
+//      in the reference's order of float operations.
+// The structure (child ranges) is the reference builder's exactly. The attributes match to a few
+// ulp: the eigen-solve's acos and cos are CUDA's double functions, and the surface formula's
+// and the opacity reach's float pow and log are taken in double and rounded once (the correctly
+// rounded value, which the host library's powf and logf give for all but a small share of
+// inputs), so they are not always the host library's.
 //
-// Built with -fmad=false: every product and sum rounds on its own, as in the host build.
+// Built with -fmad=false: every product and sum rounds on its own, as in the reference build.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,8 +35,9 @@ namespace {
 
 constexpr uint32_t kThreads = 256;
 
-// SymmetricEigen.cpp:8-41 (the host restatement's steps): eigenvalues of the symmetric 3x3
-// (upper triangle), descending, as floats.
+// SymmetricEigen.cpp:8-41 (the trigonometric solution of the characteristic cubic, in the
+// reference's double operations): eigenvalues of the symmetric 3x3 (upper triangle),
+// descending, as floats.
 __device__ void eigenvaluesDesc(const float* u, float* out) {
   const double xx = u[0], xy = u[1], xz = u[2], yy = u[3], yz = u[4], zz = u[5];
   const double p1 = xy * xy + xz * xz + yz * yz;
@@ -68,16 +71,27 @@ __device__ void semiAxes(const float* cov, float* s) {
   for (int i = 0; i < 3; ++i) s[i] = sqrtf(fmaxf(e[i], 0.0f));
 }
 
+// x^y of floats as the nearest float to the exact power: the double power has far more bits
+// than the float result needs, so rounding it once gives the correctly rounded float except on
+// inputs within a double ulp of a rounding boundary.
+__device__ __forceinline__ float powRounded(float x, float y) {
+  return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y)));
+}
+__device__ __forceinline__ float logRounded(float x) {
+  return static_cast<float>(log(static_cast<double>(x)));
+}
+
 // LodTree.cpp:17-22 (Knud Thomsen's ellipsoid surface approximation)
 __device__ float ellipsoidArea(const float* s) {
   constexpr float kP = 1.6075f;
-  const float sum = powf(s[0] * s[1], kP) + powf(s[0] * s[2], kP) + powf(s[1] * s[2], kP);
-  return 4.0f * 3.14159274f * powf(sum / 3.0f, 1.0f / kP);
+  const float sum = powRounded(s[0] * s[1], kP) + powRounded(s[0] * s[2], kP) +
+                    powRounded(s[1] * s[2], kP);
+  return 4.0f * 3.14159274f * powRounded(sum / 3.0f, 1.0f / kP);
 }
 
 // LodTree.cpp:27-29
 __device__ float lodOpacityReach(float alpha) {
-  return alpha > 1.0f ? sqrtf(1.0f + 2.71828175f * logf(alpha)) : 1.0f;
+  return alpha > 1.0f ? sqrtf(1.0f + 2.71828175f * logRounded(alpha)) : 1.0f;
 }
 
 __device__ __forceinline__ uint64_t spreadBits3(uint32_t v) {

@@ -804,8 +804,9 @@ sk_status sk_upload_lod_world(sk_context* handle, const sk_lod_view* tree, int32
     sk::host::CloudRef ref{tree->nodes.positions, tree->nodes.covariances, tree->nodes.colors,
                            tree->nodes.alphas, tree->nodes.sh, tree->nodes.count,
                            tree->nodes.sh ? std::max(0, std::min(tree->nodes.sh_degree, 3)) : 0};
-    sk::host::buildSelection(ref, reinterpret_cast<const sk::LodNode*>(tree->layout),
-                             tree->node_count, clusters, leaves);
+    if (!sk::host::buildSelection(ref, reinterpret_cast<const sk::LodNode*>(tree->layout),
+                                  tree->node_count, clusters, leaves))
+      return ctx->fail(SK_E_INVALID, "invalid LOD hierarchy: the layout is not breadth first");
   }
   sk::World fresh;
   st = ctx->uploadCloud(tree->nodes, maxSh, fresh);

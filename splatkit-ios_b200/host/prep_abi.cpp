@@ -43,8 +43,10 @@ sk_status sk_build_lod_selection(const sk_lod_view* tree, sk_lod_cluster* cluste
   if (!tree || !tree->layout || tree->nodes.count != tree->node_count) return SK_E_INVALID;
   std::vector<sk::LodCluster> c;
   std::vector<uint32_t> l;
-  sk::host::buildSelection(cloudRef(tree->nodes), reinterpret_cast<const sk::LodNode*>(tree->layout),
-                           tree->node_count, c, l);
+  if (!sk::host::buildSelection(cloudRef(tree->nodes),
+                                reinterpret_cast<const sk::LodNode*>(tree->layout), tree->node_count,
+                                c, l))
+    return SK_E_INVALID;  // not a breadth-first layout
   if (clusterCount) *clusterCount = static_cast<uint32_t>(c.size());
   if (leafCount) *leafCount = static_cast<uint32_t>(l.size());
   if (clusters) std::memcpy(clusters, c.data(), std::min<size_t>(c.size(), clusterCapacity) * 64);

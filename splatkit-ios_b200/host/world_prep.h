@@ -3,7 +3,7 @@
 // bytes:
 //   packSplatRange / packShRange   splatkit-engine/src/rendering/GpuLayout.cpp:92-137
 //   toHalf                         splat-core/include/splat/math/Half.h:12-38
-//   buildLodSelectionData          splat-core/src/lod/LodSelection.cpp:47-133
+//   buildLodSelectionData          splat-core/src/lod/LodSelection.cpp:47-133 (selection.cpp)
 //   LOD depth (validateLodTree)    splat-core/src/lod/LodFile.cpp:103-141,336-344
 //   LodThreshold                   splatkit-engine/include/splatkit/rendering/LodThreshold.h:12-43
 //   gpuWorldBytes                  splatkit-engine/src/rendering/GpuLayout.cpp:14-20,72-77
@@ -52,8 +52,9 @@ void packSplats(const CloudRef& cloud, size_t offset, size_t count, GpuSplat* ou
 void packSh(const CloudRef& cloud, int degree, size_t offset, size_t count, uint32_t* out,
             uint32_t stride, int threads);
 
-// The interior-cluster records and leaf references of a BFS-laid-out tree.
-void buildSelection(const CloudRef& nodes, const LodNode* layout, uint32_t nodeCount,
+// The interior-cluster records and leaf references of a BFS-laid-out tree (selection.cpp). False,
+// with both left empty, when the layout is not breadth first.
+bool buildSelection(const CloudRef& nodes, const LodNode* layout, uint32_t nodeCount,
                     std::vector<LodCluster>& clusters, std::vector<uint32_t>& leaves);
 
 // Checks the BFS topology and the leaf count; returns the deepest node depth (the number of

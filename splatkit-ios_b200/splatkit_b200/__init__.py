@@ -249,8 +249,6 @@ _SIGNATURES = {
                                             ctypes.c_uint32]),
     "sk_upload_lodsplat_file": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_uint32]),
     "sk_write_lodsplat": (ctypes.c_int32, [ctypes.POINTER(_LodView), _f32p, _f32p, ctypes.c_char_p]),
-    "sk_build_lod_tree": (ctypes.c_int32, [ctypes.POINTER(_Cloud), _f32p, _f32p, ctypes.c_uint32, ctypes.c_uint32,
-                                           ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     "sk_build_lod_tree_device": (ctypes.c_int32, [ctypes.POINTER(_Cloud), _f32p, _f32p, ctypes.c_uint32,
                                                   ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     "sk_lod_tree_view": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(_LodView), _f32p, _f32p]),
@@ -938,12 +936,11 @@ def _tree_array(owner: _TreeMemory, ptr, dtype, shape) -> Optional[np.ndarray]:
 
 
 def build_lod_tree(cloud: Cloud, bounds_min=None, bounds_max=None, octree_depth: int = 0,
-                   cluster_leaves: int = 0, selection: bool = True, device: bool = False) -> LodTree:
-    """buildLodTree: bounds default to the cloud's, else the positions' own box. On the host
-    (sk_build_lod_tree, bit for bit the reference's tree) or, with device=True, on the current GPU
-    (sk_build_lod_tree_device: the same layout, attributes within a few ulp)."""
+                   cluster_leaves: int = 0, selection: bool = True) -> LodTree:
+    """buildLodTree on the current GPU (sk_build_lod_tree_device): bounds default to the cloud's,
+    else the positions' own box. The reference builder's layout, attributes within a few ulp."""
     lib = library()
-    entry = "sk_build_lod_tree_device" if device else "sk_build_lod_tree"
+    entry = "sk_build_lod_tree_device"
     lo = bounds_min if bounds_min is not None else cloud.bounds_min
     hi = bounds_max if bounds_max is not None else cloud.bounds_max
     lo = None if lo is None else np.ascontiguousarray(lo, np.float32)
