@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kThreads)
                   uint32_t* __restrict__ keysOut, uint32_t* __restrict__ valuesOut,
                   const uint32_t* count, uint32_t capacity, uint32_t shift,
                   const uint32_t* __restrict__ digitBase, uint64_t* status, uint32_t* counters,
-                  uint32_t epoch, uint32_t* error) {
+                  uint32_t epoch, uint32_t* error, uint32_t withheldPlusOne) {
   chainedKernelStart();
   __shared__ ScatterSmem<kPer> s;
   constexpr uint32_t kTile = kThreads * kPer;
@@ -135,19 +135,22 @@ __global__ void __launch_bounds__(kThreads)
       total += c;
     }
     s.digitTotal[d] = total;
-    // Publish, then look back over earlier tiles for this digit.
+    // Publish, then look back over earlier tiles for this digit. A tile named by the test hook
+    // (withheldPlusOne = tile + 1; 0 names none) publishes nothing, so its successors' bounded
+    // waits run out.
     uint64_t* mine = status + static_cast<size_t>(tile) * kBins + d;
+    const bool publish = tile + 1u != withheldPlusOne;
     uint32_t exclusive = 0;
     if (tile == 0) {
-      storeStatus(mine, makeStatus(epoch, kFlagPrefix, total));
+      if (publish) storeStatus(mine, makeStatus(epoch, kFlagPrefix, total));
     } else {
-      storeStatus(mine, makeStatus(epoch, kFlagAggregate, total));
+      if (publish) storeStatus(mine, makeStatus(epoch, kFlagAggregate, total));
       for (int j = static_cast<int>(tile) - 1; j >= 0; --j) {
         const uint64_t w = waitStatus(status + static_cast<size_t>(j) * kBins + d, epoch, error);
         exclusive += static_cast<uint32_t>(w);
         if (((w >> 32) & 3u) == kFlagPrefix) break;
       }
-      storeStatus(mine, makeStatus(epoch, kFlagPrefix, exclusive + total));
+      if (publish) storeStatus(mine, makeStatus(epoch, kFlagPrefix, exclusive + total));
     }
     s.globalBase[d] = digitBase[d] + exclusive;
     // Exclusive scan of the tile's digit totals: where each digit's run starts locally.
@@ -283,7 +286,7 @@ cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
 #define SK_SCATTER_PER(IMPLICIT, WRITE, PER)                                               \
   e = launchChained(scatterKernel<IMPLICIT, WRITE, PER>, tiles, kThreads, stream, kin, vin,  \
                     kout, vout, a.count, a.capacity, 8 * p, bases + p * kBins, a.status,   \
-                    counters, epoch, a.error)
+                    counters, epoch, a.error, p == 0 ? a.withheldTilePlusOne : 0u)
 #define SK_SCATTER(IMPLICIT, WRITE)                                                        \
   do {                                                                                     \
     if (tileKeys == 2048) SK_SCATTER_PER(IMPLICIT, WRITE, 8u);                             \

@@ -95,6 +95,9 @@ struct SortArgs {
   // 1: the kernel that wrote the keys already summed their digits and left the bases in the
   // workspace (VisibilityArgs.sortPasses); the histogram pass is skipped
   uint32_t basesReady;
+  // test hook (sk_testing_withhold_sort_status): tile + 1 of the first pass whose look-back
+  // status words are not published; 0: none
+  uint32_t withheldTilePlusOne;
 };
 // Where a bound workspace keeps the digit accumulators (zero between sorts) and the bases.
 uint32_t* sortDigitAccumulators(const SortArgs& args);

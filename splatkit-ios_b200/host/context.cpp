@@ -25,9 +25,14 @@ namespace sk {
 
 // ---- buffers ------------------------------------------------------------------------------
 
+std::atomic<uint32_t> gTestFailedAllocations{0};
+
 cudaError_t DeviceBuffer::allocate(size_t n) {
   n = std::max<size_t>(n, 256);
   if (n <= bytes && ptr) return cudaSuccess;
+  // test hook (sk_testing_fail_device_allocations): this allocation fails as if out of memory
+  for (uint32_t left = gTestFailedAllocations.load(); left > 0;)
+    if (gTestFailedAllocations.compare_exchange_weak(left, left - 1)) return cudaErrorMemoryAllocation;
   void* fresh = nullptr;
   const cudaError_t e = cudaMalloc(&fresh, n);
   if (e != cudaSuccess) {
@@ -91,6 +96,10 @@ sk_status Context::fail(sk_status code, const std::string& message) {
 }
 
 sk_status Context::check(cudaError_t e, const char* what) {
+  if (testInjectedError != cudaSuccess) {  // test hook: a stand-in for a failing call
+    e = testInjectedError;
+    testInjectedError = cudaSuccess;
+  }
   if (e == cudaSuccess) return SK_OK;
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
@@ -343,6 +352,8 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     a.basesReady = 1;
     a.epoch = nextEpoch(4);
     a.error = error;
+    a.withheldTilePlusOne = testWithheldTile;
+    testWithheldTile = 0;
     e = launchSort(a, s);
   }
   if (timed) cudaEventRecord(events[3], s);

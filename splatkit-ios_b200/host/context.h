@@ -27,6 +27,9 @@ inline int hostThreadsPublic() {
   return static_cast<int>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
 }
 
+// Test hook (sk_testing_fail_device_allocations): how many of the next device allocations fail.
+extern std::atomic<uint32_t> gTestFailedAllocations;
+
 // Owning device allocation; allocate() only grows, and keeps the old memory when it fails.
 struct DeviceBuffer {
   void* ptr = nullptr;
@@ -168,6 +171,11 @@ struct Context {
   uint32_t epoch = 1;
   std::atomic<bool> failed{false};
   std::string error;
+  // test hooks (include/splatkit_b200_testing.h), each used once: the depth-sort tile of the next
+  // frame that withholds its status words (tile + 1; 0: none), and the CUDA status the next
+  // check() reads instead of its own
+  uint32_t testWithheldTile = 0;
+  cudaError_t testInjectedError = cudaSuccess;
 
   ~Context();
 

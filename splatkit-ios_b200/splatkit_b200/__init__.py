@@ -272,6 +272,10 @@ _SIGNATURES = {
                                                   ctypes.c_uint32, ctypes.c_int32,
                                                   ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_void_p]),
+    # test hooks (include/splatkit_b200_testing.h)
+    "sk_testing_fail_device_allocations": (None, [ctypes.c_uint32]),
+    "sk_testing_fail_next_check": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32]),
+    "sk_testing_withhold_sort_status": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
 }
 
 _lib: Optional[ctypes.CDLL] = None
@@ -544,6 +548,14 @@ class Renderer:
     def upload_tile(self, offset: int, cloud: Cloud):
         v = cloud.view()
         self._check(self._lib.sk_upload_tile(self._h, offset, ctypes.byref(v)), "tile")
+
+    def testing_fail_next_check(self, cuda_error: int):
+        """Test hook: the next CUDA status this context checks reads as `cuda_error`."""
+        self._check(self._lib.sk_testing_fail_next_check(self._h, cuda_error), "testing")
+
+    def testing_withhold_sort_status(self, tile: int):
+        """Test hook: in the next frame, depth-sort tile `tile` publishes no look-back status."""
+        self._check(self._lib.sk_testing_withhold_sort_status(self._h, tile), "testing")
 
     def world(self):
         n = ctypes.c_uint32()
@@ -1004,6 +1016,11 @@ def radix_argsort_noalloc(keys_ptr: int, count_ptr: int, capacity: int, bits: in
                                             error_ptr, stream)
     if st != SK_OK:
         raise SplatError(st, "sk_radix_argsort_noalloc")
+
+
+def testing_fail_device_allocations(count: int):
+    """Test hook: the next `count` device allocations of the library fail as out of memory."""
+    library().sk_testing_fail_device_allocations(count)
 
 
 def sort_workspace_bytes(capacity: int) -> int:
