@@ -290,8 +290,10 @@ sk_status sk_read_tile_lists(sk_context* ctx, uint32_t* ranges, uint32_t* values
                              uint32_t capacity, uint32_t* count);
 
 /* ---- batched multi-view rendering ---------------------------------------------------------
- * Many views, of one or several contexts' resident (flat) worlds and of different target sizes,
- * drawn together: each stage runs once over the whole batch. The same frame pipeline and
+ * Many views, of one or several contexts' resident worlds and of different target sizes, drawn
+ * together: each stage runs once over the whole batch. A view of a LOD world first selects its
+ * cut on the batch's stream (with the context's current LOD threshold and splat limit, which the
+ * batch reads but does not adapt) and is drawn from the cut. The same frame pipeline and
  * arithmetic as sk_draw, so every view's image and survivor count equal what sk_draw gives for
  * that view with 16-bit depth keys. Submissions go round robin to `lanes` CUDA streams and
  * overlap on the device; a submission's results (RGBA8 images, survivor counts) are copied to
@@ -310,7 +312,7 @@ typedef struct {
 
 typedef struct {
   sk_context* world;   /* the context whose resident world this view draws */
-  sk_frame frame;      /* camera; at most one range (none: the whole world) */
+  sk_frame frame;      /* camera; at most one range (none: the whole world; a LOD world: none) */
   uint32_t width, height;
 } sk_batch_view;
 
@@ -359,7 +361,8 @@ sk_status sk_batch_autotune(sk_batch* batch, const sk_batch_view* views, uint32_
 sk_status sk_batch_set_tuning(sk_batch* batch, const sk_batch_tuning* tuning);
 
 /* ---- serving: continuous batching of render requests --------------------------------------
- * A server holds resident scenes (contexts with flat worlds, added once) and a scheduler thread.
+ * A server holds resident scenes (contexts with flat or LOD worlds, added once) and a scheduler
+ * thread.
  * Requests are queued as they arrive; whenever one of the server's lanes is free the scheduler
  * takes the queued requests in arrival order (up to max_batch_views views and
  * max_batch_splats drawn records, within the memory budget) and runs them as one batch, so
@@ -368,8 +371,11 @@ sk_status sk_batch_set_tuning(sk_batch* batch, const sk_batch_tuning* tuning);
  * buffer. Admission: a request is priced like the reference's gpuWorldBytes (52 bytes per drawn
  * record plus its image) and waits until the priced bytes of the requests in flight leave room
  * for it under memory_budget minus the resident scenes; a request that can never fit, or that
- * has waited longer than max_queue_ms, completes with SK_E_ADMISSION. Results equal sk_draw's
- * for the same view (16-bit depth keys, default policy). */
+ * has waited longer than max_queue_ms, completes with SK_E_ADMISSION. A request for a LOD scene
+ * is priced at the scene's cut capacity; its cut is selected with the scene's LOD threshold,
+ * which every completed request of the scene then adapts (LodThreshold::update,
+ * splatkit-engine/include/splatkit/rendering/LodThreshold.h:27-36), as the scene's own frames
+ * would. Results equal sk_draw's for the same view (16-bit depth keys, default policy). */
 typedef struct sk_server sk_server;
 
 typedef struct {

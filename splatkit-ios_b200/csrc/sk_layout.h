@@ -133,9 +133,10 @@ constexpr uint32_t kTileSize = 16;  // composite tile edge in pixels
 // list and keeps, per warp quadrant, only the splats that reach it.
 constexpr uint32_t kBinSize = 2 * kTileSize;
 
-// One view of a batch (device table, 80 bytes): the world range it draws, where its work items,
-// tiles and pixels start in the batch-wide arrays, and its target size. Views are listed in
-// submission order; itemStart, tileBase and pixelOffset grow with the view index.
+// One view of a batch (device table, 96 bytes): the world range it draws (or, for a LOD world,
+// the cut its selection wrote), where its work items, tiles and pixels start in the batch-wide
+// arrays, and its target size. Views are listed in submission order; itemStart, tileBase and
+// pixelOffset grow with the view index.
 struct alignas(16) BatchView {
   const GpuSplat* splats;
   const uint32_t* sh;
@@ -149,8 +150,12 @@ struct alignas(16) BatchView {
   uint32_t binsX, binsY; // binning cells per row and column
   uint32_t width, height;
   uint64_t pixelOffset;  // first pixel of this view in the batch image
-  uint32_t pad[2];
+  const uint32_t* indices;     // a LOD view: its cut, the record indices to draw in emission
+                               // order (null: the range offset .. offset + count)
+  const uint32_t* indexCount;  // a LOD view: the cut's length (device word); count bounds it
+  uint32_t worldCount;         // records of the world (every cut index is below it)
+  uint32_t pad;
 };
-static_assert(sizeof(BatchView) == 80, "BatchView is 80 bytes");
+static_assert(sizeof(BatchView) == 96, "BatchView is 96 bytes");
 
 }  // namespace sk

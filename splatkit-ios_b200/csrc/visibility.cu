@@ -467,8 +467,9 @@ __global__ void __launch_bounds__(kThreads, 4)
   finishTile(a.counters);
 }
 
-// A batch of views in one launch. Work item i is a 1024-record chunk of one view's range;
-// items are numbered view by view, so one look-back chain over all items places every view's
+// A batch of views in one launch. Work item i is a 1024-record chunk of one view's range (or of
+// a LOD view's cut, in emission order: the chunks past the cut's length hold nothing); items
+// are numbered view by view, so one look-back chain over all items places every view's
 // survivors contiguously, in (view, source) order, and the first item of each view records
 // where that view starts. Keys carry the view id above the 16-bit depth key, so one stable
 // sort orders all views at once.
@@ -502,8 +503,17 @@ __global__ void __launch_bounds__(kThreads, 4)
     const uint32_t chunk = item - view.itemStart;
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
     const uint32_t first = chunk * kTileSplats + warp * (32 * kItems) + lane;
+    // a LOD view draws its cut (written by this stream's selection before this kernel)
+    const uint32_t drawn = view.indices ? min(view.count, *view.indexCount) : view.count;
     auto indexOf = [&](uint32_t t) -> uint32_t {
-      return t < view.count ? view.offset + t : 0xffffffffu;
+      if (t >= drawn) return 0xffffffffu;
+      if (!view.indices) return view.offset + t;
+      const uint32_t index = view.indices[t];
+      if (index >= view.worldCount) {
+        atomicOr(a.error, SK_DEVERR_BOUNDS);
+        return 0xffffffffu;
+      }
+      return index;
     };
     projectTile<D, true>(s, cam, view.splats, view.sh, view.shStride, PartLabels{}, first, v << 16,
                          indexOf);

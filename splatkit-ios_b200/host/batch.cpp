@@ -8,6 +8,8 @@
 //   depth order, views back to back) -> binning with batch-wide tile ids -> stable tile sort ->
 //   tile ranges -> composite of every tile of every view -> images, survivor counts and
 //   counters copied to pinned memory.
+// A view of a LOD world selects its cut first (on the lane's stream, with its context's current
+// threshold) and its visibility items draw the cut instead of a range.
 // The arithmetic per view is the plain frame's, so the images and counts equal sk_draw's.
 #include "batch.h"
 
@@ -120,23 +122,75 @@ sk_status Batch::reserve(BatchLane& l, uint32_t sources, uint32_t instances, uin
   return SK_OK;
 }
 
+sk_status Batch::reserveLod(BatchLane& l, uint32_t indices, uint32_t frontier, uint32_t views) {
+  cudaError_t e = cudaSuccess;
+  auto grab = [&](DeviceBuffer& b, size_t n) {
+    if (e == cudaSuccess) e = b.allocate(n);
+  };
+  frontier = std::max({frontier, l.lodFrontierCapacity, 1u});
+  const uint32_t tiles = (frontier + lodTileClusters() - 1) / lodTileClusters();
+  const void* before[3] = {l.lodStatus.ptr, l.lodCounters.ptr, l.lodState.ptr};
+  grab(l.lodIndices, size_t{std::max(indices, 1u)} * 4);
+  grab(l.lodReports, size_t{std::max(views, 1u)} * 8 * 4);
+  grab(l.lodFrontier[0], size_t{frontier} * 4);
+  grab(l.lodFrontier[1], size_t{frontier} * 4);
+  grab(l.lodCosts, size_t{frontier} * 8);
+  grab(l.lodOffsets, size_t{frontier} * 16);
+  grab(l.lodPackets, size_t{frontier} * 16);
+  grab(l.lodState, 256);
+  grab(l.lodStatus, size_t{tiles} * 3 * 8);
+  grab(l.lodCounters, 2 * 4);
+  if (e == cudaSuccess) e = l.hostLodReports.allocate(size_t{std::max(views, 1u)} * 8 * 4);
+  // fresh selection scratch: status words read "not ready", counters and state start at zero
+  if (e == cudaSuccess && (before[0] != l.lodStatus.ptr || before[1] != l.lodCounters.ptr ||
+                           before[2] != l.lodState.ptr)) {
+    e = cudaMemsetAsync(l.lodStatus.ptr, 0, l.lodStatus.bytes, l.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l.lodCounters.ptr, 0, l.lodCounters.bytes, l.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l.lodState.ptr, 0, l.lodState.bytes, l.stream);
+  }
+  if (e != cudaSuccess) return check(e, "batch LOD buffers");
+  l.lodFrontierCapacity = frontier;
+  l.lodIndexCapacity = std::max(l.lodIndexCapacity, indices);
+  l.lodReportViews = std::max(l.lodReportViews, views);
+  return SK_OK;
+}
+
 sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t count) {
   l.table.resize(count);
   l.cams.resize(count);
   l.worlds.resize(count);
-  uint32_t items = 0, tiles = 0, bins = 0, degree = 0;
+  l.lodPlans.clear();
+  uint32_t items = 0, tiles = 0, bins = 0, degree = 0, lodIndices = 0, lodFrontier = 0;
   uint64_t pixels = 0, sources = 0;
   for (uint32_t i = 0; i < count; ++i) {
     const sk_batch_view& v = views[i];
     auto* ctx = reinterpret_cast<Context*>(v.world);
     if (!ctx || ctx->device != device) return fail(SK_E_INVALID, "a view has no context on this device");
     const World& w = ctx->world;
-    if (!w.splats.ptr || w.lod) return fail(SK_E_INVALID, "a view's context holds no flat world");
+    if (!w.splats.ptr) return fail(SK_E_INVALID, "a view's context holds no world");
     if (v.width == 0 || v.height == 0 || v.width > 16384 || v.height > 16384)
       return fail(SK_E_INVALID, "view size out of range");
     uint32_t offset = 0, n = w.count;
     if (v.frame.range_count > 1) return fail(SK_E_INVALID, "a batch view draws at most one range");
-    if (v.frame.range_count == 1) {
+    if (w.lod) {
+      // the view draws the cut its selection writes: at most the world's cut capacity
+      if (v.frame.range_count != 0) return fail(SK_E_INVALID, "a LOD view draws its cut, not a range");
+      n = w.lodCapacity;
+      LodPlan plan;
+      plan.view = i;
+      plan.clusters = static_cast<const LodCluster*>(w.clusters.ptr);
+      plan.leaves = static_cast<const uint32_t*>(w.leaves.ptr);
+      plan.clusterCount = w.clusterCount;
+      plan.capacity = w.lodCapacity;
+      plan.limit = ctx->lodLimit == 0 ? w.lodCapacity : std::min(ctx->lodLimit, w.lodCapacity);
+      plan.rounds = w.rounds;
+      plan.pixelLimit = ctx->threshold.pixels();
+      plan.indexOffset = lodIndices;
+      if (uint64_t{lodIndices} + n > 0x7fffffffu) return fail(SK_E_INVALID, "batch too large");
+      lodIndices += n;
+      lodFrontier = std::max(lodFrontier, std::max(1u, std::min(w.lodCapacity, w.clusterCount)));
+      l.lodPlans.push_back(plan);
+    } else if (v.frame.range_count == 1) {
       if (!v.frame.ranges) return fail(SK_E_INVALID, "range missing");
       offset = v.frame.ranges[0].offset;
       n = v.frame.ranges[0].count;
@@ -162,6 +216,7 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
     t.binsX = (v.width + kBinSize - 1) / kBinSize;
     t.binsY = (v.height + kBinSize - 1) / kBinSize;
     t.pixelOffset = pixels;
+    t.worldCount = w.count;
     const uint64_t chunks = std::max<uint64_t>(1, (uint64_t{n} + visibilityTileSplats() - 1) /
                                                       visibilityTileSplats());
     if (uint64_t{items} + chunks > 0x7fffffffu || uint64_t{tiles} + t.tilesX * tilesY > 0x7fffffffu ||
@@ -185,6 +240,15 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
       std::max<uint64_t>(l.instances, sources * 4), 0x7fffffffu));
   sk_status st = reserve(l, static_cast<uint32_t>(sources), guess, items, tiles, count, pixels);
   if (st != SK_OK) return st;
+  if (!l.lodPlans.empty()) {
+    st = reserveLod(l, lodIndices, lodFrontier, static_cast<uint32_t>(l.lodPlans.size()));
+    if (st != SK_OK) return st;
+    for (size_t k = 0; k < l.lodPlans.size(); ++k) {
+      BatchView& t = l.table[l.lodPlans[k].view];
+      t.indices = static_cast<const uint32_t*>(l.lodIndices.ptr) + l.lodPlans[k].indexOffset;
+      t.indexCount = static_cast<const uint32_t*>(l.lodReports.ptr) + k * 8;  // report word 0
+    }
+  }
   // Every view's lists written in place when each has at most kDirectMaxCells cells.
   uint32_t mostSources = 1, mostCells = 1;
   for (const BatchView& t : l.table) {
@@ -240,6 +304,34 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     if (e == cudaSuccess)
       e = cudaMemsetAsync(probe.status, 0, sortWorkspaceBytesFor(l.instances, kMinSortTileKeys) -
                           (reinterpret_cast<char*>(probe.status) - static_cast<char*>(l.tileSortWorkspace.ptr)), s);
+  }
+  // every LOD view's cut, one view after another in the lane's selection scratch
+  for (size_t k = 0; e == cudaSuccess && k < l.lodPlans.size(); ++k) {
+    const LodPlan& p = l.lodPlans[k];
+    LodArgs a{};
+    a.clusters = p.clusters;
+    a.leaves = p.leaves;
+    a.clusterCount = p.clusterCount;
+    a.capacity = p.capacity;
+    a.limit = p.limit;
+    a.pixelLimit = p.pixelLimit;
+    a.colorWeight = 4.0f;
+    a.cull = policy.enable_frustum_culling ? 1u : 0u;
+    a.rounds = p.rounds;
+    a.frontierCapacity = l.lodFrontierCapacity;
+    a.frontier[0] = static_cast<uint32_t*>(l.lodFrontier[0].ptr);
+    a.frontier[1] = static_cast<uint32_t*>(l.lodFrontier[1].ptr);
+    a.costs = static_cast<uint2*>(l.lodCosts.ptr);
+    a.offsets = static_cast<uint4*>(l.lodOffsets.ptr);
+    a.packets = static_cast<uint4*>(l.lodPackets.ptr);
+    a.indices = static_cast<uint32_t*>(l.lodIndices.ptr) + p.indexOffset;
+    a.state = static_cast<LodState*>(l.lodState.ptr);
+    a.status = static_cast<uint64_t*>(l.lodStatus.ptr);
+    a.counters = static_cast<uint32_t*>(l.lodCounters.ptr);
+    a.epoch = nextEpoch(2 * p.rounds + 2);
+    a.error = error;
+    a.report = static_cast<uint32_t*>(l.lodReports.ptr) + k * 8;
+    e = launchLodSelect(static_cast<const Camera*>(l.cameras.ptr) + p.view, a, s);
   }
   if (e == cudaSuccess) {
     BatchVisibilityArgs v{};
@@ -359,7 +451,9 @@ sk_status Batch::enqueue(BatchLane& l) {
   const cudaStream_t s = l.stream;
   // the shape a captured graph is valid for: every view's world, range and size
   std::vector<uint64_t> shape;
-  if (tuning.graphs) {
+  // a LOD view's selection bakes its context's threshold into the launch: no graph replay
+  const bool useGraph = tuning.graphs && l.lodPlans.empty();
+  if (useGraph) {
     shape.reserve(size_t{l.viewCount} * 4 + 2);
     shape.push_back(l.viewCount);
     shape.push_back(l.shDegree);
@@ -386,6 +480,9 @@ sk_status Batch::enqueue(BatchLane& l) {
     if (r == cudaSuccess)
       r = cudaMemcpyAsync(l.hostViewFirst.ptr, l.viewFirst.ptr, size_t{l.viewCount + 1} * 4,
                           cudaMemcpyDeviceToHost, s);
+    if (r == cudaSuccess && !l.lodPlans.empty())
+      r = cudaMemcpyAsync(l.hostLodReports.ptr, l.lodReports.ptr, l.lodPlans.size() * 8 * 4,
+                          cudaMemcpyDeviceToHost, s);
     if (l.destinations.empty()) {
       if (r == cudaSuccess)
         r = cudaMemcpyAsync(l.hostImage.ptr, l.image.ptr, l.totalPixels * 4, cudaMemcpyDeviceToHost, s);
@@ -401,7 +498,7 @@ sk_status Batch::enqueue(BatchLane& l) {
   };
   sk_status st = SK_OK;
   if (e != cudaSuccess) return check(e, "batch");
-  if (tuning.graphs) {
+  if (useGraph) {
     if (!l.graph || l.graphShape != shape) {
       if (l.graph) cudaGraphExecDestroy(l.graph);
       l.graph = nullptr;

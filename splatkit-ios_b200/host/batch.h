@@ -6,6 +6,12 @@
 // (images, survivor counts, counters) are copied back into the lane's pinned memory by the
 // same stream, so they are on the host once the submission completes. A lane can capture its
 // stage sequence as a CUDA graph and replay it while its views keep their worlds and sizes.
+//
+// A view of a LOD world first has its cut selected on the lane's stream (the selection kernels
+// of csrc/lod.cu with the view's camera and its context's adaptive threshold, one view after
+// another in the lane's own LOD scratch); the batch's visibility pass then draws each such view
+// from its cut. The selection reports (cut length, limited) come back with the other results,
+// for the caller to feed its threshold.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -31,6 +37,16 @@ struct BatchTuning {
   uint32_t sortTileKeys = 4096; // keys per radix scatter tile: 2048, 4096 or 6144
 };
 
+// The selection one LOD view of a submission runs (LodArgs less the lane's scratch).
+struct LodPlan {
+  uint32_t view = 0;            // index in the submission
+  const LodCluster* clusters = nullptr;
+  const uint32_t* leaves = nullptr;
+  uint32_t clusterCount = 0, capacity = 0, limit = 0, rounds = 0;
+  float pixelLimit = 1.0f;
+  uint32_t indexOffset = 0;     // where its cut starts in the lane's index buffer
+};
+
 struct BatchLane {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr, start = nullptr, end = nullptr;
@@ -46,8 +62,14 @@ struct BatchLane {
   DeviceBuffer cellLists, cellStatus, entryBases;
   bool directLists = false;
   uint32_t cellGroupsPerView = 0;
+  // LOD views: every view's cut, each view's six report words (LodState's first six), and the
+  // selection scratch the views share in turn (sized for the largest)
+  DeviceBuffer lodIndices, lodReports, lodFrontier[2], lodCosts, lodOffsets, lodPackets, lodState,
+      lodStatus, lodCounters;
+  uint32_t lodIndexCapacity = 0, lodFrontierCapacity = 0, lodReportViews = 0;
+  std::vector<LodPlan> lodPlans;
   // pinned host
-  PinnedBuffer hostViews, hostCameras, hostCounters, hostViewFirst, hostImage;
+  PinnedBuffer hostViews, hostCameras, hostCounters, hostViewFirst, hostImage, hostLodReports;
   // the submission it holds
   uint64_t ticket = 0;
   bool busy = false, harvested = true;
@@ -82,6 +104,8 @@ struct Batch {
   uint32_t nextEpoch(uint32_t n);
   sk_status reserve(BatchLane& lane, uint32_t sources, uint32_t instances, uint32_t items,
                     uint32_t tiles, uint32_t views, uint64_t pixels);
+  // The LOD views' cuts (indices in total), reports and selection scratch (frontier entries).
+  sk_status reserveLod(BatchLane& lane, uint32_t indices, uint32_t frontier, uint32_t views);
   // Fills the lane's view table and cameras from the request; no device work.
   sk_status prepare(BatchLane& lane, const sk_batch_view* views, uint32_t count);
   // Enqueues the lane's whole batch on its stream (uploads, stages, readbacks, done event).

@@ -6,6 +6,12 @@
 // so requests that arrive while other batches are on the GPU join the next one and their work
 // overlaps with what is in flight. Completed lanes are harvested by polling their events; each
 // request's image has already been copied into its caller's buffer by the lane's stream.
+//
+// A scene is a context with a flat world or a LOD world. What stays on the device between
+// requests for a scene: its records, harmonics and (LOD) selection data, and each lane's scratch,
+// cuts and selection buffers; what carries from one request to the next on the host is a LOD
+// scene's adaptive threshold (LodThreshold), fed by every completed request's selection report
+// the way a context feeds it from its own frames, so a scene's cuts track its load.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -38,6 +44,7 @@ struct Pending {
 struct Scene {
   Context* ctx = nullptr;
   uint64_t worldBytes = 0;
+  uint64_t requests = 0;  // completed requests (a LOD scene's threshold has seen each)
 };
 
 struct LaneWork {
@@ -97,6 +104,15 @@ void Server::harvest(uint32_t i) {
   const auto end = Clock::now();
   LaneWork& w = work[i];
   const auto* first = static_cast<const uint32_t*>(l.hostViewFirst.ptr);
+  // LOD scenes: each request's cut feeds its scene's threshold (LodThreshold::update with the
+  // selected and limited counts, as a context does after each of its frames)
+  const auto* reports = static_cast<const uint32_t*>(l.hostLodReports.ptr);
+  for (size_t k = 0; st == SK_OK && k < l.lodPlans.size(); ++k) {
+    const uint32_t* r = reports + k * 8;
+    Scene& scene = scenes[w.requests[l.lodPlans[k].view].request.scene];
+    scene.ctx->threshold.update(r[0], r[4], l.lodPlans[k].limit);
+  }
+  for (const Pending& p : w.requests) ++scenes[p.request.scene].requests;
   for (size_t k = 0; k < w.requests.size(); ++k) {
     const uint32_t visible = st == SK_OK ? first[k + 1] - first[k] : 0u;
     complete(w.requests[k], st == SK_OK ? SK_OK : st, visible,
@@ -156,8 +172,9 @@ bool Server::launch(uint32_t i) {
     const Pending& p = w.requests[k];
     views[k].world = reinterpret_cast<sk_context*>(scenes[p.request.scene].ctx);
     views[k].frame = p.request.frame;
-    views[k].frame.ranges = &p.range;
-    views[k].frame.range_count = 1;
+    const bool lod = scenes[p.request.scene].ctx->world.lod;
+    views[k].frame.ranges = lod ? nullptr : &p.range;
+    views[k].frame.range_count = lod ? 0 : 1;
     views[k].width = p.request.width;
     views[k].height = p.request.height;
     l.destinations[k] = p.request.image;
@@ -275,9 +292,11 @@ sk_status sk_server_add_scene(sk_server* handle, sk_context* world, uint32_t* sc
   auto* s = reinterpret_cast<Server*>(handle);
   auto* ctx = reinterpret_cast<sk::Context*>(world);
   if (!s || !ctx) return SK_E_INVALID;
-  if (ctx->device != s->config.device || !ctx->world.splats.ptr || ctx->world.lod)
-    return s->fail(SK_E_INVALID, "a scene is a context with a flat world on the server's device");
-  const uint64_t bytes = sk::host::worldBytes(ctx->world.count, ctx->world.shDegree, 0, 0, 0);
+  if (ctx->device != s->config.device || !ctx->world.splats.ptr)
+    return s->fail(SK_E_INVALID, "a scene is a context with a world on the server's device");
+  const sk::World& w = ctx->world;
+  const uint64_t bytes = sk::host::worldBytes(w.count, w.shDegree, 0, w.lod ? w.clusterCount : 0,
+                                              w.lod ? w.leafRefCount : 0);
   std::lock_guard<std::mutex> g(s->mutex);
   if (s->residentBytes + bytes > s->config.memory_budget) {
     s->error = "the scene does not fit the memory budget";
@@ -299,6 +318,11 @@ sk_status sk_server_submit(sk_server* handle, const sk_request* r, uint64_t* id)
     return SK_E_INVALID;
   }
   const sk::Context* ctx = s->scenes[r->scene].ctx;
+  const bool lod = ctx->world.lod;
+  if (lod && r->frame.range_count != 0) {
+    s->error = "a request for a LOD scene draws its cut, not a range";
+    return SK_E_INVALID;
+  }
   sk::Pending p;
   p.id = ++s->nextId;
   p.request = *r;
@@ -309,7 +333,7 @@ sk_status sk_server_submit(sk_server* handle, const sk_request* r, uint64_t* id)
   }
   p.request.frame.ranges = nullptr;
   p.degree = static_cast<uint32_t>(std::max(0, std::min(r->frame.sh_degree, ctx->world.shDegree)));
-  p.splats = p.range.count;
+  p.splats = lod ? ctx->world.lodCapacity : p.range.count;  // a cut draws at most its capacity
   p.priced = sk::kDrawBytesPerSplat * p.splats + uint64_t{r->width} * r->height * 4;
   p.arrival = sk::Clock::now();
   s->queue.push_back(p);

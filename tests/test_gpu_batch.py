@@ -181,3 +181,42 @@ def test_every_tuning_draws_the_same_images_and_the_tuner_picks_one(worlds):
         assert chosen["gpu_ms"] > 0 and chosen["views_per_s"] > 0
         ticket = batch.submit(views)
         check_against_plain(batch, ticket, views)
+
+
+@pytest.mark.gpu
+def test_lod_views_select_their_cuts_in_the_batch(cuda_device):
+    """Views of two LOD worlds and a flat one in one submission, graphs asked for (a batch with
+    LOD views runs its stages directly): each LOD view's cut is selected on the batch's stream
+    with its context's threshold and the view equals sk_draw's frame of that context."""
+    policy = sk.Policy(lod_error_pixels=1.5, sort_depth_bits=16)
+    renderers = []
+    for seed in (81, 82):
+        tree = sk.build_lod_tree(synthetic.clustered_cloud(30, 500, seed=seed, half_extent=20.0))
+        r = sk.Renderer(64, 64, image_format=sk.FORMAT_RGBA8)
+        r.apply_render_policy(policy)
+        r.upload_lod_world(tree, 0, 4_000_000)
+        renderers.append(r)
+    flat_cloud = synthetic.random_cloud(25_000, seed=83, sh_degree=0)
+    flat = sk.Renderer(64, 64, image_format=sk.FORMAT_RGBA8)
+    flat.apply_render_policy(policy)
+    flat.upload_world(flat_cloud, 0)
+    views = []
+    for i in range(9):
+        w, h = SIZES[i % len(SIZES)]
+        eye = np.array([-20.0 + 5.0 * i, 2.0, 30.0], np.float32)
+        view = skcam.look_at_view(eye, (0.0, 0.0, 0.0))
+        if i % 3 == 2:
+            frame = sk.Frame(view, proj_for(w, h), eye, [(0, flat_cloud.count)], 0)
+            views.append(sk.BatchView(flat, frame, w, h))
+        else:
+            views.append(sk.BatchView(renderers[i % 3], sk.Frame(view, proj_for(w, h), eye, [], 0), w, h))
+    try:
+        with sk.Batch(lanes=2, max_views=16, use_graphs=True) as batch:
+            for _ in range(2):  # the second submission reuses the lane's LOD buffers
+                ticket = batch.submit(views)
+                batch.wait(ticket)
+                assert batch.stats(ticket)["device_error"] == 0
+            check_against_plain(batch, ticket, views)
+    finally:
+        for r in renderers + [flat]:
+            r.close()

@@ -94,3 +94,96 @@ def test_admission_sheds_what_cannot_fit(scenes):
     for (s, _, w, h), c in zip(frames, done):
         fits = 52 * scenes[s][1].count + 4 * w * h <= 52 * 100_000
         assert c["status"] == (sk.SK_OK if fits else sk.SK_E_ADMISSION), (s, w, h)
+
+
+# ---- LOD scenes ------------------------------------------------------------------------------
+LOD_W, LOD_H = 480, 320
+
+
+def lod_frame(x, w=LOD_W, h=LOD_H):
+    eye = np.array([x, 1.7, 35.0], np.float32)
+    view = skcam.look_at_view(eye, (x * 0.5, 0.0, 0.0))
+    proj = skcam.perspective(math.radians(60.0), w / h, 0.05, 400.0)
+    return sk.Frame(view, proj, eye, [], 0)
+
+
+@pytest.fixture(scope="module")
+def lod_trees(cuda_device):
+    trees = []
+    for seed in (71, 72):
+        cloud = synthetic.clustered_cloud(40, 600, seed=seed, half_extent=25.0)
+        trees.append(sk.build_lod_tree(cloud))
+    return trees
+
+
+def lod_renderer(tree, policy):
+    r = sk.Renderer(64, 64, image_format=sk.FORMAT_RGBA8)
+    r.apply_render_policy(policy)
+    r.upload_lod_world(tree, 0, 4_000_000)
+    return r
+
+
+@pytest.mark.gpu
+def test_lod_scene_requests_equal_their_plain_frames(lod_trees, cuda_device):
+    """LOD scenes beside a flat one: each request's cut is selected on the server's lane and its
+    image equals the plain frame of the scene's own context."""
+    policy = sk.Policy(lod_error_pixels=1.5, sort_depth_bits=16)
+    flat_cloud = synthetic.random_cloud(30_000, seed=73, sh_degree=0)
+    flat = sk.Renderer(64, 64, image_format=sk.FORMAT_RGBA8)
+    flat.apply_render_policy(policy)
+    flat.upload_world(flat_cloud, 0)
+    scenes = [(lod_renderer(t, policy), None) for t in lod_trees] + [(flat, flat_cloud)]
+    rng = np.random.default_rng(74)
+    frames = []
+    for i in range(24):
+        s = int(rng.integers(0, 3))
+        w, h = SIZES[int(rng.integers(0, len(SIZES)))]
+        f = lod_frame(float(rng.uniform(-30, 30)), w, h)
+        if s == 2:
+            f = sk.Frame(f.view, f.proj, f.camera_position, [(0, flat_cloud.count)], 0)
+        frames.append((s, f, w, h))
+    arrivals = np.cumsum(rng.exponential(200.0, len(frames)))
+    try:
+        done, images = serve(scenes, frames, arrivals)
+        batched = 0
+        for (s, f, w, h), c, img in zip(frames, done, images):
+            assert c["status"] == sk.SK_OK
+            want, visible = plain_image(scenes[s][0], f, w, h)
+            assert c["visible"] == visible > 0
+            assert np.array_equal(img.array, want)
+            batched += c["batch_views"] > 1
+        assert batched > 0
+    finally:
+        for r, _ in scenes:
+            r.close()
+
+
+@pytest.mark.gpu
+def test_a_lod_scene_keeps_its_threshold_across_requests(lod_trees, cuda_device):
+    """A splat limit that binds: the scene's adaptive threshold rises request after request
+    (LodThreshold.h:27-36), fed by each completed request's cut. Served one at a time, the
+    requests draw exactly the frames the scene's own context draws for the same camera path."""
+    tree = lod_trees[0]
+    leaves = tree.leaf_count
+    policy = sk.Policy(lod_error_pixels=0.5, lod_splat_limit=leaves // 6, sort_depth_bits=16)
+    served_scene = lod_renderer(tree, policy)
+    plain = lod_renderer(tree, policy)
+    frames = [(0, lod_frame(-20.0 + 2.0 * k), LOD_W, LOD_H) for k in range(12)]
+    try:
+        with sk.Server(lanes=1, max_batch_views=1) as server:
+            server.add_scene(served_scene)
+            images = [sk.HostImage(LOD_W, LOD_H) for _ in frames]
+            requests = [sk.Request(0, f, w, h, img) for (_, f, w, h), img in zip(frames, images)]
+            done = server.replay(requests, [0.0] * len(frames))
+        thresholds = []
+        for (_, f, w, h), c, img in zip(frames, done, images):
+            assert c["status"] == sk.SK_OK
+            want, visible = plain_image(plain, f, w, h)
+            thresholds.append(plain.stats()["lod_pixels"])
+            assert c["visible"] == visible
+            assert np.array_equal(img.array, want)
+        assert thresholds[-1] > thresholds[0] > 0.5  # the limit bound and the threshold rose
+        assert served_scene.stats()["lod_pixels"] == pytest.approx(thresholds[-1])
+    finally:
+        served_scene.close()
+        plain.close()
