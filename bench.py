@@ -457,6 +457,7 @@ def run_ours(args):
             line["cpu_baseline"] = cpu_baseline(args.bits, args.warmup - 1, args.warmup)
         if world == 1 and not args.no_batch and args.bits == 16:
             line["batch64"] = measure_batch(r)
+            line["sort_large"] = measure_sort_large()
         if world == 1 and not args.no_lod and args.bits == 16:
             line["lod_walk"] = measure_lod_walk()
         if world == 1 and not args.no_serve and args.bits == 16:
@@ -507,6 +508,60 @@ def time_key_width(r, frame, flush, bits, steps, warmup):
             "sort_keys_per_s": visible / (mean["sort_ms"] / 1000.0),
             "how": "device time per frame (frame events), then a second pass with per-stage "
                    "events; L2 flushed before every frame"}
+
+
+def measure_sort_large(keys_n=40_000_000, reps=20):
+    """The depth sort where HBM can bind: the argsort operator (sk_radix_argsort_device) over 40M
+    keys (160 MB, above the 126 MB L2), 16-bit and 32-bit keys, device time per call with CUDA
+    events on the sort's stream. Algorithmic bytes per key: 4 (one all-digit histogram read) + 12
+    (first pass: read the key, write key and value) + 16 per middle pass + 12 (last pass, no key
+    write): 28 B at 16 bits, 60 B at 32."""
+    import torch
+
+    import splatkit_b200 as sk
+
+    dev = torch.device("cuda")
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(40)
+    out = {}
+    peak, peak_kind = measured_peaks()
+    for bits, per_key in ((16, 28), (32, 60)):
+        hi = 1 << bits
+        keys = torch.randint(0, hi, (keys_n,), device=dev, generator=gen, dtype=torch.int64)
+        keys = (keys - (1 << 31) if bits == 32 else keys).to(torch.int32)
+        count = torch.tensor([keys_n], dtype=torch.int32, device=dev)
+        order = torch.empty(keys_n, dtype=torch.int32, device=dev)
+        ws = torch.zeros(sk.sort_workspace_bytes(keys_n), dtype=torch.uint8, device=dev)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        stream = torch.cuda.current_stream().cuda_stream
+        sort_bits = bits
+
+        def call():
+            sk.radix_argsort_device(keys.data_ptr(), count.data_ptr(), keys_n, sort_bits, order.data_ptr(),
+                                    ws.data_ptr(), ws.numel(), err.data_ptr(), stream)
+
+        for _ in range(3):
+            call()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(reps):
+            call()
+        end.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(end) / reps
+        # spot check: the order sorts the keys stably
+        k = keys.cpu().numpy().view(np.uint32)
+        o = order.cpu().numpy()
+        sorted_ok = bool(np.all(np.diff(k[o].astype(np.int64)) >= 0)) and int(err.item()) == 0
+        gbs = per_key * keys_n / (ms / 1000.0) / 1e9
+        out[f"bits{bits}"] = {"ms": ms, "keys_per_s": keys_n / (ms / 1000.0), "algorithmic_bytes_per_key": per_key,
+                              "gbs": gbs, "frac": gbs / peak, "sorted": sorted_ok}
+        del keys, order, ws
+    out["peak_gbs"] = peak
+    out["peak_kind"] = peak_kind
+    out["workload"] = f"{keys_n} uniform random keys, stable argsort, {reps} back-to-back calls"
+    return out
 
 
 # ---- batched multi-view: 64 views of the 1M SH3 scene, mixed resolutions ----------------------

@@ -87,7 +87,7 @@ def test_device_tree_build_gives_the_reference_layout_and_cuts(walk_tree, cuda_d
     builder's exactly and node attributes agree within a few ulp; drawn along the whole 300-frame
     walk, each frame's cut (node indices in emission order) equals the reference tree's."""
     d = walk_tree
-    gpu = sk.build_lod_tree(walk_cloud(), device=True)
+    gpu = sk.build_lod_tree(walk_cloud())
     assert gpu.leaf_count == d["leaf_count"] and len(gpu.layout) == len(d["layout"])
     np.testing.assert_array_equal(gpu.layout["child_start"], d["layout"]["child_start"])
     np.testing.assert_array_equal(gpu.layout["child_count"], d["layout"]["child_count"])
