@@ -5,9 +5,9 @@
 // The reference runs histogram -> scan -> scatter per pass (SplatRadixSort.metal:17-171). Here:
 //   1. one upfront pass reads every key once and builds all digit histograms; the block that
 //      finishes last turns them into exclusive digit bases;
-//   2. one scatter pass per digit. Each tile (1024 to 6144 keys, 4096 by default) ranks its
-//      keys per warp with ballot matching (8 ballots per row, rows in source order, so ranking
-//      is stable), publishes
+//   2. one scatter pass per digit. Each tile (2048, 4096 or 6144 keys, 4096 by default) ranks
+//      its keys per warp with ballot matching (8 ballots per row, rows in source order, so
+//      ranking is stable), publishes
 //      its per-digit counts, and learns how many keys of each digit the tiles before it hold
 //      by decoupled look-back (bounded waits), then reorders locally in shared memory and
 //      writes each digit run contiguously.
@@ -262,8 +262,7 @@ cudaError_t sortResetWorkspace(const SortArgs& a, cudaStream_t stream) {
 cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
   const uint32_t passes = static_cast<uint32_t>(min(max(a.bits, 8), 32) + 7) / 8u;
   const uint32_t tileKeys = tileKeysOf(a);
-  if (tileKeys != 1024 && tileKeys != 2048 && tileKeys != 4096 && tileKeys != 6144)
-    return cudaErrorInvalidValue;
+  if (tileKeys != 2048 && tileKeys != 4096 && tileKeys != 6144) return cudaErrorInvalidValue;
   const uint32_t tiles = sortTiles(a.capacity, tileKeys);
   if (tiles > a.statusTiles) return cudaErrorInvalidValue;  // the workspace was bound for larger tiles
   uint32_t* accum = a.histogram;
@@ -291,8 +290,7 @@ cudaError_t launchSort(const SortArgs& a, cudaStream_t stream) {
                     counters, epoch, a.error, p == 0 ? a.withheldTilePlusOne : 0u)
 #define SK_SCATTER(IMPLICIT, WRITE)                                                        \
   do {                                                                                     \
-    if (tileKeys == 1024) SK_SCATTER_PER(IMPLICIT, WRITE, 4u);                             \
-    else if (tileKeys == 2048) SK_SCATTER_PER(IMPLICIT, WRITE, 8u);                        \
+    if (tileKeys == 2048) SK_SCATTER_PER(IMPLICIT, WRITE, 8u);                             \
     else if (tileKeys == 6144) SK_SCATTER_PER(IMPLICIT, WRITE, 24u);                       \
     else SK_SCATTER_PER(IMPLICIT, WRITE, 16u);                                             \
   } while (0)

@@ -90,7 +90,7 @@ struct SortArgs {
   uint32_t* counters;   // 2 * 5 words
   uint32_t epoch;       // uses epoch .. epoch + 3
   uint32_t* error;
-  uint32_t tileKeys;    // keys per scatter tile: 1024, 2048, 4096 (0: the default) or 6144
+  uint32_t tileKeys;    // keys per scatter tile: 2048, 4096 (0: the default) or 6144
   uint32_t statusTiles; // tiles the bound status region holds (set by the bind)
   // 1: the kernel that wrote the keys already summed their digits and left the bases in the
   // workspace (VisibilityArgs.sortPasses); the histogram pass is skipped

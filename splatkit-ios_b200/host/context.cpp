@@ -134,7 +134,7 @@ sk_status Context::reserveScratch(FrameScratch& f, uint32_t sources, uint32_t in
   grab(f.projected, size_t{sources} * sizeof(Projected));
   grab(f.spans, size_t{sources} * 16);
   grab(f.order, size_t{sources} * 4);
-  grab(f.sortWorkspace, sortWorkspaceBytesFor(sources, kMinDepthSortTileKeys));
+  grab(f.sortWorkspace, sortWorkspaceBytes(sources));
   grab(f.visStatus, size_t{visTiles} * 8);
   grab(f.binSums, size_t{binBlocks(sources)} * 4);
   grab(f.instKeys, size_t{instances} * 4);
@@ -306,8 +306,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
   }
   // The depth sort's workspace: the cull sums the digits of the keys it writes into it.
   SortArgs depthSort{};
-  sortBindWorkspaceFor(depthSort, f.sortWorkspace.ptr, f.sources, kMinDepthSortTileKeys);
-  depthSort.tileKeys = depthSortTileKeys(f.sources);
+  sortBindWorkspace(depthSort, f.sortWorkspace.ptr, f.sources);
   if (e == cudaSuccess) {
     VisibilityArgs v{};
     v.splats = static_cast<const GpuSplat*>(world.splats.ptr);

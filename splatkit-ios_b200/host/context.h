@@ -23,14 +23,6 @@ inline constexpr uint32_t kMaxRanges = 65536;             // MetalVisibilityPass
 inline constexpr float kTransmittanceCutoff = 1e-4f;
 // Scatter tile size of the plain frame's tile sort (measured: 4096 beats 2048 at 4.5M pairs).
 inline constexpr uint32_t kTileSortTileKeys = 4096;
-// Keys per scatter tile of a frame's depth sort: small tiles while the survivors are few, so the
-// scatter passes fill the GPU (a million keys make about a thousand 1024-key tiles, two waves of
-// resident tiles on 148 SMs); 4096 once there are keys enough for that. The frame's sort
-// workspace is laid out for the smallest.
-inline constexpr uint32_t kMinDepthSortTileKeys = 1024;
-inline uint32_t depthSortTileKeys(uint32_t capacity) {
-  return capacity <= (2u << 20) ? 1024u : (capacity <= (4u << 20) ? 2048u : 4096u);
-}
 inline int hostThreadsPublic() {
   return static_cast<int>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
 }
