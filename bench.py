@@ -51,6 +51,8 @@ def parse(argv=None):
     p.add_argument("--no-batch", action="store_true", help="skip the 64-view batched comparison")
     p.add_argument("--no-serve", action="store_true", help="skip the serving comparison")
     p.add_argument("--no-lod", action="store_true", help="skip the LOD walk")
+    p.add_argument("--sort-large-only", action="store_true",
+                   help="only the 40M-key argsort measurement (one JSON object), e.g. as a profiling target")
     return p.parse_args(argv)
 
 
@@ -879,6 +881,9 @@ def cpu_baseline(bits, warmup, first):
 
 def main():
     args = parse()
+    if args.sort_large_only:
+        print(json.dumps({"sort_large": measure_sort_large()}), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
