@@ -41,18 +41,30 @@ __global__ void __launch_bounds__(kThreads)
   for (uint32_t i = threadIdx.x; i < kMaxPasses * kBins; i += kThreads) (&h[0][0])[i] = 0;
   __syncthreads();
   const uint32_t n = clampCount(count, capacity);
-  const uint32_t stride = gridDim.x * kThreads;
-  for (uint32_t i = (blockIdx.x * kThreads + threadIdx.x) * 4; i < n; i += stride * 4) {
-    uint32_t k[4];
-    if (i + 3 < n) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(keys + i));
-      k[0] = v.x, k[1] = v.y, k[2] = v.z, k[3] = v.w;
-    } else {
-      for (uint32_t j = 0; j < 4; ++j) k[j] = i + j < n ? keys[i + j] : 0u;
+  const uint32_t stride = gridDim.x * kThreads * 4;  // keys per grid step of one uint4 per thread
+  // four 16-byte loads in flight per thread, then their 16 keys counted
+  for (uint32_t base = (blockIdx.x * kThreads + threadIdx.x) * 4; base < n; base += stride * 4) {
+    uint4 v[4];
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+      const uint32_t i = base + q * stride;
+      if (i + 3 < n) {
+        v[q] = __ldg(reinterpret_cast<const uint4*>(keys + i));
+      } else {
+        v[q].x = i < n ? keys[i] : 0u;
+        v[q].y = i + 1 < n ? keys[i + 1] : 0u;
+        v[q].z = i + 2 < n ? keys[i + 2] : 0u;
+        v[q].w = i + 3 < n ? keys[i + 3] : 0u;
+      }
     }
-    for (uint32_t j = 0; j < 4; ++j) {
-      if (i + j >= n) break;
-      for (uint32_t p = 0; p < passes; ++p) atomicAdd(&h[p][(k[j] >> (8 * p)) & 0xffu], 1u);
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+      const uint32_t i = base + q * stride;
+      const uint32_t k[4] = {v[q].x, v[q].y, v[q].z, v[q].w};
+      for (uint32_t j = 0; j < 4; ++j) {
+        if (i + j >= n) break;
+        for (uint32_t p = 0; p < passes; ++p) atomicAdd(&h[p][(k[j] >> (8 * p)) & 0xffu], 1u);
+      }
     }
   }
   __syncthreads();
