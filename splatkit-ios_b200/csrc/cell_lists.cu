@@ -307,7 +307,15 @@ __global__ void __launch_bounds__(kThreads)
       cell = spanCell(sSpan[item], p - itemStart, a.tilesX);
       val = sValue[item];
     }
-    const uint32_t peers = __match_any_sync(0xffffffffu, cell);
+    // lanes of this round with the same cell: 13 ballots (cells are below 4096; an idle lane's
+    // 0xffffffff differs from every cell in bit 12)
+    uint32_t peers = 0xffffffffu;
+#pragma unroll
+    for (uint32_t b = 0; b < 13; ++b) {
+      const bool bit = (cell >> b) & 1u;
+      const uint32_t vote = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? vote : ~vote;
+    }
     const uint32_t half = (cell & 1u) * 16;
     uint32_t slot = 0;
     if (valid) slot = where[cell] + ((mine[cell >> 1] >> half) & 0xffffu) + __popc(peers & below);
