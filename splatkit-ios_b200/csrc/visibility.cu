@@ -306,14 +306,11 @@ struct VisibilitySmem {
 };
 
 // Projects one 1024-record tile into shared memory: survivors' keys and records at their
-// source slot, and per warp row the mask of survivors. indexOf(t) gives the record index of
+// source slot, and per warp row the mask of survivors. Part styles (when labels are given) and
+// the reveal glow are applied to each survivor's record after its projection. indexOf(t) gives the record index of
 // tile position t, or 0xffffffff past the end. keyHigh is or-ed into every key (the view id of a
 // batch, above a 16-bit key). One record per row of the warp, not unrolled (the projection is
 // large); the next row's record is fetched while this one is projected.
-// With harmonics (D >= 1) the records leave here with their base colour only: the survivors'
-// harmonics colour, part style and reveal glow are applied later by colorSurvivors, spread over
-// the whole block (a part style's drop decision depends on opacity alone and is taken here). With
-// none, the style and glow are applied here.
 template <int D, bool kKey16, typename IndexOf>
 __device__ __forceinline__ void projectTile(VisibilitySmem& s, const Camera& cam,
                                             const GpuSplat* __restrict__ splats,
@@ -342,14 +339,9 @@ __device__ __forceinline__ void projectTile(VisibilitySmem& s, const Camera& cam
     const uint32_t slot = warp * (32 * kItems) + r * 32 + lane;
     if (index != 0xffffffffu) {
       uint32_t key, rec[8];
-      visible = projectSplat<0, kKey16>(cam, lo, hi, index, sh, shStride, key, rec);
-      if constexpr (D == 0) {
-        if (visible && parts.labels) visible = styleRecord(parts, index, rec);
-        if (visible) revealGlow(cam, asF(lo.y), rec);
-      } else if (visible && parts.labels) {
-        uint32_t styled[8] = {rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], rec[6], rec[7]};
-        visible = styleRecord(parts, index, styled);  // the decision only; colours come later
-      }
+      visible = projectSplat<D, kKey16>(cam, lo, hi, index, sh, shStride, key, rec);
+      if (visible && parts.labels) visible = styleRecord(parts, index, rec);
+      if (visible) revealGlow(cam, asF(lo.y), rec);
       if (visible) {
         s.key[slot] = key | keyHigh;
         s.rec[2 * slot] = make_uint4(rec[0], rec[1], rec[2], rec[3]);
@@ -363,15 +355,11 @@ __device__ __forceinline__ void projectTile(VisibilitySmem& s, const Camera& cam
   __syncwarp();
 }
 
-// Order-preserving compaction of the tile's survivors, in two parts. rankTile (the whole block):
-// the warps' survivor counts, the tile's aggregate published at once for the tiles after it, and
-// survivor k of the tile -> its source slot; it leaves the count in s.tileCount and ends with a
-// barrier. placeTile (warp 0 only): the tile's offset by decoupled look-back over status[0 ..
-// tile], then its inclusive prefix published; the offset is in s.tileBase after the block's next
-// barrier. Nothing else the block does needs the offset before the copy-out, so the survivors'
-// colours are finished while warp 0 looks back.
-__device__ __forceinline__ void rankTile(VisibilitySmem& s, uint64_t* status, uint32_t tile,
-                                         uint32_t epoch) {
+// Order-preserving compaction of the tile's survivors: warp totals, the tile's offset by
+// decoupled look-back over status[0 .. tile], then survivor k of the tile -> its source slot.
+// Leaves the offset and count in s.tileBase / s.tileCount.
+__device__ __forceinline__ void compactTile(VisibilitySmem& s, uint64_t* status, uint32_t tile,
+                                            uint32_t epoch, uint32_t* error) {
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
   uint32_t warpTotal = 0;
 #pragma unroll
@@ -388,14 +376,17 @@ __device__ __forceinline__ void rankTile(VisibilitySmem& s, uint64_t* status, ui
     }
     const uint32_t aggregate = __shfl_sync(0xffffffffu, inclusive, 31);
     if (lane < kThreads / 32) s.warpBase[lane] = inclusive - mine;
+    uint32_t exclusive = 0;
+    if (tile == 0) {
+      if (lane == 0) storeStatus(status, makeStatus(epoch, kFlagPrefix, aggregate));
+    } else {
+      if (lane == 0) storeStatus(status + tile, makeStatus(epoch, kFlagAggregate, aggregate));
+      exclusive = warpLookback(status, tile, epoch, error);
+      if (lane == 0) storeStatus(status + tile, makeStatus(epoch, kFlagPrefix, exclusive + aggregate));
+    }
     if (lane == 0) {
+      s.tileBase = exclusive;
       s.tileCount = aggregate;
-      if (tile == 0) {
-        s.tileBase = 0;
-        storeStatus(status, makeStatus(epoch, kFlagPrefix, aggregate));
-      } else {
-        storeStatus(status + tile, makeStatus(epoch, kFlagAggregate, aggregate));
-      }
     }
   }
   __syncthreads();
@@ -408,56 +399,6 @@ __device__ __forceinline__ void rankTile(VisibilitySmem& s, uint64_t* status, ui
     pos += __popc(mask);
   }
   __syncthreads();
-}
-
-__device__ __forceinline__ void placeTile(VisibilitySmem& s, uint64_t* status, uint32_t tile,
-                                          uint32_t epoch, uint32_t* error) {
-  if (tile == 0) return;
-  const uint32_t exclusive = warpLookback(status, tile, epoch, error);
-  if (laneId() == 0) {
-    storeStatus(status + tile, makeStatus(epoch, kFlagPrefix, exclusive + s.tileCount));
-    s.tileBase = exclusive;
-  }
-}
-
-// The survivors' final colours (D >= 1): base colour plus harmonics (SplatProjection.metalh:
-// 126-131), then the part style and the reveal glow, as projectSplat and projectTile would have
-// applied them in place, survivor k of the tile by thread k mod kThreads. The opacity half of the
-// record is already final.
-template <int D>
-__device__ __forceinline__ void colorSurvivors(VisibilitySmem& s, const Camera& cam,
-                                               const GpuSplat* __restrict__ splats,
-                                               const uint32_t* __restrict__ sh, uint32_t shStride,
-                                               const PartLabels& parts) {
-  if constexpr (D >= 1) {
-    for (uint32_t k = threadIdx.x; k < s.tileCount; k += kThreads) {
-      const uint32_t slot = s.slotOf[k];
-      uint4 hi = s.rec[2 * slot + 1];
-      const uint32_t index = hi.w;
-      const uint4 lo = __ldg(reinterpret_cast<const uint4*>(splats + index));
-      ShWords<D> words;
-      words.load(sh, index, shStride);
-      const uint32_t rgba8 = lo.w;
-      float rgb[3] = {blockUnorm8[rgba8 & 0xffu], blockUnorm8[(rgba8 >> 8) & 0xffu],
-                      blockUnorm8[(rgba8 >> 16) & 0xffu]};
-      const float dx = asF(lo.x) - cam.cameraPosition[0];
-      const float dy = asF(lo.y) - cam.cameraPosition[1];
-      const float dz = asF(lo.z) - cam.cameraPosition[2];
-      const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
-      float c[3];
-      shColor<D>(words, dx / len, dy / len, dz / len, c);
-#pragma unroll
-      for (int j = 0; j < 3; ++j) rgb[j] = fmaxf(rgb[j] + c[j], 0.0f);
-      uint32_t rec[8];
-      rec[4] = packHalf2(rgb[0], rgb[1]);
-      rec[5] = floatToHalf(rgb[2]) | (hi.y & 0xffff0000u);
-      if (parts.labels) styleRecord(parts, index, rec);
-      revealGlow(cam, asF(lo.y), rec);
-      hi.x = rec[4];
-      hi.y = rec[5];
-      s.rec[2 * slot + 1] = hi;
-    }
-  }
 }
 
 // Coalesced copy-out: consecutive threads write consecutive survivors, with the tiles each
@@ -508,10 +449,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       return index;
     };
     projectTile<D, kKey16>(s, cam, a.splats, a.sh, a.shStride, a.parts, first, 0u, indexOf);
-    rankTile(s, a.status, tile, a.epoch);
-    if (warp == 0) placeTile(s, a.status, tile, a.epoch, a.error);
-    colorSurvivors<D>(s, cam, a.splats, a.sh, a.shStride, a.parts);
-    __syncthreads();
+    compactTile(s, a.status, tile, a.epoch, a.error);
     if (tile == tiles - 1 && threadIdx.x == 0) *a.visibleCount = s.tileBase + s.tileCount;
     copyOutTile(s, a.keys, a.projected, a.spans, cam.screenSize[0], cam.screenSize[1], a.tilesX,
                 a.tilesY, digits, a.sortPasses);
@@ -579,10 +517,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     };
     projectTile<D, true>(s, cam, view.splats, view.sh, view.shStride, PartLabels{}, first, v << 16,
                          indexOf);
-    rankTile(s, a.status, item, a.epoch);
-    if (warp == 0) placeTile(s, a.status, item, a.epoch, a.error);
-    colorSurvivors<D>(s, cam, view.splats, view.sh, view.shStride, PartLabels{});
-    __syncthreads();
+    compactTile(s, a.status, item, a.epoch, a.error);
     if (threadIdx.x == 0) {
       if (chunk == 0) a.viewFirst[v] = s.tileBase;
       if (item == a.items - 1) {
