@@ -407,8 +407,9 @@ typedef struct {
 sk_status sk_server_create(const sk_server_config* config, sk_server** out);
 void sk_server_destroy(sk_server* server);
 const char* sk_server_last_error(const sk_server* server);
-/* Adds the context's resident world as a scene; the context must outlive the server and keep
- * its world while the server runs. */
+/* Adds the context's resident world (flat or LOD) as a scene; the context must outlive the
+ * server and keep its world while the server runs, and is not drawn with directly meanwhile (the
+ * server's thread adapts a LOD scene's threshold in it). */
 sk_status sk_server_add_scene(sk_server* server, sk_context* world, uint32_t* scene);
 /* Queues a request (any thread); its arrival time is now. */
 sk_status sk_server_submit(sk_server* server, const sk_request* request, uint64_t* id);
