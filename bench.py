@@ -629,9 +629,9 @@ def measure_batch(renderer):
             "plain_views_per_s": plain_rate, "batched_views_per_s": batch_rate,
             "speedup": batch_rate / plain_rate, "batched_gpu_ms_per_submission": gpu_ms,
             "images_identical": bool(same), "autotuned": tuning,
-            "how": "plain: resize + draw + read_image per view; batched: autotuned (emission, "
-                   "radix tile, lanes of 3), then 8 submissions of 64 views, CUDA-graph replay, "
-                   "every image copied back; host-timed"}
+            "how": "plain: resize + draw + read_image per view; batched: autotuned (cell-list "
+                   "construction, emission, radix tile, lanes of 3), then 8 submissions of 64 views, "
+                   "CUDA-graph replay, every image copied back; host-timed"}
 
 
 # ---- LOD walk: 6M leaves in 2000 clusters, 300 frames at 1920x1080 ----------------------------

@@ -349,11 +349,15 @@ typedef struct {
                                  each warp's tile instances evenly over its lanes */
   uint32_t sort_tile_keys;    /* keys per radix-sort scatter tile: 2048, 4096 or 6144 */
   uint32_t lanes;             /* submissions in flight (<= the batch's lanes) */
+  uint32_t sorted_lists;      /* cell lists: 0 written in place per view where every view has at
+                                 most 4096 binning cells, 1 always by the batch-wide stable sort
+                                 of (cell, splat) pairs */
   double gpu_ms;              /* autotune: device time of the chosen kernels for the sample */
   double views_per_s;         /* autotune: throughput with `lanes` in flight, images read back */
 } sk_batch_tuning;
-/* Times the sample views under every emission strategy and sort tile size (device time), then
- * with 1..lanes submissions in flight (host time, images read back), and keeps the fastest.
+/* Times the sample views under every cell-list construction, emission strategy and sort tile
+ * size (device time), then with 1..lanes submissions in flight (host time, images read back),
+ * and keeps the fastest.
  * Waits for submissions in flight first; their tickets stay readable until their lanes are
  * reused. */
 sk_status sk_batch_autotune(sk_batch* batch, const sk_batch_view* views, uint32_t count,

@@ -255,7 +255,8 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
     mostSources = std::max(mostSources, t.count);
     mostCells = std::max(mostCells, t.binsX * t.binsY);
   }
-  l.directLists = mostCells <= kDirectMaxCells && cellListsConfigure() == cudaSuccess;
+  l.directLists = !tuning.sortedLists && mostCells <= kDirectMaxCells &&
+                  cellListsConfigure() == cudaSuccess;
   if (l.directLists) {
     l.cellGroupsPerView = (mostCells + 31) / 32;
     void* before[3] = {l.cellLists.ptr, l.cellStatus.ptr, l.entryBases.ptr};
@@ -457,6 +458,9 @@ sk_status Batch::enqueue(BatchLane& l) {
     shape.reserve(size_t{l.viewCount} * 4 + 2);
     shape.push_back(l.viewCount);
     shape.push_back(l.shDegree);
+    // the launch shapes it was captured with
+    shape.push_back((uint64_t{tuning.sortTileKeys} << 2) | (tuning.balancedEmit ? 2u : 0u) |
+                    (l.directLists ? 1u : 0u));
     for (uint32_t i = 0; i < l.viewCount; ++i) {
       const BatchView& t = l.table[i];
       shape.push_back(reinterpret_cast<uint64_t>(t.splats));
@@ -754,12 +758,16 @@ sk_status sk_batch_autotune(sk_batch* handle, const sk_batch_view* views, uint32
   for (auto& l : b->lanes) l.busy = false;
   const bool graphs = b->tuning.graphs;
   b->tuning.graphs = false;
-  // 1. kernel shapes, timed on the device: emission strategy x radix tile size
+  // 1. kernel shapes, timed on the device: cell-list construction x emission strategy (which
+  // only the sorted lists use) x radix tile size
   double best = 1e30;
   sk::BatchTuning chosen = b->tuning;
   sk::BatchLane& lane = b->lanes[0];
+  for (const bool sorted : {false, true})
   for (const bool balanced : {false, true}) {
+    if (!sorted && !balanced) continue;  // in-place lists emit no (cell, splat) pairs
     for (const uint32_t tileKeys : {2048u, 4096u, 6144u}) {
+      b->tuning.sortedLists = sorted;
       b->tuning.balancedEmit = balanced;
       b->tuning.sortTileKeys = tileKeys;
       double ms = 0;
@@ -773,11 +781,13 @@ sk_status sk_batch_autotune(sk_batch* handle, const sk_batch_view* views, uint32
       }
       if (ms < best) {
         best = ms;
+        chosen.sortedLists = sorted;
         chosen.balancedEmit = balanced;
         chosen.sortTileKeys = tileKeys;
       }
     }
   }
+  b->tuning.sortedLists = chosen.sortedLists;
   b->tuning.balancedEmit = chosen.balancedEmit;
   b->tuning.sortTileKeys = chosen.sortTileKeys;
   // 2. submissions in flight, timed on the host with every image copied back
@@ -819,6 +829,7 @@ sk_status sk_batch_autotune(sk_batch* handle, const sk_batch_view* views, uint32
   out->emission_balanced = chosen.balancedEmit ? 1u : 0u;
   out->sort_tile_keys = chosen.sortTileKeys;
   out->lanes = bestLanes;
+  out->sorted_lists = chosen.sortedLists ? 1u : 0u;
   out->gpu_ms = best / 2.0;
   out->views_per_s = bestRate;
   return SK_OK;
@@ -832,6 +843,7 @@ sk_status sk_batch_set_tuning(sk_batch* handle, const sk_batch_tuning* t) {
   b->tuning.balancedEmit = t->emission_balanced != 0;
   b->tuning.sortTileKeys = t->sort_tile_keys;
   b->tuning.activeLanes = t->lanes;
+  b->tuning.sortedLists = t->sorted_lists != 0;
   b->nextLane = 0;
   return SK_OK;
 }

@@ -35,6 +35,7 @@ struct BatchTuning {
   bool graphs = false;          // replay captured stage sequences
   bool balancedEmit = true;     // binning emission strategy (BinArgs::balanced)
   uint32_t sortTileKeys = 4096; // keys per radix scatter tile: 2048, 4096 or 6144
+  bool sortedLists = false;     // cell lists by the batch-wide sort even where in place fits
 };
 
 // The selection one LOD view of a submission runs (LodArgs less the lane's scratch).

@@ -137,7 +137,8 @@ class _Completion(ctypes.Structure):
 
 class _BatchTuning(ctypes.Structure):
     _fields_ = [("emission_balanced", ctypes.c_uint32), ("sort_tile_keys", ctypes.c_uint32),
-                ("lanes", ctypes.c_uint32), ("gpu_ms", ctypes.c_double), ("views_per_s", ctypes.c_double)]
+                ("lanes", ctypes.c_uint32), ("sorted_lists", ctypes.c_uint32), ("gpu_ms", ctypes.c_double),
+                ("views_per_s", ctypes.c_double)]
 
 
 class _LodsplatHeader(ctypes.Structure):
@@ -734,8 +735,8 @@ class Batch:
         self._check(self._lib.sk_batch_autotune(self._h, arr, len(views), ctypes.byref(t)), "autotune")
         return {name: getattr(t, name) for name, _ in _BatchTuning._fields_}
 
-    def set_tuning(self, emission_balanced: int, sort_tile_keys: int, lanes: int):
-        t = _BatchTuning(emission_balanced, sort_tile_keys, lanes, 0.0, 0.0)
+    def set_tuning(self, emission_balanced: int, sort_tile_keys: int, lanes: int, sorted_lists: int = 0):
+        t = _BatchTuning(emission_balanced, sort_tile_keys, lanes, sorted_lists, 0.0, 0.0)
         self._check(self._lib.sk_batch_set_tuning(self._h, ctypes.byref(t)), "set_tuning")
 
     def poll(self, ticket: int) -> bool:

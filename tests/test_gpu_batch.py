@@ -170,12 +170,14 @@ def test_batch_rejects_what_it_cannot_draw(worlds, cuda_device):
 def test_every_tuning_draws_the_same_images_and_the_tuner_picks_one(worlds):
     views = views_for(worlds, 6, start_frame=21)
     with sk.Batch(lanes=2, max_views=8) as batch:
-        for balanced in (0, 1):
-            for tile_keys in (2048, 4096, 6144):
-                batch.set_tuning(balanced, tile_keys, 1)
-                ticket = batch.submit(views)
-                check_against_plain(batch, ticket, views)
+        for sorted_lists in (0, 1):
+            for balanced in (0, 1):
+                for tile_keys in (2048, 4096, 6144):
+                    batch.set_tuning(balanced, tile_keys, 1, sorted_lists)
+                    ticket = batch.submit(views)
+                    check_against_plain(batch, ticket, views)
         chosen = batch.autotune(views)
+        assert chosen["sorted_lists"] in (0, 1)
         assert chosen["sort_tile_keys"] in (2048, 4096, 6144)
         assert chosen["emission_balanced"] in (0, 1) and 1 <= chosen["lanes"] <= 2
         assert chosen["gpu_ms"] > 0 and chosen["views_per_s"] > 0
