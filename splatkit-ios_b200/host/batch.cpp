@@ -758,71 +758,80 @@ sk_status sk_batch_autotune(sk_batch* handle, const sk_batch_view* views, uint32
   for (auto& l : b->lanes) l.busy = false;
   const bool graphs = b->tuning.graphs;
   b->tuning.graphs = false;
-  // 1. kernel shapes, timed on the device: cell-list construction x emission strategy (which
-  // only the sorted lists use) x radix tile size
-  double best = 1e30;
-  sk::BatchTuning chosen = b->tuning;
+  // 1. per cell-list construction, its kernel shapes timed on the device: emission strategy
+  // (which only the sorted lists use) x radix tile size
   sk::BatchLane& lane = b->lanes[0];
-  for (const bool sorted : {false, true})
-  for (const bool balanced : {false, true}) {
-    if (!sorted && !balanced) continue;  // in-place lists emit no (cell, splat) pairs
-    for (const uint32_t tileKeys : {2048u, 4096u, 6144u}) {
-      b->tuning.sortedLists = sorted;
-      b->tuning.balancedEmit = balanced;
-      b->tuning.sortTileKeys = tileKeys;
-      double ms = 0;
-      for (int rep = 0; rep < 3; ++rep) {  // the first run allocates and warms up
-        const sk_status st = runOnce(*b, lane, views, count);
+  sk::BatchTuning shapes[2] = {b->tuning, b->tuning};
+  double deviceMs[2] = {1e30, 1e30};
+  for (int sorted = 0; sorted < 2; ++sorted) {
+    for (const bool balanced : {false, true}) {
+      if (!sorted && !balanced) continue;  // in-place lists emit no (cell, splat) pairs
+      for (const uint32_t tileKeys : {2048u, 4096u, 6144u}) {
+        b->tuning.sortedLists = sorted != 0;
+        b->tuning.balancedEmit = balanced;
+        b->tuning.sortTileKeys = tileKeys;
+        double ms = 0;
+        for (int rep = 0; rep < 3; ++rep) {  // the first run allocates and warms up
+          const sk_status st = runOnce(*b, lane, views, count);
+          if (st != SK_OK) {
+            b->tuning.graphs = graphs;
+            return st;
+          }
+          if (rep > 0) ms += lane.gpuMs;
+        }
+        if (ms < deviceMs[sorted]) {
+          deviceMs[sorted] = ms;
+          shapes[sorted] = b->tuning;
+        }
+      }
+    }
+  }
+  // 2. per construction, 1..lanes submissions in flight, timed on the host with every image
+  // copied back (the constructions load the device differently when lanes overlap)
+  double bestRate = 0;
+  uint32_t bestLanes = 1;
+  sk::BatchTuning chosen = shapes[0];
+  double best = deviceMs[0];
+  for (int sorted = 0; sorted < 2; ++sorted) {
+    b->tuning.sortedLists = shapes[sorted].sortedLists;
+    b->tuning.balancedEmit = shapes[sorted].balancedEmit;
+    b->tuning.sortTileKeys = shapes[sorted].sortTileKeys;
+    for (uint32_t n = 1; n <= b->lanes.size(); ++n) {
+      b->tuning.activeLanes = n;
+      b->nextLane = 0;
+      for (uint32_t k = 0; k < n; ++k) {  // every lane allocates and warms up untimed
+        const sk_status st = runOnce(*b, b->lanes[k], views, count);
         if (st != SK_OK) {
           b->tuning.graphs = graphs;
           return st;
         }
-        if (rep > 0) ms += lane.gpuMs;
       }
-      if (ms < best) {
-        best = ms;
-        chosen.sortedLists = sorted;
-        chosen.balancedEmit = balanced;
-        chosen.sortTileKeys = tileKeys;
+      const uint32_t rounds = 3 * n + 3;
+      std::vector<uint64_t> tickets;
+      const auto t0 = std::chrono::steady_clock::now();
+      for (uint32_t k = 0; k < rounds; ++k) {
+        uint64_t t = 0;
+        const sk_status st = sk_batch_submit(handle, views, count, &t);
+        if (st != SK_OK) {
+          b->tuning.graphs = graphs;
+          return st;
+        }
+        tickets.push_back(t);
+      }
+      for (uint32_t k = rounds - std::min(rounds, n); k < rounds; ++k) sk_batch_wait(handle, tickets[k]);
+      const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      const double rate = rounds * count / s;
+      if (rate > bestRate * 1.03) {  // more lanes, or the other construction, only when clearly faster
+        bestRate = rate;
+        bestLanes = n;
+        chosen = shapes[sorted];
+        best = deviceMs[sorted];
       }
     }
   }
   b->tuning.sortedLists = chosen.sortedLists;
   b->tuning.balancedEmit = chosen.balancedEmit;
   b->tuning.sortTileKeys = chosen.sortTileKeys;
-  // 2. submissions in flight, timed on the host with every image copied back
-  double bestRate = 0;
-  uint32_t bestLanes = 1;
-  for (uint32_t n = 1; n <= b->lanes.size(); ++n) {
-    b->tuning.activeLanes = n;
-    b->nextLane = 0;
-    for (uint32_t k = 0; k < n; ++k) {  // every lane allocates and warms up untimed
-      const sk_status st = runOnce(*b, b->lanes[k], views, count);
-      if (st != SK_OK) {
-        b->tuning.graphs = graphs;
-        return st;
-      }
-    }
-    const uint32_t rounds = 3 * n + 3;
-    std::vector<uint64_t> tickets;
-    const auto t0 = std::chrono::steady_clock::now();
-    for (uint32_t k = 0; k < rounds; ++k) {
-      uint64_t t = 0;
-      const sk_status st = sk_batch_submit(handle, views, count, &t);
-      if (st != SK_OK) {
-        b->tuning.graphs = graphs;
-        return st;
-      }
-      tickets.push_back(t);
-    }
-    for (uint32_t k = rounds - std::min(rounds, n); k < rounds; ++k) sk_batch_wait(handle, tickets[k]);
-    const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    const double rate = rounds * count / s;
-    if (rate > bestRate * 1.03) {  // more lanes only when clearly faster
-      bestRate = rate;
-      bestLanes = n;
-    }
-  }
   b->tuning.activeLanes = bestLanes;
   b->tuning.graphs = graphs;
   b->nextLane = 0;
