@@ -12,6 +12,10 @@
 //      starts each cell after warps 0..w-1, then each warp walks its output 32 entries at a time
 //      in depth order and writes each entry at its cell's next slot (lanes of one round that
 //      share a cell take consecutive slots).
+// A batch of views runs each pass once for all of them (launchCellListsBatch): every block finds
+// its view in a table (its first count/emit block and first cell group), works on that view's
+// ranks, cells and workspace rows, and the look-back of pass 2 runs over the groups of all views
+// in order, so each view's entries start where the previous view's end.
 // Entries of a cell therefore appear in depth order, which is exactly what the stable sort
 // gives.
 #include <cuda_runtime.h>
@@ -37,24 +41,24 @@ constexpr uint32_t kScanWarps = kScanThreads / 32;
 constexpr uint32_t kRowsInRegisters = 32;         // block rows one scan warp keeps
 
 struct Work {
-  uint32_t* blockCounts;  // blocks x cells
-  uint32_t* blockStarts;  // blocks x cells: the block's first slot in each cell's list
-  uint64_t* status;       // one look-back word per group of 32 cells
-  const uint32_t* rankRange;  // a batch view's ranks (CellLists), else null
-  uint32_t* entryBase;
+  uint32_t* blockRows;  // blocks x cells: each block's count per cell, then (after pass 2) its
+                        // first slot in each cell's list
+  uint64_t* status;     // one look-back word per group of 32 cells
+  // a whole batch in one launch (views non-null): the view table, each view's ranks
+  // [viewFirst[v], viewFirst[v + 1]) of args.order, and the workspace its rows are in
+  const CellListView* views;
+  uint32_t viewCount;
+  const uint32_t* viewFirst;
+  uint8_t* base;
 };
 
-// The ranks the lists are built from: [first, first + n) of the depth order.
-__device__ __forceinline__ void ranksOf(const BinArgs& a, const Work& w, uint32_t& first,
-                                        uint32_t& n) {
-  if (w.rankRange) {
-    first = w.rankRange[0];
-    n = min(w.rankRange[1] - first, a.capacity);
-  } else {
-    first = 0;
-    n = min(*a.count, a.capacity);
-  }
-}
+// What one block of a pass works on: its block (or cell group) within its view, the view's ranks
+// [first, first + n) of the depth order, cells, workspace rows and cell ranges.
+struct Job {
+  uint32_t block, first, n, cells, tilesX;
+  uint32_t* blockRows;
+  uint2* ranges;
+};
 
 __host__ __device__ inline uint32_t cellWords(uint32_t cells) { return (cells + 1) / 2; }
 __host__ __device__ inline size_t align16(size_t n) { return (n + 15) & ~size_t{15}; }
@@ -63,19 +67,48 @@ __host__ __device__ inline uint32_t blocksFor(uint32_t capacity) {
   return (capacity + kBlockRanks - 1) / kBlockRanks;
 }
 
+// The job of block (or cell group, byGroup) `index` of a pass.
+__device__ __forceinline__ Job jobOf(const BinArgs& a, const Work& w, uint32_t cells,
+                                     uint32_t index, bool byGroup, uint2* ranges) {
+  Job j;
+  if (!w.views) {  // a frame: the ranks [0, count) of the depth order
+    j.block = index;
+    j.first = 0;
+    j.n = min(*a.count, a.capacity);
+    j.cells = cells;
+    j.tilesX = a.tilesX;
+    j.blockRows = w.blockRows;
+    j.ranges = ranges;
+    return j;
+  }
+  uint32_t lo = 0, hi = w.viewCount;  // the last view whose first block (group) is <= index
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    const uint32_t start = byGroup ? w.views[mid].groupBase : w.views[mid].blockBase;
+    if (start <= index) lo = mid; else hi = mid;
+  }
+  const CellListView v = w.views[lo];
+  j.block = index - (byGroup ? v.groupBase : v.blockBase);
+  j.first = w.viewFirst[lo];
+  j.n = min(w.viewFirst[lo + 1] - j.first, v.capacity);
+  j.cells = v.cells;
+  j.tilesX = v.tilesX;
+  j.blockRows = reinterpret_cast<uint32_t*>(w.base + v.work);
+  j.ranges = ranges + v.binBase;
+  return j;
+}
+
 __host__ __device__ inline Work workOf(void* workspace, uint32_t blocks, uint32_t cells) {
   uint8_t* p = static_cast<uint8_t*>(workspace);
   Work w{};
-  w.blockCounts = reinterpret_cast<uint32_t*>(p);
-  p += align16(size_t{blocks} * cells * 4);
-  w.blockStarts = reinterpret_cast<uint32_t*>(p);
+  w.blockRows = reinterpret_cast<uint32_t*>(p);
   p += align16(size_t{blocks} * cells * 4);
   w.status = reinterpret_cast<uint64_t*>(p);
   return w;
 }
 
 size_t workBytes(uint32_t blocks, uint32_t cells) {
-  return 2 * align16(size_t{blocks} * cells * 4) + size_t{cellGroups(cells)} * 8;
+  return align16(size_t{blocks} * cells * 4) + size_t{cellGroups(cells)} * 8;
 }
 
 // Pass 1: each block's instances per cell.
@@ -83,10 +116,11 @@ __global__ void __launch_bounds__(kThreads)
     cellCountKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells) {
   chainedKernelStart();
   __shared__ uint32_t hist[kDirectMaxCells];
-  uint32_t first, n;
-  ranksOf(a, work, first, n);
-  const uint32_t* order = a.order + first;
-  const uint32_t begin = blockIdx.x * kBlockRanks;
+  const Job job = jobOf(a, work, cells, blockIdx.x, false, nullptr);
+  const uint32_t n = job.n;
+  cells = job.cells;
+  const uint32_t* order = a.order + job.first;
+  const uint32_t begin = job.block * kBlockRanks;
   if (begin >= n) return;  // rows of idle blocks are never read
   for (uint32_t c = threadIdx.x; c < cells; c += kThreads) hist[c] = 0;
   __syncthreads();
@@ -102,9 +136,9 @@ __global__ void __launch_bounds__(kThreads)
     span[r] = value[r] != 0xffffffffu ? __ldg(a.spans + value[r]) : make_uint4(0, 0, 0, 0);
 #pragma unroll
   for (uint32_t r = 0; r < kItems; ++r)
-    visitCells(span[r], a.tilesX, [](uint32_t c) { atomicAdd(&hist[c], 1u); });
+    visitCells(span[r], job.tilesX, [](uint32_t c) { atomicAdd(&hist[c], 1u); });
   __syncthreads();
-  uint32_t* row = work.blockCounts + size_t{blockIdx.x} * cells;
+  uint32_t* row = job.blockRows + size_t{job.block} * cells;
   for (uint32_t c = threadIdx.x; c < cells; c += kThreads) row[c] = hist[c];
 }
 
@@ -117,28 +151,27 @@ __global__ void __launch_bounds__(kScanThreads, 1)
   chainedKernelStart();
   __shared__ uint32_t part[kScanWarps][33];
   __shared__ uint32_t cellStart[32];
-  const uint32_t group = takeTile(counters);
-  uint32_t first, n;
-  ranksOf(a, work, first, n);
-  const uint32_t viewBase = work.entryBase ? work.entryBase[0] : 0u;
-  const uint32_t active = blocksFor(n);
+  const uint32_t group = takeTile(counters);  // over all views of a batch
+  const Job job = jobOf(a, work, cells, group, true, ranges);
+  cells = job.cells;
+  const uint32_t active = blocksFor(job.n);
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
-  const uint32_t cell = group * 32 + lane;
+  const uint32_t cell = job.block * 32 + lane;
   const bool valid = cell < cells;
   const uint32_t share = (active + kScanWarps - 1) / kScanWarps;
   const uint32_t r0 = min(warp * share, active), r1 = min(r0 + share, active);
-  const uint32_t* counts = work.blockCounts + cell;
+  uint32_t* rows = job.blockRows + cell;
   uint32_t v[kRowsInRegisters];
   uint32_t sum = 0;
 #pragma unroll
   for (uint32_t k = 0; k < kRowsInRegisters; ++k) {
     const uint32_t row = r0 + k;
-    v[k] = valid && row < r1 ? __ldcg(counts + size_t{row} * cells) : 0u;
+    v[k] = valid && row < r1 ? __ldcg(rows + size_t{row} * cells) : 0u;
     sum += v[k];
   }
   if (valid)
     for (uint32_t row = r0 + kRowsInRegisters; row < r1; ++row)
-      sum += __ldcg(counts + size_t{row} * cells);
+      sum += __ldcg(rows + size_t{row} * cells);
   part[warp][lane] = sum;
   __syncthreads();
   uint32_t run = 0;
@@ -162,35 +195,30 @@ __global__ void __launch_bounds__(kScanThreads, 1)
       if (lane == 0)
         storeStatus(work.status + group, makeStatus(epoch, kFlagPrefix, before + aggregate));
     }
-    const uint32_t start = viewBase + before + inc - total;
+    const uint32_t start = before + inc - total;
     cellStart[lane] = start;
     if (valid)
-      ranges[cell] = make_uint2(min(start, a.instanceCapacity),
-                                min(start + total, a.instanceCapacity));
+      job.ranges[cell] = make_uint2(min(start, a.instanceCapacity),
+                                    min(start + total, a.instanceCapacity));
     if (group == gridDim.x - 1 && lane == 31) {
-      const uint32_t entries = viewBase + before + aggregate;
+      const uint32_t entries = before + aggregate;
       *a.instanceCount = entries;
-      if (work.entryBase) {
-        work.entryBase[1] = entries;
-        if (entries > a.instanceCapacity) *a.overflow = 1u;
-      } else {
-        *a.overflow = entries > a.instanceCapacity ? 1u : 0u;
-      }
+      *a.overflow = entries > a.instanceCapacity ? 1u : 0u;
     }
   }
   __syncthreads();
-  if (valid) {
+  if (valid) {  // each count becomes the block's first slot in the cell, in place
     run += cellStart[lane];
-    uint32_t* starts = work.blockStarts + cell;
 #pragma unroll
     for (uint32_t k = 0; k < kRowsInRegisters; ++k) {
       const uint32_t row = r0 + k;
-      if (row < r1) starts[size_t{row} * cells] = run;
+      if (row < r1) rows[size_t{row} * cells] = run;
       run += v[k];
     }
     for (uint32_t row = r0 + kRowsInRegisters; row < r1; ++row) {
-      starts[size_t{row} * cells] = run;
-      run += __ldcg(counts + size_t{row} * cells);
+      const uint32_t count = __ldcg(rows + size_t{row} * cells);
+      rows[size_t{row} * cells] = run;
+      run += count;
     }
   }
   finishTile(counters);
@@ -207,16 +235,17 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ uint32_t stageValue[kWarps][kChunk];
   __shared__ uint32_t stageOffset[kWarps][kChunk];
   __shared__ uint32_t startItem[kWarps][32];
-  uint32_t first, n;
-  ranksOf(a, work, first, n);
-  const uint32_t* order = a.order + first;
-  const uint32_t begin = blockIdx.x * kBlockRanks;
+  const Job job = jobOf(a, work, cells, blockIdx.x, false, nullptr);
+  const uint32_t n = job.n, tilesX = job.tilesX;
+  cells = job.cells;
+  const uint32_t* order = a.order + job.first;
+  const uint32_t begin = job.block * kBlockRanks;
   if (begin >= n) return;
   const uint32_t words = cellWords(cells);
   uint32_t* slots = cellSmem;
   uint32_t* where = cellSmem + kWarps * words;
   for (uint32_t i = threadIdx.x; i < kWarps * words; i += kThreads) slots[i] = 0;
-  const uint32_t* starts = work.blockStarts + size_t{blockIdx.x} * cells;
+  const uint32_t* starts = job.blockRows + size_t{job.block} * cells;
   for (uint32_t c = threadIdx.x; c < cells; c += kThreads) where[c] = __ldcg(starts + c);
   __syncthreads();
 
@@ -236,7 +265,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (uint32_t r = 0; r < kItems; ++r) {
     span[r] = value[r] != 0xffffffffu ? __ldg(a.spans + value[r]) : make_uint4(0, 0, 0, 0);
-    visitCells(span[r], a.tilesX,
+    visitCells(span[r], tilesX,
                [mine](uint32_t c) { atomicAdd(mine + (c >> 1), 1u << ((c & 1u) * 16)); });
   }
   // the warp's items in (row, lane) order = depth order, with their first output position
@@ -304,7 +333,7 @@ __global__ void __launch_bounds__(kThreads)
     const bool valid = p < total;
     uint32_t cell = 0xffffffffu, val = 0;
     if (valid) {
-      cell = spanCell(sSpan[item], p - itemStart, a.tilesX);
+      cell = spanCell(sSpan[item], p - itemStart, tilesX);
       val = sValue[item];
     }
     // lanes of this round with the same cell: 13 ballots (cells are below 4096; an idle lane's
@@ -357,10 +386,7 @@ cudaError_t launchCellLists(const BinArgs& a, const CellLists& lists, cudaStream
   cudaError_t e = cellListsConfigure();
   if (e != cudaSuccess) return e;
   const uint32_t blocks = blocksFor(a.capacity);
-  Work work = workOf(lists.workspace, blocks, cells);
-  if (lists.status) work.status = lists.status;
-  work.rankRange = lists.rankRange;
-  work.entryBase = lists.entryBase;
+  const Work work = workOf(lists.workspace, blocks, cells);
   e = launchChained(cellCountKernel, blocks, kThreads, stream, a, work, cells);
   if (e != cudaSuccess) return e;
   e = launchChained(cellScanKernel, cellGroups(cells), kScanThreads, stream, a, work, cells,
@@ -368,6 +394,34 @@ cudaError_t launchCellLists(const BinArgs& a, const CellLists& lists, cudaStream
   if (e != cudaSuccess) return e;
   return launchChainedShared(cellEmitKernel, blocks, kThreads, emitDynamicBytes(cells), stream, a,
                              work, cells);
+}
+
+uint32_t cellListBlocks(uint32_t capacity) { return blocksFor(std::max(capacity, 1u)); }
+
+size_t cellListRowBytes(uint32_t capacity, uint32_t cells) {
+  return align16(size_t{cellListBlocks(capacity)} * cells * 4);
+}
+
+cudaError_t launchCellListsBatch(const BinArgs& a, const CellListBatch& lists, cudaStream_t stream) {
+  if (lists.viewCount == 0 || lists.blocks == 0 || lists.groups == 0 || lists.mostCells == 0 ||
+      lists.mostCells > kDirectMaxCells)
+    return cudaErrorInvalidValue;
+  cudaError_t e = cellListsConfigure();
+  if (e != cudaSuccess) return e;
+  Work work{};
+  work.status = lists.status;
+  work.views = lists.views;
+  work.viewCount = lists.viewCount;
+  work.viewFirst = lists.viewFirst;
+  work.base = static_cast<uint8_t*>(lists.workspace);
+  const uint32_t cells = lists.mostCells;  // each block reads its own view's from the table
+  e = launchChained(cellCountKernel, lists.blocks, kThreads, stream, a, work, cells);
+  if (e != cudaSuccess) return e;
+  e = launchChained(cellScanKernel, lists.groups, kScanThreads, stream, a, work, cells,
+                    lists.ranges, lists.counters, lists.epoch, lists.error);
+  if (e != cudaSuccess) return e;
+  return launchChainedShared(cellEmitKernel, lists.blocks, kThreads, emitDynamicBytes(cells),
+                             stream, a, work, cells);
 }
 
 }  // namespace sk

@@ -159,18 +159,39 @@ struct CellLists {
   uint32_t* counters;   // two words, zero before the first launch (each launch restores them)
   uint32_t epoch;       // look-back epoch, fresh per launch
   uint32_t* error;      // SK_DEVERR_* bits
-  // One view of a batch (null for a plain frame): its ranks are [rankRange[0], rankRange[1]) of
-  // args.order (args.capacity bounds their count), its entries follow entryBase[0] earlier ones
-  // (the entry count after it is written to entryBase[1], args.overflow only set), and its
-  // look-back words are `status` (one per group of 32 cells, cleared before the batch).
-  const uint32_t* rankRange;
-  uint32_t* entryBase;
-  uint64_t* status;
 };
 // Whether a target of `cells` cells takes the direct path.
 bool cellListsFit(uint32_t capacity, uint32_t cells);
 size_t cellListBytes(uint32_t capacity, uint32_t cells);
 cudaError_t launchCellLists(const BinArgs& args, const CellLists& lists, cudaStream_t stream);
+
+// Every view of a batch in one launch per pass. View v's ranks are [viewFirst[v], viewFirst[v+1])
+// of args.order (at most `capacity` of them), its cells binBase .. binBase + cells of the batch's
+// ranges; its count/emit blocks are blockBase .. blockBase + blocks (cellListBlocks(capacity)),
+// its cell groups groupBase .. groupBase + (cells + 31) / 32, and its block rows the
+// cellListRowBytes(capacity, cells) bytes at workspace + work. The look-back runs over the groups
+// of all views in view order, so view v's entries follow those of views 0..v-1; args.instanceCount
+// receives the total and args.overflow whether it exceeds args.instanceCapacity.
+struct CellListView {
+  uint32_t blockBase, groupBase, cells, tilesX;
+  uint32_t binBase, capacity, blocks, pad;
+  uint64_t work;
+};
+struct CellListBatch {
+  const CellListView* views;  // device table, views in order
+  uint32_t viewCount;
+  const uint32_t* viewFirst;  // viewCount + 1 rank offsets (device)
+  void* workspace;            // the views' block rows, no clearing needed
+  uint64_t* status;           // one look-back word per cell group of the batch, zero beforehand
+  uint2* ranges;              // the batch's cells
+  uint32_t* counters;         // two words, zero before the first launch (each launch restores them)
+  uint32_t epoch;
+  uint32_t* error;
+  uint32_t blocks, groups, mostCells;  // totals over the views; the largest view's cells
+};
+uint32_t cellListBlocks(uint32_t capacity);
+size_t cellListRowBytes(uint32_t capacity, uint32_t cells);
+cudaError_t launchCellListsBatch(const BinArgs& args, const CellListBatch& lists, cudaStream_t stream);
 // Sets the emission kernel's shared-memory limit (once; before any stream capture).
 cudaError_t cellListsConfigure();
 

@@ -250,21 +250,41 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
     }
   }
   // Every view's lists written in place when each has at most kDirectMaxCells cells.
-  uint32_t mostSources = 1, mostCells = 1;
-  for (const BatchView& t : l.table) {
-    mostSources = std::max(mostSources, t.count);
-    mostCells = std::max(mostCells, t.binsX * t.binsY);
-  }
+  uint32_t mostCells = 1;
+  for (const BatchView& t : l.table) mostCells = std::max(mostCells, t.binsX * t.binsY);
   l.directLists = !tuning.sortedLists && mostCells <= kDirectMaxCells &&
                   cellListsConfigure() == cudaSuccess;
   if (l.directLists) {
-    l.cellGroupsPerView = (mostCells + 31) / 32;
-    void* before[3] = {l.cellLists.ptr, l.cellStatus.ptr, l.entryBases.ptr};
-    cudaError_t e = l.cellLists.allocate(cellListBytes(mostSources, mostCells));
-    if (e == cudaSuccess) e = l.cellStatus.allocate(size_t{count} * l.cellGroupsPerView * 8);
-    if (e == cudaSuccess) e = l.entryBases.allocate(size_t{count + 1} * 4);
+    // view v's count/emit blocks, cell groups and block rows follow those of views 0..v-1
+    CellListBatch& cb = l.cellBatch;
+    cb = CellListBatch{};
+    cb.viewCount = count;
+    cb.mostCells = mostCells;
+    std::vector<CellListView> cellViews(count);
+    uint64_t rowBytes = 0;
+    for (uint32_t v = 0; v < count; ++v) {
+      const BatchView& t = l.table[v];
+      CellListView& c = cellViews[v];
+      c.capacity = std::max(t.count, 1u);
+      c.cells = t.binsX * t.binsY;
+      c.tilesX = t.binsX;
+      c.binBase = t.binBase;
+      c.blocks = cellListBlocks(c.capacity);
+      c.blockBase = cb.blocks;
+      c.groupBase = cb.groups;
+      c.work = rowBytes;
+      cb.blocks += c.blocks;
+      cb.groups += (c.cells + 31) / 32;
+      rowBytes += cellListRowBytes(c.capacity, c.cells);
+    }
+    void* before[3] = {l.cellLists.ptr, l.cellStatus.ptr, l.cellViews.ptr};
+    cudaError_t e = l.cellLists.allocate(rowBytes);
+    if (e == cudaSuccess) e = l.cellStatus.allocate(size_t{cb.groups} * 8);
+    if (e == cudaSuccess) e = l.cellViews.allocate(size_t{count} * sizeof(CellListView));
+    if (e == cudaSuccess) e = l.hostCellViews.allocate(size_t{count} * sizeof(CellListView));
     if (e != cudaSuccess) return check(e, "batch cell lists");
-    if (before[0] != l.cellLists.ptr || before[1] != l.cellStatus.ptr || before[2] != l.entryBases.ptr) {
+    std::memcpy(l.hostCellViews.ptr, cellViews.data(), size_t{count} * sizeof(CellListView));
+    if (before[0] != l.cellLists.ptr || before[1] != l.cellStatus.ptr || before[2] != l.cellViews.ptr) {
       if (l.graph) cudaGraphExecDestroy(l.graph);  // a captured graph points at the old buffers
       l.graph = nullptr;
       l.graphShape.clear();
@@ -288,11 +308,12 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
   if (e == cudaSuccess && !l.directLists)
     e = clearTileRanges(static_cast<uint2*>(l.ranges.ptr), l.totalBins, s);
   if (e == cudaSuccess && l.directLists) {
-    // each view's entries start where the previous view's end; its cell groups' look-back words
-    // must read "not ready" (a replayed graph reuses its epochs)
-    e = cudaMemsetAsync(l.entryBases.ptr, 0, size_t{l.viewCount + 1} * 4, s);
+    // the look-back words of the batch's cell groups must read "not ready" (a replayed graph
+    // reuses its epochs); the view table goes up with the other tables
+    e = cudaMemsetAsync(l.cellStatus.ptr, 0, size_t{l.cellBatch.groups} * 8, s);
     if (e == cudaSuccess)
-      e = cudaMemsetAsync(l.cellStatus.ptr, 0, size_t{l.viewCount} * l.cellGroupsPerView * 8, s);
+      e = cudaMemcpyAsync(l.cellViews.ptr, l.hostCellViews.ptr,
+                          size_t{l.viewCount} * sizeof(CellListView), cudaMemcpyHostToDevice, s);
   }
   if (e == cudaSuccess && clearStatus) {
     e = cudaMemsetAsync(l.visStatus.ptr, 0, size_t{l.totalItems} * 8, s);
@@ -365,31 +386,29 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     a.error = error;
     e = launchSort(a, s);
   }
-  for (uint32_t v = 0; e == cudaSuccess && l.directLists && v < l.viewCount; ++v) {
-    // view v's ranks are order[viewFirst[v] .. viewFirst[v + 1]) (views in order by the key's
-    // high bits), its cells binBase .. binBase + binsX * binsY of the batch
-    const BatchView& t = l.table[v];
+  if (e == cudaSuccess && l.directLists) {
+    // every view's lists in one launch per pass: view v's ranks are order[viewFirst[v] ..
+    // viewFirst[v + 1]) (views in order by the key's high bits), its cells binBase .. binBase +
+    // binsX * binsY of the batch
     BinArgs b{};
     b.spans = static_cast<const uint4*>(l.spans.ptr);
     b.order = static_cast<const uint32_t*>(l.order.ptr);
     b.count = &fc->visible;
-    b.capacity = std::max(t.count, 1u);
-    b.width = t.width, b.height = t.height, b.tilesX = t.binsX, b.tilesY = t.binsY;
+    b.capacity = l.sources;
     b.instanceValues = static_cast<uint32_t*>(l.instValuesSorted.ptr);
     b.instanceCapacity = l.instances;
     b.instanceCount = &fc->instances;
     b.overflow = &fc->overflow;
-    CellLists cl{};
-    cl.cells = t.binsX * t.binsY;
+    CellListBatch cl = l.cellBatch;
+    cl.views = static_cast<const CellListView*>(l.cellViews.ptr);
+    cl.viewFirst = viewFirst;
     cl.workspace = l.cellLists.ptr;
-    cl.ranges = static_cast<uint2*>(l.ranges.ptr) + t.binBase;
+    cl.status = static_cast<uint64_t*>(l.cellStatus.ptr);
+    cl.ranges = static_cast<uint2*>(l.ranges.ptr);
     cl.counters = counters + 8;
     cl.epoch = nextEpoch(1);
     cl.error = error;
-    cl.rankRange = viewFirst + v;
-    cl.entryBase = static_cast<uint32_t*>(l.entryBases.ptr) + v;
-    cl.status = static_cast<uint64_t*>(l.cellStatus.ptr) + size_t{v} * l.cellGroupsPerView;
-    e = launchCellLists(b, cl, s);
+    e = launchCellListsBatch(b, cl, s);
   }
   if (e == cudaSuccess && !l.directLists) {
     BinArgs b{};

@@ -58,11 +58,12 @@ struct BatchLane {
   DeviceBuffer keys, projected, spans, order, sortWorkspace, visStatus, binSums;
   DeviceBuffer instKeys, instValues, instKeysSorted, instValuesSorted, tileSortWorkspace;
   DeviceBuffer ranges, viewFirst, counters, frameCounters, viewTable, cameras, image;
-  // direct cell lists (every view at most kDirectMaxCells cells): one workspace reused view
-  // after view, per view the look-back words of its cell groups, and each view's first entry
-  DeviceBuffer cellLists, cellStatus, entryBases;
+  // direct cell lists (every view at most kDirectMaxCells cells), all views in one launch per
+  // pass: every view's block rows, the look-back words of the batch's cell groups, the view
+  // table (host copy in hostCellViews) and its totals
+  DeviceBuffer cellLists, cellStatus, cellViews;
   bool directLists = false;
-  uint32_t cellGroupsPerView = 0;
+  CellListBatch cellBatch{};
   // LOD views: every view's cut, each view's six report words (LodState's first six), and the
   // selection scratch the views share in turn (sized for the largest)
   DeviceBuffer lodIndices, lodReports, lodFrontier[2], lodCosts, lodOffsets, lodPackets, lodState,
@@ -70,7 +71,8 @@ struct BatchLane {
   uint32_t lodIndexCapacity = 0, lodFrontierCapacity = 0, lodReportViews = 0;
   std::vector<LodPlan> lodPlans;
   // pinned host
-  PinnedBuffer hostViews, hostCameras, hostCounters, hostViewFirst, hostImage, hostLodReports;
+  PinnedBuffer hostViews, hostCameras, hostCounters, hostViewFirst, hostImage, hostLodReports,
+      hostCellViews;
   // the submission it holds
   uint64_t ticket = 0;
   bool busy = false, harvested = true;
