@@ -224,17 +224,51 @@ __global__ void __launch_bounds__(kScanThreads, 1)
   finishTile(counters);
 }
 
+// visit(cell, position, item) for every cell of the warp's items whose position offset + k lies
+// in [lo, hi); k numbers a span's cells as spanCell does (mask bits upward, or box order), item
+// is itemBase + the owning lane. A masked span is walked by its own lane, a box of more than 64
+// cells by the whole warp. Every lane calls this.
+template <typename Visit>
+__device__ __forceinline__ void visitPositions(const uint4 s, uint32_t tilesX, uint32_t offset,
+                                               uint32_t lo, uint32_t hi, uint32_t itemBase,
+                                               Visit visit) {
+  const uint32_t w = s.y & 0xffffu, area = s.y >> 16;
+  const uint32_t first = spanFirstCell(s, tilesX);
+  const uint32_t lane = laneId();
+  if (area <= 64 && offset < hi && offset + __popc(s.z) + __popc(s.w) > lo) {
+    uint32_t pos = offset;
+    for (uint32_t m = s.z; m != 0u; m &= m - 1, ++pos)
+      if (pos >= lo && pos < hi) visit(boxCell(first, __ffs(m) - 1, w, tilesX), pos, itemBase + lane);
+    for (uint32_t m = s.w; m != 0u; m &= m - 1, ++pos)
+      if (pos >= lo && pos < hi) visit(boxCell(first, 31 + __ffs(m), w, tilesX), pos, itemBase + lane);
+  }
+  uint32_t big = __ballot_sync(0xffffffffu, area > 64 && offset < hi && offset + area > lo);
+  while (big != 0u) {
+    const uint32_t src = __ffs(big) - 1;
+    big &= big - 1;
+    const uint32_t bw = __shfl_sync(0xffffffffu, w, src);
+    const uint32_t barea = __shfl_sync(0xffffffffu, area, src);
+    const uint32_t bfirst = __shfl_sync(0xffffffffu, first, src);
+    const uint32_t boff = __shfl_sync(0xffffffffu, offset, src);
+    const uint32_t k0 = lo > boff ? lo - boff : 0u, k1 = min(barea, hi - boff);
+    for (uint32_t k = k0 + lane; k < k1; k += 32) visit(boxCell(bfirst, k, bw, tilesX), boff + k, itemBase + src);
+  }
+}
+
 // Pass 3. Dynamic shared memory: kWarps x words per-warp slot counters (16-bit halves: a warp's
 // slots count from the block's first slot in the cell, at most 1024 on), then each cell's first
-// slot for the block.
+// slot for the block. A warp's entries, in depth order, are staged as (cell, item) pairs kWindow
+// positions at a time: the counting walk stages the first window, and a warp with more entries
+// walks its items again for each further one.
+constexpr uint32_t kWindow = 1024;
+
 __global__ void __launch_bounds__(kThreads)
     cellEmitKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells) {
   chainedKernelStart();
   extern __shared__ uint32_t cellSmem[];
-  __shared__ uint4 stageSpan[kWarps][kChunk];
   __shared__ uint32_t stageValue[kWarps][kChunk];
-  __shared__ uint32_t stageOffset[kWarps][kChunk];
-  __shared__ uint32_t startItem[kWarps][32];
+  __shared__ uint16_t stageCell[kWarps][kWindow];
+  __shared__ uint8_t stageItem[kWarps][kWindow];
   const Job job = jobOf(a, work, cells, blockIdx.x, false, nullptr);
   const uint32_t n = job.n, tilesX = job.tilesX;
   cells = job.cells;
@@ -251,10 +285,9 @@ __global__ void __launch_bounds__(kThreads)
 
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
   uint32_t* mine = slots + warp * words;
-  uint4* sSpan = stageSpan[warp];
   uint32_t* sValue = stageValue[warp];
-  uint32_t* sOffset = stageOffset[warp];
-  uint32_t* sStart = startItem[warp];
+  uint16_t* sCell = stageCell[warp];
+  uint8_t* sItem = stageItem[warp];
   uint32_t value[kItems];
   uint4 span[kItems];
 #pragma unroll
@@ -262,16 +295,13 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t i = begin + warp * kChunk + r * 32 + lane;
     value[r] = i < n ? order[i] : 0xffffffffu;
   }
-#pragma unroll
-  for (uint32_t r = 0; r < kItems; ++r) {
-    span[r] = value[r] != 0xffffffffu ? __ldg(a.spans + value[r]) : make_uint4(0, 0, 0, 0);
-    visitCells(span[r], tilesX,
-               [mine](uint32_t c) { atomicAdd(mine + (c >> 1), 1u << ((c & 1u) * 16)); });
-  }
   // the warp's items in (row, lane) order = depth order, with their first output position
+  uint32_t offset[kItems];
   uint32_t total = 0;
 #pragma unroll
   for (uint32_t r = 0; r < kItems; ++r) {
+    span[r] = value[r] != 0xffffffffu ? __ldg(a.spans + value[r]) : make_uint4(0, 0, 0, 0);
+    sValue[r * 32 + lane] = value[r];
     const uint32_t cnt = spanCount(span[r]);
     uint32_t inc = cnt;
 #pragma unroll
@@ -279,11 +309,20 @@ __global__ void __launch_bounds__(kThreads)
       const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
       if (lane >= static_cast<uint32_t>(o)) inc += up;
     }
-    sSpan[r * 32 + lane] = span[r];
-    sValue[r * 32 + lane] = value[r];
-    sOffset[r * 32 + lane] = total + inc - cnt;
+    offset[r] = total + inc - cnt;
     total += __shfl_sync(0xffffffffu, inc, 31);
   }
+  // count every entry by cell; stage the first window
+#pragma unroll
+  for (uint32_t r = 0; r < kItems; ++r)
+    visitPositions(span[r], tilesX, offset[r], 0u, 0xffffffffu, r * 32,
+                   [mine, sCell, sItem](uint32_t c, uint32_t pos, uint32_t item) {
+                     atomicAdd(mine + (c >> 1), 1u << ((c & 1u) * 16));
+                     if (pos < kWindow) {
+                       sCell[pos] = static_cast<uint16_t>(c);
+                       sItem[pos] = static_cast<uint8_t>(item);
+                     }
+                   });
   __syncthreads();
   // warp w's first slot per cell: the counts of warps 0..w-1 (both halves of a word at once)
   for (uint32_t q = threadIdx.x; q < words; q += kThreads) {
@@ -297,61 +336,47 @@ __global__ void __launch_bounds__(kThreads)
   }
   __syncthreads();
 
-  // Output position p of the warp belongs to the last item whose offset is <= p. Per round of
-  // 32 positions, the items that open inside the round (offset in [p0, p0 + 32) and at least one
-  // entry) mark their offset in a bit mask, and a lane takes the last mark at or before it, or
-  // the item that held the round's first position.
   const uint32_t below = lanemaskLt();
-  int cur = -1;           // the item holding position p0
-  uint32_t curStart = 0;  // its offset
-  for (uint32_t p0 = 0; p0 < total; p0 += 32) {
-    uint32_t opening = 0;
-    for (int base = cur + 1; base < static_cast<int>(kChunk); base += 32) {
-      const int j = base + static_cast<int>(lane);
-      const uint32_t s = j < static_cast<int>(kChunk) ? sOffset[j] : 0xffffffffu;
-      uint32_t next = __shfl_down_sync(0xffffffffu, s, 1);  // the following item's offset
-      if (lane == 31 || j + 1 >= static_cast<int>(kChunk))
-        next = j + 1 < static_cast<int>(kChunk) ? sOffset[j + 1] : total;
-      const bool inside = s < p0 + 32;
-      const bool opens = inside && next > s;
-      if (opens) sStart[s - p0] = static_cast<uint32_t>(j);
-      opening |= __reduce_or_sync(0xffffffffu, opens ? 1u << (s - p0) : 0u);
-      if (!__shfl_sync(0xffffffffu, inside, 31)) break;
-    }
-    __syncwarp();
-    const uint32_t p = p0 + lane;
-    const uint32_t upTo = opening & (0xffffffffu >> (31 - lane));
-    int item = cur;
-    uint32_t itemStart = curStart;
-    if (upTo != 0u) {
-      const uint32_t h = 31 - __clz(upTo);
-      item = static_cast<int>(sStart[h]);
-      itemStart = p0 + h;
-    }
-    cur = __shfl_sync(0xffffffffu, item, 31);
-    curStart = __shfl_sync(0xffffffffu, itemStart, 31);
-    const bool valid = p < total;
-    uint32_t cell = 0xffffffffu, val = 0;
-    if (valid) {
-      cell = spanCell(sSpan[item], p - itemStart, tilesX);
-      val = sValue[item];
-    }
-    // lanes of this round with the same cell: 13 ballots (cells are below 4096; an idle lane's
-    // 0xffffffff differs from every cell in bit 12)
-    uint32_t peers = 0xffffffffu;
+  for (uint32_t w0 = 0; w0 < total; w0 += kWindow) {
+    const uint32_t w1 = min(total, w0 + kWindow);
+    if (w0 > 0) {  // stage the next window (its spans re-read from L2)
+      __syncwarp();
 #pragma unroll
-    for (uint32_t b = 0; b < 13; ++b) {
-      const bool bit = (cell >> b) & 1u;
-      const uint32_t vote = __ballot_sync(0xffffffffu, bit);
-      peers &= bit ? vote : ~vote;
+      for (uint32_t r = 0; r < kItems; ++r) {
+        const uint4 sp = value[r] != 0xffffffffu ? __ldg(a.spans + value[r]) : make_uint4(0, 0, 0, 0);
+        visitPositions(sp, tilesX, offset[r], w0, w1, r * 32,
+                       [sCell, sItem, w0](uint32_t c, uint32_t pos, uint32_t item) {
+                         sCell[pos - w0] = static_cast<uint16_t>(c);
+                         sItem[pos - w0] = static_cast<uint8_t>(item);
+                       });
+      }
     }
-    const uint32_t half = (cell & 1u) * 16;
-    uint32_t slot = 0;
-    if (valid) slot = where[cell] + ((mine[cell >> 1] >> half) & 0xffffu) + __popc(peers & below);
     __syncwarp();
-    if (valid && lane == 31 - __clz(peers)) atomicAdd(mine + (cell >> 1), __popc(peers) << half);
-    __syncwarp();
-    if (valid && slot < a.instanceCapacity) a.instanceValues[slot] = val;
+    for (uint32_t p0 = w0; p0 < w1; p0 += 32) {
+      const uint32_t p = p0 + lane;
+      const bool valid = p < w1;
+      uint32_t cell = 0xffffffffu, val = 0;
+      if (valid) {
+        cell = sCell[p - w0];
+        val = sValue[sItem[p - w0]];
+      }
+      // lanes of this round with the same cell: 13 ballots (cells are below 4096; an idle lane's
+      // 0xffffffff differs from every cell in bit 12)
+      uint32_t peers = 0xffffffffu;
+#pragma unroll
+      for (uint32_t b = 0; b < 13; ++b) {
+        const bool bit = (cell >> b) & 1u;
+        const uint32_t vote = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? vote : ~vote;
+      }
+      const uint32_t half = (cell & 1u) * 16;
+      uint32_t slot = 0;
+      if (valid) slot = where[cell] + ((mine[cell >> 1] >> half) & 0xffffu) + __popc(peers & below);
+      __syncwarp();
+      if (valid && lane == 31 - __clz(peers)) atomicAdd(mine + (cell >> 1), __popc(peers) << half);
+      __syncwarp();
+      if (valid && slot < a.instanceCapacity) a.instanceValues[slot] = val;
+    }
   }
 }
 

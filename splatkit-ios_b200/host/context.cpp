@@ -88,6 +88,7 @@ Context::~Context() {
       if (ev) cudaEventDestroy(ev);
   }
   if (stream) cudaStreamDestroy(stream);
+  if (stream2) cudaStreamDestroy(stream2);
 }
 
 sk_status Context::fail(sk_status code, const std::string& message) {
@@ -437,34 +438,65 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
 }
 
 ViewTarget Context::plainView(const Slot& slot) {
+  const bool second = &slot == &slots[1];
   ViewTarget v;
   v.width = width;
   v.height = height;
   v.image = imageOf(slot.image);
-  v.counters = static_cast<FrameCounters*>(frameCounters.ptr);
+  v.counters = static_cast<FrameCounters*>(second ? frameCounters2.ptr : frameCounters.ptr);
   v.hostCounters = static_cast<FrameCounters*>(slot.hostCounters.ptr);
-  v.camera = static_cast<const Camera*>(camera.ptr);
+  v.camera = static_cast<const Camera*>(second ? camera2.ptr : camera.ptr);
   return v;
 }
 
-// Enqueues the slot's frame. Its pinned camera is free: the frame that used the slot before
-// has finished. The device camera is rewritten after the previous frame's kernels, in stream
-// order.
+sk_status Context::prepareSecondSlot() {
+  cudaError_t e = cudaSuccess;
+  if (!stream2) e = cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = frameCounters2.allocate(sizeof(FrameCounters));
+  if (e == cudaSuccess) e = camera2.allocate(sizeof(Camera));
+  if (e != cudaSuccess) return check(e, "second frame slot");
+  if (!twoImages) {  // the slots' frames must not draw into one image
+    twoImages = true;
+    const sk_status st = reserveView(width, height);
+    if (st != SK_OK) {
+      twoImages = false;
+      return st;
+    }
+  }
+  if (scratch2.sources < scratch.sources || scratch2.instanceCapacity < scratch.instanceCapacity ||
+      scratch2.maxTiles < scratch.maxTiles)
+    return reserveScratch(scratch2, std::max(scratch.sources, scratch2.sources),
+                          std::max(scratch.instanceCapacity, scratch2.instanceCapacity),
+                          scratch.maxTiles, stream2);
+  return SK_OK;
+}
+
+cudaError_t Context::syncStreams() {
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (e == cudaSuccess && stream2) e = cudaStreamSynchronize(stream2);
+  return e;
+}
+
+// Enqueues the slot's frame on the slot's stream. Its pinned camera is free: the frame that used
+// the slot before has finished. The slot's device camera is rewritten after that frame's
+// kernels, in stream order.
 sk_status Context::enqueueSlot(uint32_t index) {
   Slot& slot = slots[index];
+  const cudaStream_t s = streamOf(index);
   *static_cast<Camera*>(slot.hostCamera.ptr) = cameraFor(slot.frame, width, height);
-  cudaError_t e = cudaMemcpyAsync(camera.ptr, slot.hostCamera.ptr, sizeof(Camera),
-                                  cudaMemcpyHostToDevice, stream);
+  const ViewTarget view = plainView(slot);
+  cudaError_t e = cudaMemcpyAsync(const_cast<Camera*>(view.camera), slot.hostCamera.ptr,
+                                  sizeof(Camera), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return check(e, "camera upload");
   // the image this frame draws into may still be on its way to a capture's host buffer
   if (imageCopied[slot.image]) {
-    e = cudaStreamWaitEvent(stream, imageFree[slot.image], 0);
+    e = cudaStreamWaitEvent(s, imageFree[slot.image], 0);
     if (e != cudaSuccess) return check(e, "capture wait");
   }
-  sk_status st = enqueuePipeline(scratch, plainView(slot), slot.frame, slot.total, stream,
-                                 timeStages, slot.events);
+  sk_status st = enqueuePipeline(scratchOf(index), view, slot.frame, slot.total, s, timeStages,
+                                 slot.events);
   if (st != SK_OK) return st;
-  st = check(cudaEventRecord(slot.done, stream), "frame");
+  st = check(cudaEventRecord(slot.done, s), "frame");
   if (st != SK_OK) return st;
   // captures of this frame copy its image once it is drawn (again after a redraw)
   for (auto& c : captures)
@@ -501,7 +533,7 @@ sk_status Context::finishOldest() {
   if (c.overflow) {
     // Every frame in flight drew with these list buffers (or after one that did, into the same
     // image): wait for all of them, grow the buffers and draw them all again, in order.
-    e = cudaStreamSynchronize(stream);
+    e = syncStreams();
     if (e != cudaSuccess) return check(e, "frame wait");
     uint32_t most = c.instances;
     for (const uint32_t k : inFlight) {
@@ -511,6 +543,7 @@ sk_status Context::finishOldest() {
     const uint32_t need = static_cast<uint32_t>(
         std::min<uint64_t>(uint64_t{most} + most / 4 + 1024, 0x7fffffffu));
     sk_status st = reserveScratch(scratch, scratch.sources, need, scratch.maxTiles, stream);
+    if (st == SK_OK && stream2) st = prepareSecondSlot();
     for (size_t k = 0; st == SK_OK && k < inFlight.size(); ++k) st = enqueueSlot(inFlight[k]);
     if (st != SK_OK) {
       inFlight.clear();  // nothing of theirs is left running
@@ -518,6 +551,7 @@ sk_status Context::finishOldest() {
     }
     return finishOldest();
   }
+  lastSlot = inFlight.front();
   inFlight.pop_front();
   ++completed;
   lastCounters = c;
@@ -641,7 +675,7 @@ void sk_destroy(sk_context* handle) {
   auto* ctx = reinterpret_cast<Context*>(handle);
   if (!ctx) return;
   cudaSetDevice(ctx->device);
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->stream) ctx->syncStreams();
   delete ctx;
 }
 
@@ -729,7 +763,7 @@ sk_status sk_upload_world(sk_context* handle, const sk_cloud_view* cloud, int32_
   if (!cloud) return SK_E_INVALID;
   sk_status st = ctx->finishFrame(true);
   if (st == SK_E_DEVICE) return st;
-  cudaStreamSynchronize(ctx->stream);
+  ctx->syncStreams();
   // Build the new world aside; the old one stays until everything succeeded.
   sk::World fresh;
   st = ctx->uploadCloud(*cloud, maxSh, fresh);
@@ -748,7 +782,7 @@ sk_status sk_create_slab(sk_context* handle, uint32_t capacity, int32_t shDegree
   if (shDegree < 0 || shDegree > 3) return SK_E_INVALID;
   sk_status st = ctx->finishFrame(true);
   if (st == SK_E_DEVICE) return st;
-  cudaStreamSynchronize(ctx->stream);
+  ctx->syncStreams();
   sk::World fresh;
   cudaError_t e = fresh.splats.allocate(size_t{capacity} * sizeof(sk::GpuSplat));
   if (e == cudaSuccess) e = fresh.sh.allocate(size_t{capacity} * sk::shDeviceStride(shDegree) * 4);
@@ -803,7 +837,7 @@ sk_status sk_upload_lod_world(sk_context* handle, const sk_lod_view* tree, int32
   if (budget == 0) return ctx->fail(SK_E_INVALID, "LOD budget is zero");
   sk_status st = ctx->finishFrame(true);
   if (st == SK_E_DEVICE) return st;
-  cudaStreamSynchronize(ctx->stream);
+  ctx->syncStreams();
   // Selection data: the tree's own, else built once here (MetalLodSelection.mm:68-74).
   std::vector<sk::LodCluster> clusters;
   std::vector<uint32_t> leaves;
@@ -874,6 +908,10 @@ sk_status sk_draw(sk_context* handle, const sk_frame* frame) {
   if (!ctx->world.splats.ptr) total = 0;
   uint32_t index = 0;
   while (std::find(ctx->inFlight.begin(), ctx->inFlight.end(), index) != ctx->inFlight.end()) ++index;
+  if (index == 1) {
+    const sk_status st = ctx->prepareSecondSlot();
+    if (st != SK_OK) return st;
+  }
   sk::Context::Slot& slot = ctx->slots[index];
   if (ctx->twoImages) ctx->imageSlot ^= 1u;
   slot.frame = *frame;
@@ -899,7 +937,7 @@ sk_status sk_wait_idle(sk_context* handle) {
   SK_CTX(handle);
   const sk_status st = ctx->finishFrame(true);
   if (st != SK_OK) return st;
-  return ctx->check(cudaStreamSynchronize(ctx->stream), "wait");
+  return ctx->check(ctx->syncStreams(), "wait");
 }
 
 sk_status sk_read_image(sk_context* handle, void* host, size_t bytes, int32_t format) {
@@ -1040,9 +1078,9 @@ sk_status sk_read_visible(sk_context* handle, uint32_t* keys, void* projected, u
   if (count) *count = n;
   const uint32_t copy = std::min(n, capacity);
   cudaError_t e = cudaSuccess;
-  if (keys && copy) e = cudaMemcpy(keys, ctx->scratch.keys.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
+  if (keys && copy) e = cudaMemcpy(keys, ctx->scratchOf(ctx->lastSlot).keys.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && projected && copy)
-    e = cudaMemcpy(projected, ctx->scratch.projected.ptr, size_t{copy} * 32, cudaMemcpyDeviceToHost);
+    e = cudaMemcpy(projected, ctx->scratchOf(ctx->lastSlot).projected.ptr, size_t{copy} * 32, cudaMemcpyDeviceToHost);
   return ctx->check(e, "readback");
 }
 
@@ -1054,7 +1092,7 @@ sk_status sk_read_order(sk_context* handle, uint32_t* order, uint32_t capacity, 
   if (count) *count = n;
   const uint32_t copy = std::min(n, capacity);
   if (!order || !copy) return SK_OK;
-  return ctx->check(cudaMemcpy(order, ctx->scratch.order.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
+  return ctx->check(cudaMemcpy(order, ctx->scratchOf(ctx->lastSlot).order.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
                     "readback");
 }
 
@@ -1069,7 +1107,7 @@ sk_status sk_read_cut(sk_context* handle, uint32_t* indices, uint32_t capacity, 
   if (lod6) std::memcpy(lod6, ctx->lastCounters.lod, 24);
   const uint32_t copy = std::min(n, capacity);
   if (!indices || !copy) return SK_OK;
-  return ctx->check(cudaMemcpy(indices, ctx->scratch.lodIndices.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
+  return ctx->check(cudaMemcpy(indices, ctx->scratchOf(ctx->lastSlot).lodIndices.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost),
                     "readback");
 }
 
@@ -1078,15 +1116,15 @@ sk_status sk_read_tile_lists(sk_context* handle, uint32_t* ranges, uint32_t* val
   SK_CTX(handle);
   sk_status st = ctx->finishFrame(true);
   if (st != SK_OK) return st;
-  const uint32_t n = std::min(ctx->lastCounters.instances, ctx->scratch.instanceCapacity);
+  const uint32_t n = std::min(ctx->lastCounters.instances, ctx->scratchOf(ctx->lastSlot).instanceCapacity);
   if (count) *count = n;
   cudaError_t e = cudaSuccess;
   const size_t bins = size_t{(ctx->width + sk::kBinSize - 1) / sk::kBinSize} *
                       ((ctx->height + sk::kBinSize - 1) / sk::kBinSize);
-  if (ranges) e = cudaMemcpy(ranges, ctx->scratch.ranges.ptr, bins * 8, cudaMemcpyDeviceToHost);
+  if (ranges) e = cudaMemcpy(ranges, ctx->scratchOf(ctx->lastSlot).ranges.ptr, bins * 8, cudaMemcpyDeviceToHost);
   const uint32_t copy = std::min(n, capacity);
   if (e == cudaSuccess && values && copy)
-    e = cudaMemcpy(values, ctx->scratch.instValuesSorted.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
+    e = cudaMemcpy(values, ctx->scratchOf(ctx->lastSlot).instValuesSorted.ptr, size_t{copy} * 4, cudaMemcpyDeviceToHost);
   return ctx->check(e, "readback");
 }
 

@@ -131,8 +131,20 @@ struct Context {
   // Frame slots: like the reference's frame loop (MetalFrameSlots.h:8) a flat world keeps two
   // frames in flight, so the host enqueues the next frame while the GPU draws the last; a
   // slot holds what finishing (or drawing again) its frame needs. LOD worlds keep one, so the
-  // adaptive threshold sees every frame's cut before the next selection.
+  // adaptive threshold sees every frame's cut before the next selection. Slot 1 draws on its
+  // own stream with its own scratch, counters, camera and image (set up the first time two
+  // frames are in flight), so the two frames' kernels run side by side on the device.
   static constexpr uint32_t kFrameSlots = 2;
+  cudaStream_t stream2 = nullptr;
+  FrameScratch scratch2;
+  DeviceBuffer frameCounters2, camera2;
+  uint32_t lastSlot = 0;  // slot of the last finished frame (whose scratch the read-backs copy)
+  FrameScratch& scratchOf(uint32_t slot) { return slot ? scratch2 : scratch; }
+  cudaStream_t streamOf(uint32_t slot) const { return slot ? stream2 : stream; }
+  // Slot 1's stream, scratch (as large as slot 0's) and view buffers, and a second image.
+  sk_status prepareSecondSlot();
+  // Waits for everything enqueued on the frame streams.
+  cudaError_t syncStreams();
   struct Slot {
     PinnedBuffer hostCounters, hostCamera;
     cudaEvent_t done = nullptr;

@@ -168,3 +168,44 @@ def test_timing_modes_draw_the_same_image(cuda_device):
     assert stats["frame"]["gpu_ms"] > 0 and stats["frame"]["composite_ms"] == 0
     for mode in (True, "frame", False):
         assert stats[mode]["draw_count"] == stats[True]["draw_count"]
+
+
+@pytest.mark.gpu
+def test_overlapped_frames_equal_frames_drawn_alone(cuda_device):
+    # draws without a wait alternate between the two frame slots, each on its own stream with its
+    # own scratch and image: every frame's image equals the one drawn alone, and the read-backs
+    # after the last draw give that frame's survivors, records and order
+    w, h = 640, 480
+    cloud = synthetic.random_cloud(150_000, seed=12, sh_degree=2)
+    frames = frames_for(cloud, w, h, range(0, 50, 5))
+    alone = sk.Renderer(w, h, image_format=sk.FORMAT_RGBA8)
+    alone.upload_world(cloud, 2)
+    want = []
+    for f in frames:
+        alone.draw(f)
+        keys, projected = alone.read_visible()
+        want.append((alone.read_image(sk.FORMAT_RGBA8).copy(), keys, projected, alone.read_order()))
+    alone.close()
+    r = sk.Renderer(w, h, image_format=sk.FORMAT_RGBA8)
+    r.upload_world(cloud, 2)
+    buffers = [pinned_image(w, h, sk.FORMAT_RGBA8) for _ in frames]
+    tickets = []
+    for f, b in zip(frames, buffers):
+        tickets.append(r.capture_next_frame(b))
+        r.draw(f)
+    got = [r.wait_capture(t).copy() for t in tickets]
+    keys, projected = r.read_visible()
+    order = r.read_order()
+    for g, expected in zip(got, want):
+        assert np.array_equal(g, expected[0])
+    assert np.array_equal(keys, want[-1][1]) and projected.tobytes() == want[-1][2].tobytes()
+    assert np.array_equal(order, want[-1][3])
+    # plain draws in flight (no captures): the image and read-backs are the last frame's
+    for k in (3, 4, 7):
+        r.draw(frames[k])
+    assert np.array_equal(r.read_image(sk.FORMAT_RGBA8), want[7][0])
+    keys, projected = r.read_visible()
+    assert np.array_equal(keys, want[7][1]) and np.array_equal(r.read_order(), want[7][3])
+    stats = r.stats()
+    r.close()
+    assert stats["submitted_frames"] == stats["completed_frames"] == len(frames) + 3
