@@ -71,8 +71,27 @@ __device__ __forceinline__ uint4 tileSpan(const uint4 lo, const uint4 hi, float 
   const uint32_t w = x1 - x0 + 1, area = w * (y1 - y0 + 1);
   uint64_t mask = 0;
   if (area <= 64) {
-    for (uint32_t k = 0; k < area; ++k)
-      if (quadTouchesTile(q, x0 + k % w, y0 + k / w, height)) mask |= 1ull << k;
+    // quadTouchesTile over the box's cells row by row (bit k = cell (x0 + k % w, y0 + k / w)),
+    // with the quad's extents along x, y and the two normals taken once
+    const float half = 0.5f * static_cast<float>(kBinSize);
+    const float exq = q.r * (fabsf(q.a1x) + fabsf(q.a2x)) + half;
+    const float eyq = q.r * (fabsf(q.a1y) + fabsf(q.a2y)) + half;
+    const float n1x = -q.a1y, n1y = q.a1x, n2x = -q.a2y, n2y = q.a2x;
+    const float e1 = q.r * fabsf(q.a2x * n1x + q.a2y * n1y) + half * (fabsf(n1x) + fabsf(n1y));
+    const float e2 = q.r * fabsf(q.a1x * n2x + q.a1y * n2y) + half * (fabsf(n2x) + fabsf(n2y));
+    uint32_t k = 0;
+    for (uint32_t ty = y0; ty <= y1; ++ty) {
+      const float ry = height - (static_cast<float>(ty * kBinSize) + half);
+      const float dy = ry - q.cy;
+      const bool rowIn = !(fabsf(dy) > eyq);
+      for (uint32_t tx = x0; tx <= x1; ++tx, ++k) {
+        const float rx = static_cast<float>(tx * kBinSize) + half;
+        const float dx = rx - q.cx;
+        const bool hit = rowIn && !(fabsf(dx) > exq) && !(fabsf(dx * n1x + dy * n1y) > e1) &&
+                         !(fabsf(dx * n2x + dy * n2y) > e2);
+        if (hit) mask |= 1ull << k;
+      }
+    }
     if (mask == 0) return make_uint4(0, 0, 0, 0);
   }
   return make_uint4(x0 | (y0 << 16), w | (area << 16), static_cast<uint32_t>(mask),
