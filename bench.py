@@ -449,7 +449,9 @@ def run_ours(args):
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 4 + 64,
                     "how": "per step capture_next_frame into pinned memory + draw (camera 208 B "
                            "up), then wait for the previous step's image (8.3 MB down, copied "
-                           "while this frame draws); no GPU timing events; host-timed",
+                           "while this frame draws); the two frames in flight run on the "
+                           "context's two frame streams and overlap on the device; no GPU "
+                           "timing events; host-timed",
                     "blocking_read_image_frames_per_s": blocking_value},
             "clocks": clocks.summary(),
             "gpu_launches": launches_per_frame * args.steps,
@@ -721,7 +723,8 @@ def serve_trace(count, rate, seed=2000):
 def run_served(renderers, frames, arrivals, max_queue_ms=0.0, lanes=2, max_batch_views=16,
                max_batch_splats=96_000_000):
     """Replays the trace through the continuous-batching server: completed requests over the wall
-    time from the first arrival to the last completion, and the latency percentiles."""
+    time from the first arrival to the last completion, and the latency percentiles. One untimed
+    replay of the same trace first, so that the lanes have grown to the trace's batches."""
     import splatkit_b200 as sk
 
     ring = [sk.HostImage(3840, 2160) for _ in range(96)]
@@ -730,7 +733,7 @@ def run_served(renderers, frames, arrivals, max_queue_ms=0.0, lanes=2, max_batch
                    max_queue_ms=max_queue_ms) as server:
         for r in renderers:
             server.add_scene(r)
-        server.replay(reqs[:32], [0.0] * 32)
+        server.replay(reqs, arrivals)
         t0 = time.perf_counter()
         done = server.replay(reqs, arrivals)
         elapsed = time.perf_counter() - t0
@@ -747,10 +750,16 @@ def run_served(renderers, frames, arrivals, max_queue_ms=0.0, lanes=2, max_batch
 def run_plain(renderers, frames, arrivals):
     """The same trace through the plain per-frame loop (resize, draw, blocking read back, one
     request at a time as it arrives): completed requests over the wall time from the first
-    arrival to the last completion, as for the server, and the loop's busy-time capacity."""
+    arrival to the last completion, as for the server, and the loop's busy-time capacity. Like
+    the server, the loop first runs the trace once untimed."""
     import splatkit_b200 as sk
 
     pinned = sk.HostImage(3840, 2160)
+    for scene, f, w, h in frames:
+        r = renderers[scene]
+        r.resize(w, h)
+        r.draw(f)
+        r.read_image(sk.FORMAT_RGBA8, out=pinned.array.reshape(-1)[:w * h * 4].reshape(h, w, 4))
     lat, busy = [], 0.0
     t0 = time.perf_counter()
     for i, (scene, f, w, h) in enumerate(frames):

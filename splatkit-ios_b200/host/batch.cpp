@@ -61,8 +61,19 @@ uint32_t bitsFor(uint64_t values) {  // key bits, a multiple of 8, for keys < va
 
 sk_status Batch::reserve(BatchLane& l, uint32_t sources, uint32_t instances, uint32_t items,
                          uint32_t tiles, uint32_t views, uint64_t pixels) {
-  sources = std::max(sources, 1u);
-  instances = std::max(instances, 1u);
+  // A buffer that must grow grows by at least half again: freeing the old one waits for the
+  // whole device, so a lane should reach its working size in a few steps, not one per batch.
+  auto grown32 = [](uint32_t need, uint32_t have) -> uint32_t {
+    return need > have ? static_cast<uint32_t>(std::min<uint64_t>(
+                             std::max<uint64_t>(need, uint64_t{have} + have / 2), 0x7fffffffu))
+                       : need;
+  };
+  sources = grown32(std::max(sources, 1u), l.sources);
+  instances = grown32(std::max(instances, 1u), l.instances);
+  items = grown32(items, l.items);
+  tiles = grown32(tiles, l.tiles);
+  views = grown32(views, l.views);
+  if (pixels > l.pixels) pixels = std::max(pixels, l.pixels + l.pixels / 2);
   cudaError_t e = cudaSuccess;
   auto grab = [&](DeviceBuffer& b, size_t n) {
     if (e == cudaSuccess) e = b.allocate(n);
@@ -278,7 +289,9 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
       rowBytes += cellListRowBytes(c.capacity, c.cells);
     }
     void* before[3] = {l.cellLists.ptr, l.cellStatus.ptr, l.cellViews.ptr};
-    cudaError_t e = l.cellLists.allocate(rowBytes);
+    cudaError_t e = l.cellLists.allocate(
+        rowBytes > l.cellLists.bytes ? std::max<uint64_t>(rowBytes, l.cellLists.bytes + l.cellLists.bytes / 2)
+                                     : rowBytes);
     if (e == cudaSuccess) e = l.cellStatus.allocate(size_t{cb.groups} * 8);
     if (e == cudaSuccess) e = l.cellViews.allocate(size_t{count} * sizeof(CellListView));
     if (e == cudaSuccess) e = l.hostCellViews.allocate(size_t{count} * sizeof(CellListView));
