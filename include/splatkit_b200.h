@@ -299,7 +299,11 @@ sk_status sk_read_tile_lists(sk_context* ctx, uint32_t* ranges, uint32_t* values
  * overlap on the device; a submission's results (RGBA8 images, survivor counts) are copied to
  * pinned host memory by the same stream and stay readable until its lane is reused, `lanes`
  * submissions later. The contexts' worlds must not be replaced while a submission that draws
- * them is in flight. The batch keeps no reference to a context beyond the submit call. */
+ * them is in flight. The batch keeps no reference to a context beyond the submit call.
+ * A lane's device buffers grow stream-ordered (cudaMallocAsync on the lane's stream, at least
+ * half again each time), so growing one lane never waits for the others. From the first batch or
+ * server on, the device's default memory pool keeps the memory lanes give back, for later lanes
+ * of any batch or server in the process; cudaMemPoolTrimTo on that pool returns it. */
 typedef struct sk_batch sk_batch;
 
 typedef struct {

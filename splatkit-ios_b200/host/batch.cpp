@@ -17,6 +17,7 @@
 #include <cmath>
 #include <chrono>
 #include <cstring>
+#include <mutex>
 #include <memory>
 
 namespace sk {
@@ -27,6 +28,21 @@ BatchLane::~BatchLane() {
   if (start) cudaEventDestroy(start);
   if (end) cudaEventDestroy(end);
   if (stream) cudaStreamDestroy(stream);
+}
+
+void holdPooledMemory(int device) {
+  static std::mutex m;
+  static std::vector<bool> held;
+  std::lock_guard<std::mutex> g(m);
+  if (held.size() <= static_cast<size_t>(device)) held.resize(device + 1, false);
+  if (held[device]) return;
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess)
+      held[device] = true;
+  }
+  cudaGetLastError();
 }
 
 sk_status Batch::fail(sk_status code, const std::string& message) {
@@ -76,7 +92,7 @@ sk_status Batch::reserve(BatchLane& l, uint32_t sources, uint32_t instances, uin
   if (pixels > l.pixels) pixels = std::max(pixels, l.pixels + l.pixels / 2);
   cudaError_t e = cudaSuccess;
   auto grab = [&](DeviceBuffer& b, size_t n) {
-    if (e == cudaSuccess) e = b.allocate(n);
+    if (e == cudaSuccess) e = b.allocateOn(n, l.stream);
   };
   auto pin = [&](PinnedBuffer& b, size_t n) {
     if (e == cudaSuccess) e = b.allocate(n);
@@ -136,7 +152,7 @@ sk_status Batch::reserve(BatchLane& l, uint32_t sources, uint32_t instances, uin
 sk_status Batch::reserveLod(BatchLane& l, uint32_t indices, uint32_t frontier, uint32_t views) {
   cudaError_t e = cudaSuccess;
   auto grab = [&](DeviceBuffer& b, size_t n) {
-    if (e == cudaSuccess) e = b.allocate(n);
+    if (e == cudaSuccess) e = b.allocateOn(n, l.stream);
   };
   frontier = std::max({frontier, l.lodFrontierCapacity, 1u});
   const uint32_t tiles = (frontier + lodTileClusters() - 1) / lodTileClusters();
@@ -289,11 +305,11 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
       rowBytes += cellListRowBytes(c.capacity, c.cells);
     }
     void* before[3] = {l.cellLists.ptr, l.cellStatus.ptr, l.cellViews.ptr};
-    cudaError_t e = l.cellLists.allocate(
+    cudaError_t e = l.cellLists.allocateOn(
         rowBytes > l.cellLists.bytes ? std::max<uint64_t>(rowBytes, l.cellLists.bytes + l.cellLists.bytes / 2)
-                                     : rowBytes);
-    if (e == cudaSuccess) e = l.cellStatus.allocate(size_t{cb.groups} * 8);
-    if (e == cudaSuccess) e = l.cellViews.allocate(size_t{count} * sizeof(CellListView));
+                                     : rowBytes, l.stream);
+    if (e == cudaSuccess) e = l.cellStatus.allocateOn(size_t{cb.groups} * 8, l.stream);
+    if (e == cudaSuccess) e = l.cellViews.allocateOn(size_t{count} * sizeof(CellListView), l.stream);
     if (e == cudaSuccess) e = l.hostCellViews.allocate(size_t{count} * sizeof(CellListView));
     if (e != cudaSuccess) return check(e, "batch cell lists");
     std::memcpy(l.hostCellViews.ptr, cellViews.data(), size_t{count} * sizeof(CellListView));
@@ -635,6 +651,7 @@ sk_status sk_batch_create(const sk_batch_config* config, sk_batch** out) {
         cudaEventCreate(&l.start) != cudaSuccess || cudaEventCreate(&l.end) != cudaSuccess)
       return SK_E_DEVICE;
   }
+  sk::holdPooledMemory(config->device);
   *out = reinterpret_cast<sk_batch*>(b.release());
   return SK_OK;
 }

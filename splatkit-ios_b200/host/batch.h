@@ -91,6 +91,12 @@ struct BatchLane {
   ~BatchLane();
 };
 
+// Lane buffers grow stream-ordered from the device's default memory pool, which from the first
+// batch or server on keeps the memory lanes give back: later growth, in this or a later batch or
+// server, reuses it instead of asking the driver (driver allocations took up to ~100 ms each
+// on a B200 while other lanes ran, and each free waited for the whole device).
+void holdPooledMemory(int device);
+
 struct Batch {
   int device = 0;
   BatchTuning tuning;

@@ -45,6 +45,23 @@ cudaError_t DeviceBuffer::allocate(size_t n) {
   return cudaSuccess;
 }
 
+cudaError_t DeviceBuffer::allocateOn(size_t n, cudaStream_t s) {
+  n = std::max<size_t>(n, 256);
+  if (n <= bytes && ptr) return cudaSuccess;
+  for (uint32_t left = gTestFailedAllocations.load(); left > 0;)
+    if (gTestFailedAllocations.compare_exchange_weak(left, left - 1)) return cudaErrorMemoryAllocation;
+  void* fresh = nullptr;
+  const cudaError_t e = cudaMallocAsync(&fresh, n, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e;
+  }
+  if (ptr) cudaFreeAsync(ptr, s);
+  ptr = fresh;
+  bytes = n;
+  return cudaSuccess;
+}
+
 void DeviceBuffer::release() {
   if (ptr) cudaFree(ptr);
   ptr = nullptr;

@@ -53,6 +53,10 @@ struct DeviceBuffer {
   }
   ~DeviceBuffer() { release(); }
   cudaError_t allocate(size_t n);
+  // Stream-ordered growth on stream s (the only stream that uses the buffer): the new memory
+  // comes from the device's memory pool and the old goes back to it after s's earlier work,
+  // so growing neither waits for the device nor, once the pool holds the memory, for the driver.
+  cudaError_t allocateOn(size_t n, cudaStream_t s);
   void release();
 };
 

@@ -265,6 +265,7 @@ sk_status sk_server_create(const sk_server_config* config, sk_server** out) {
       return SK_E_DEVICE;
   }
   s->work = std::vector<sk::LaneWork>(config->lanes);
+  sk::holdPooledMemory(config->device);
   Server* raw = s.get();
   s->scheduler = std::thread([raw] { raw->run(); });
   *out = reinterpret_cast<sk_server*>(s.release());
@@ -280,6 +281,8 @@ void sk_server_destroy(sk_server* handle) {
     s->arrived.notify_all();
   }
   if (s->scheduler.joinable()) s->scheduler.join();
+  for (auto& l : s->batch.lanes)
+    if (l.stream) cudaStreamSynchronize(l.stream);
   delete s;
 }
 
