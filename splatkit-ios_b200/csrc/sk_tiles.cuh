@@ -28,27 +28,6 @@ __device__ __forceinline__ Quad quadOf(const uint4 lo, const uint4 hi, float hal
   return q;
 }
 
-// Separating-axis test of the quad against cell (tx, ty)'s pixel square (y up).
-__device__ __forceinline__ bool quadTouchesTile(const Quad& q, uint32_t tx, uint32_t ty,
-                                                float height) {
-  const float half = 0.5f * static_cast<float>(kBinSize);
-  const float rx = static_cast<float>(tx * kBinSize) + half;
-  const float ry = height - (static_cast<float>(ty * kBinSize) + half);
-  const float dx = rx - q.cx, dy = ry - q.cy;
-  if (fabsf(dx) > q.r * (fabsf(q.a1x) + fabsf(q.a2x)) + half) return false;
-  if (fabsf(dy) > q.r * (fabsf(q.a1y) + fabsf(q.a2y)) + half) return false;
-  // normal of a1: the quad's extent along it comes from t a2 only
-  const float n1x = -q.a1y, n1y = q.a1x;
-  if (fabsf(dx * n1x + dy * n1y) >
-      q.r * fabsf(q.a2x * n1x + q.a2y * n1y) + half * (fabsf(n1x) + fabsf(n1y)))
-    return false;
-  const float n2x = -q.a2y, n2y = q.a2x;
-  if (fabsf(dx * n2x + dy * n2y) >
-      q.r * fabsf(q.a1x * n2x + q.a1y * n2y) + half * (fabsf(n2x) + fabsf(n2y)))
-    return false;
-  return true;
-}
-
 // The span of one projected record (two uint4 words) on a width x height target.
 __device__ __forceinline__ uint4 tileSpan(const uint4 lo, const uint4 hi, float width, float height,
                                           uint32_t tilesX, uint32_t tilesY) {
@@ -71,8 +50,9 @@ __device__ __forceinline__ uint4 tileSpan(const uint4 lo, const uint4 hi, float 
   const uint32_t w = x1 - x0 + 1, area = w * (y1 - y0 + 1);
   uint64_t mask = 0;
   if (area <= 64) {
-    // quadTouchesTile over the box's cells row by row (bit k = cell (x0 + k % w, y0 + k / w)),
-    // with the quad's extents along x, y and the two normals taken once
+    // Separating-axis test of the quad against each cell's pixel square (y up), the box's cells
+    // row by row (bit k = cell (x0 + k % w, y0 + k / w)); the quad's extents along x, y and the
+    // normals of a1 and a2 (along a normal of a1 the extent comes from t a2 only) are taken once.
     const float half = 0.5f * static_cast<float>(kBinSize);
     const float exq = q.r * (fabsf(q.a1x) + fabsf(q.a2x)) + half;
     const float eyq = q.r * (fabsf(q.a1y) + fabsf(q.a2y)) + half;
