@@ -1,7 +1,8 @@
 """The batched multi-view path (sk_batch_*) against the plain per-frame path, view by view.
 
 A batch runs every stage once over all its views (several worlds, several target sizes; the cell
-lists view after view, or for targets above 4096 cells one sort over all views) with the plain
+lists in place by one launch per pass over all views, or for targets above 4096 cells by one sort
+over all views) with the plain
 frame's arithmetic, so each view's image and survivor count must equal what sk_draw
 gives for that view with 16-bit depth keys — bit for bit, not just within tolerance.
 """
@@ -113,6 +114,21 @@ def test_submissions_in_flight_on_two_lanes(worlds):
         with pytest.raises(sk.SplatError):
             batch.wait(t1)
         check_against_plain(batch, t3, first)
+
+
+@pytest.mark.gpu
+def test_lanes_grow_while_the_other_lane_draws(worlds):
+    # lane buffers grow stream-ordered: each submission is larger than anything its lane held
+    # and is enqueued while the other lane's submission is still on the device; all stay exact
+    with sk.Batch(lanes=2, max_views=16) as batch:
+        tickets, submitted = [], []
+        for k, count in enumerate((2, 6, 12, 16)):
+            views = views_for(worlds, count, start_frame=20 * k)
+            tickets.append(batch.submit(views))
+            submitted.append(views)
+            if k >= 1:  # the previous submission, on the other lane, before its lane is reused
+                check_against_plain(batch, tickets[k - 1], submitted[k - 1])
+        check_against_plain(batch, tickets[-1], submitted[-1])
 
 
 @pytest.mark.gpu
