@@ -11,7 +11,9 @@
 //             the block that finishes last commits the round (SplatLOD.metal:165-181);
 //   scatter   next frontier, inline leaf indices (<= 32 leaves) and packets (SplatLOD.metal:182-208).
 // A final kernel copies packet leaves (SplatLOD.metal:210-220). Grids are sized by the frontier
-// capacity and read the live counts from the state, so no round needs the host.
+// capacity and read the live counts from the state, so no round needs the host; every kernel is
+// launched chained (programmatic dependent launch), so a round's kernels follow one another
+// without launch gaps.
 //
 // Built with -fmad=false: lodOutside and lodErrorPixels round every product and sum on their
 // own, in the order written, so the split decisions match the host oracle bit for bit.
@@ -19,6 +21,7 @@
 
 #include "sk_device.cuh"
 #include "sk_kernels.h"
+#include "sk_launch.cuh"
 
 namespace sk {
 namespace {
@@ -145,6 +148,7 @@ __device__ __forceinline__ uint32_t itemIndex(uint32_t tile, uint32_t r) {
 }
 
 __global__ void lodInitKernel(uint32_t* frontier, LodState* state) {
+  chainedKernelStart();
   frontier[0] = 0;
   LodState s{};
   s.active = 1;
@@ -154,6 +158,7 @@ __global__ void lodInitKernel(uint32_t* frontier, LodState* state) {
 __global__ void __launch_bounds__(kThreads)
     lodEvaluateKernel(const Camera* __restrict__ camera, const __grid_constant__ LodArgs a,
                       const uint32_t* __restrict__ frontier, uint32_t epoch) {
+  chainedKernelStart();
   __shared__ Camera cam;
   loadCamera(camera, &cam);
   LodState* st = a.state;
@@ -249,6 +254,7 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void __launch_bounds__(kThreads)
     lodCompactKernel(const __grid_constant__ LodArgs a, const uint32_t* __restrict__ frontier,
                      RoundSums* sums, uint32_t epoch) {
+  chainedKernelStart();
   LodState* st = a.state;
   const uint32_t tile = takeTile(a.counters);
   const uint32_t active = min(st->active, a.frontierCapacity);
@@ -314,6 +320,7 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void __launch_bounds__(kThreads)
     lodScatterKernel(const __grid_constant__ LodArgs a, const uint32_t* __restrict__ frontier,
                      uint32_t* __restrict__ next) {
+  chainedKernelStart();
   const LodState* st = a.state;
   const uint32_t active = min(st->scatterActive, a.frontierCapacity);
   const uint32_t countBase = st->scatterCount, packetBase = st->scatterPackets;
@@ -347,6 +354,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void __launch_bounds__(kThreads) lodEmitKernel(const __grid_constant__ LodArgs a) {
+  chainedKernelStart();
   const uint32_t packets = min(a.state->packets, a.frontierCapacity);
   for (uint32_t p = blockIdx.x; p < packets; p += gridDim.x) {
     const uint4 packet = a.packets[p];
@@ -360,6 +368,7 @@ __global__ void __launch_bounds__(kThreads) lodEmitKernel(const __grid_constant_
 }
 
 __global__ void lodReportKernel(const LodState* state, uint32_t* report) {
+  chainedKernelStart();
   if (threadIdx.x < 6) report[threadIdx.x] = reinterpret_cast<const uint32_t*>(state)[threadIdx.x];
 }
 
@@ -370,19 +379,22 @@ uint32_t lodTileClusters() { return kTileClusters; }
 cudaError_t launchLodSelect(const Camera* cam, const LodArgs& a, cudaStream_t stream) {
   const uint32_t grid = max(1u, (a.frontierCapacity + kTileClusters - 1) / kTileClusters);
   RoundSums* sums = reinterpret_cast<RoundSums*>(reinterpret_cast<char*>(a.state) + sizeof(LodState));
-  lodInitKernel<<<1, 1, 0, stream>>>(a.frontier[0], a.state);
-  for (uint32_t level = 0; level < a.rounds; ++level) {
+  cudaError_t e = launchChained(lodInitKernel, 1, 1, stream, a.frontier[0], a.state);
+  for (uint32_t level = 0; e == cudaSuccess && level < a.rounds; ++level) {
     const uint32_t* cur = a.frontier[level & 1u];
     uint32_t* nxt = a.frontier[(level + 1) & 1u];
     const uint32_t epoch = (a.epoch + 2 * level) & 0x3fffffffu;
-    lodEvaluateKernel<<<grid, kThreads, 0, stream>>>(cam, a, cur, epoch);
-    lodCompactKernel<<<grid, kThreads, 0, stream>>>(a, cur, sums, (epoch + 1) & 0x3fffffffu);
-    lodScatterKernel<<<min(grid * kItems, 148u * 8u), kThreads, 0, stream>>>(a, cur, nxt);
+    e = launchChained(lodEvaluateKernel, grid, kThreads, stream, cam, a, cur, epoch);
+    if (e == cudaSuccess)
+      e = launchChained(lodCompactKernel, grid, kThreads, stream, a, cur, sums,
+                        (epoch + 1) & 0x3fffffffu);
+    if (e == cudaSuccess)
+      e = launchChained(lodScatterKernel, min(grid * kItems, 148u * 8u), kThreads, stream, a, cur, nxt);
   }
   const uint32_t packetGrid = max(1u, min(a.frontierCapacity, 148u * 8u));
-  lodEmitKernel<<<packetGrid, kThreads, 0, stream>>>(a);
-  lodReportKernel<<<1, 32, 0, stream>>>(a.state, a.report);
-  return cudaGetLastError();
+  if (e == cudaSuccess) e = launchChained(lodEmitKernel, packetGrid, kThreads, stream, a);
+  if (e == cudaSuccess) e = launchChained(lodReportKernel, 1, 32, stream, a.state, a.report);
+  return e;
 }
 
 }  // namespace sk
