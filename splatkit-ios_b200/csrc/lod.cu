@@ -19,8 +19,6 @@
 // own, in the order written, so the split decisions match the host oracle bit for bit.
 #include <cuda_runtime.h>
 
-#include <algorithm>
-
 #include "sk_device.cuh"
 #include "sk_kernels.h"
 #include "sk_launch.cuh"
@@ -379,16 +377,13 @@ __global__ void lodReportKernel(const LodState* state, uint32_t* report) {
 uint32_t lodTileClusters() { return kTileClusters; }
 
 cudaError_t launchLodSelect(const Camera* cam, const LodArgs& a, cudaStream_t stream) {
+  const uint32_t grid = max(1u, (a.frontierCapacity + kTileClusters - 1) / kTileClusters);
   RoundSums* sums = reinterpret_cast<RoundSums*>(reinterpret_cast<char*>(a.state) + sizeof(LodState));
   cudaError_t e = launchChained(lodInitKernel, 1, 1, stream, a.frontier[0], a.state);
-  uint64_t most = 1;  // clusters the round's frontier can hold: the root, then fanout times more
   for (uint32_t level = 0; e == cudaSuccess && level < a.rounds; ++level) {
     const uint32_t* cur = a.frontier[level & 1u];
     uint32_t* nxt = a.frontier[(level + 1) & 1u];
     const uint32_t epoch = (a.epoch + 2 * level) & 0x3fffffffu;
-    const uint64_t bound = a.fanout ? std::min<uint64_t>(most, a.frontierCapacity) : a.frontierCapacity;
-    const uint32_t grid = std::max<uint32_t>(1u, static_cast<uint32_t>((bound + kTileClusters - 1) / kTileClusters));
-    most = std::min<uint64_t>(most * std::max(a.fanout, 1u), a.frontierCapacity);
     e = launchChained(lodEvaluateKernel, grid, kThreads, stream, cam, a, cur, epoch);
     if (e == cudaSuccess)
       e = launchChained(lodCompactKernel, grid, kThreads, stream, a, cur, sums,
