@@ -3,14 +3,13 @@
 // MetalLodSelection.mm:109-192), producing the same cut in the same emission order.
 //
 // Per round the reference dispatches evaluate, scan, budget, compact, scan, commit and scatter.
-// Here a round is two kernels:
+// Here a round is three kernels:
 //   evaluate  drop / split / forced split per frontier cluster; the exclusive prefix of the
 //             extra cost by decoupled look-back; the block that finishes last runs the capacity
 //             guard (a 256-way search for the largest accepted prefix, SplatLOD.metal:116-132);
-//   compact   denies over-budget splits, scans kids / splats / packets (three look-backs), then
-//             writes each cluster's next-frontier children, inline leaf indices (<= 32 leaves)
-//             and packets at the scanned positions (SplatLOD.metal:182-208); the block that
-//             finishes last commits the round (SplatLOD.metal:165-181).
+//   compact   denies over-budget splits, scans kids / splats / packets (three look-backs) and
+//             the block that finishes last commits the round (SplatLOD.metal:165-181);
+//   scatter   next frontier, inline leaf indices (<= 32 leaves) and packets (SplatLOD.metal:182-208).
 // A final kernel copies packet leaves (SplatLOD.metal:210-220). Grids are sized by the frontier
 // capacity and read the live counts from the state, so no round needs the host; every kernel is
 // launched chained (programmatic dependent launch), so a round's kernels follow one another
@@ -254,14 +253,12 @@ __global__ void __launch_bounds__(kThreads)
 
 __global__ void __launch_bounds__(kThreads)
     lodCompactKernel(const __grid_constant__ LodArgs a, const uint32_t* __restrict__ frontier,
-                     uint32_t* __restrict__ next, RoundSums* sums, uint32_t epoch) {
+                     RoundSums* sums, uint32_t epoch) {
   chainedKernelStart();
   LodState* st = a.state;
   const uint32_t tile = takeTile(a.counters);
   const uint32_t active = min(st->active, a.frontierCapacity);
   const uint32_t accepted = st->accepted;
-  // the round's bases: the last block commits the round only after every block has scattered
-  const uint32_t countBase = st->count, packetBase = st->packets;
   const uint32_t tiles = (active + kTileClusters - 1) / kTileClusters;
   if (tile < tiles) {
     uint32_t vals[3][kItems], flagsOf[kItems];
@@ -292,35 +289,10 @@ __global__ void __launch_bounds__(kThreads)
     const size_t stride = (a.frontierCapacity + kTileClusters - 1) / kTileClusters;
     uint64_t* const status[3] = {a.status, a.status + stride, a.status + 2 * stride};
     tileScan<3>(vals, tile, status, epoch, a.error, offs, aggregate, exclusive);
-    // scatter (SplatLOD.metal:182-208): the next frontier, inline leaf indices (<= 32 leaves) and
-    // packets, at the positions the scans gave
-#pragma unroll 1
+#pragma unroll
     for (uint32_t r = 0; r < kItems; ++r) {
       const uint32_t t = itemIndex(tile, r);
-      if (t >= active || (flagsOf[r] & kDrop)) continue;
-      const LodCluster node = loadCluster(a.clusters, frontier[t]);
-      const bool split = (flagsOf[r] & kSplit) != 0;
-      if (split) {
-        if (offs[0][r] + node.childCount > a.frontierCapacity) {
-          atomicOr(a.error, SK_DEVERR_BOUNDS);
-        } else {
-          for (uint32_t k = 0; k < node.childCount; ++k) next[offs[0][r] + k] = node.childStart + k;
-        }
-      }
-      const uint32_t count = split ? node.leafCount : 1;
-      const uint32_t destination = countBase + offs[1][r];
-      if (count > 32) {
-        if (packetBase + offs[2][r] < a.frontierCapacity)
-          a.packets[packetBase + offs[2][r]] = make_uint4(node.leafStart, count, destination, 1);
-        else
-          atomicOr(a.error, SK_DEVERR_BOUNDS);
-      } else if (destination + count > a.capacity) {
-        atomicOr(a.error, SK_DEVERR_BOUNDS);
-      } else if (!split) {
-        a.indices[destination] = node.node;
-      } else {
-        for (uint32_t k = 0; k < count; ++k) a.indices[destination + k] = a.leaves[node.leafStart + k];
-      }
+      if (t < active) a.offsets[t] = make_uint4(offs[0][r], offs[1][r], offs[2][r], flagsOf[r]);
     }
     for (int o = 16; o > 0; o >>= 1) denied += __shfl_xor_sync(0xffffffffu, denied, o);
     if (laneId() == 0 && denied) atomicAdd(&st->limited, denied);
@@ -336,9 +308,48 @@ __global__ void __launch_bounds__(kThreads)
     const volatile RoundSums* v = sums;
     const RoundSums s{v->kids, v->splats, v->packets};
     st->evaluated += active;
+    st->scatterActive = active;
+    st->scatterCount = st->count;
+    st->scatterPackets = st->packets;
     st->count += s.splats;
     st->packets += s.packets;
     st->active = s.kids;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    lodScatterKernel(const __grid_constant__ LodArgs a, const uint32_t* __restrict__ frontier,
+                     uint32_t* __restrict__ next) {
+  chainedKernelStart();
+  const LodState* st = a.state;
+  const uint32_t active = min(st->scatterActive, a.frontierCapacity);
+  const uint32_t countBase = st->scatterCount, packetBase = st->scatterPackets;
+  for (uint32_t t = blockIdx.x * kThreads + threadIdx.x; t < active; t += gridDim.x * kThreads) {
+    const uint4 local = a.offsets[t];
+    if (local.w & kDrop) continue;
+    const LodCluster node = loadCluster(a.clusters, frontier[t]);
+    const bool split = (local.w & kSplit) != 0;
+    if (split) {
+      if (local.x + node.childCount > a.frontierCapacity) {
+        atomicOr(a.error, SK_DEVERR_BOUNDS);
+      } else {
+        for (uint32_t k = 0; k < node.childCount; ++k) next[local.x + k] = node.childStart + k;
+      }
+    }
+    const uint32_t count = split ? node.leafCount : 1;
+    const uint32_t destination = countBase + local.y;
+    if (count > 32) {
+      if (packetBase + local.z < a.frontierCapacity)
+        a.packets[packetBase + local.z] = make_uint4(node.leafStart, count, destination, 1);
+      else
+        atomicOr(a.error, SK_DEVERR_BOUNDS);
+    } else if (destination + count > a.capacity) {
+      atomicOr(a.error, SK_DEVERR_BOUNDS);
+    } else if (!split) {
+      a.indices[destination] = node.node;
+    } else {
+      for (uint32_t k = 0; k < count; ++k) a.indices[destination + k] = a.leaves[node.leafStart + k];
+    }
   }
 }
 
@@ -375,8 +386,10 @@ cudaError_t launchLodSelect(const Camera* cam, const LodArgs& a, cudaStream_t st
     const uint32_t epoch = (a.epoch + 2 * level) & 0x3fffffffu;
     e = launchChained(lodEvaluateKernel, grid, kThreads, stream, cam, a, cur, epoch);
     if (e == cudaSuccess)
-      e = launchChained(lodCompactKernel, grid, kThreads, stream, a, cur, nxt, sums,
+      e = launchChained(lodCompactKernel, grid, kThreads, stream, a, cur, sums,
                         (epoch + 1) & 0x3fffffffu);
+    if (e == cudaSuccess)
+      e = launchChained(lodScatterKernel, min(grid * kItems, 148u * 8u), kThreads, stream, a, cur, nxt);
   }
   const uint32_t packetGrid = max(1u, min(a.frontierCapacity, 148u * 8u));
   if (e == cudaSuccess) e = launchChained(lodEmitKernel, packetGrid, kThreads, stream, a);

@@ -232,6 +232,7 @@ struct LodArgs {
   uint32_t frontierCapacity;
   uint32_t* frontier[2];
   uint2* costs;     // (extra | flags, exclusive prefix of extra)
+  uint4* offsets;   // (kids, splats, packets exclusive, flags)
   uint4* packets;   // (leafStart, count, destination, 1)
   uint32_t* indices;
   LodState* state;

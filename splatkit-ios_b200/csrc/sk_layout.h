@@ -95,6 +95,7 @@ static_assert(sizeof(LodCluster) == 64, "LodCluster is 64 bytes");
 struct LodState {
   uint32_t count, active, packets, accepted;
   uint32_t limited, evaluated, totalExtra, drops;
+  uint32_t scatterActive, scatterCount, scatterPackets, pad;
 };
 
 // Per-frame device counters the host reads back after a frame completes.

@@ -162,6 +162,7 @@ sk_status Batch::reserveLod(BatchLane& l, uint32_t indices, uint32_t frontier, u
   grab(l.lodFrontier[0], size_t{frontier} * 4);
   grab(l.lodFrontier[1], size_t{frontier} * 4);
   grab(l.lodCosts, size_t{frontier} * 8);
+  grab(l.lodOffsets, size_t{frontier} * 16);
   grab(l.lodPackets, size_t{frontier} * 16);
   grab(l.lodState, 256);
   grab(l.lodStatus, size_t{tiles} * 3 * 8);
@@ -372,6 +373,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     a.frontier[0] = static_cast<uint32_t*>(l.lodFrontier[0].ptr);
     a.frontier[1] = static_cast<uint32_t*>(l.lodFrontier[1].ptr);
     a.costs = static_cast<uint2*>(l.lodCosts.ptr);
+    a.offsets = static_cast<uint4*>(l.lodOffsets.ptr);
     a.packets = static_cast<uint4*>(l.lodPackets.ptr);
     a.indices = static_cast<uint32_t*>(l.lodIndices.ptr) + p.indexOffset;
     a.state = static_cast<LodState*>(l.lodState.ptr);

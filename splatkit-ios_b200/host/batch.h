@@ -66,7 +66,7 @@ struct BatchLane {
   CellListBatch cellBatch{};
   // LOD views: every view's cut, each view's six report words (LodState's first six), and the
   // selection scratch the views share in turn (sized for the largest)
-  DeviceBuffer lodIndices, lodReports, lodFrontier[2], lodCosts, lodPackets, lodState,
+  DeviceBuffer lodIndices, lodReports, lodFrontier[2], lodCosts, lodOffsets, lodPackets, lodState,
       lodStatus, lodCounters;
   uint32_t lodIndexCapacity = 0, lodFrontierCapacity = 0, lodReportViews = 0;
   std::vector<LodPlan> lodPlans;

@@ -189,6 +189,7 @@ sk_status Context::reserveLod(FrameScratch& f, const World& w, cudaStream_t s) {
   grab(f.lodFrontier[0], size_t{frontier} * 4);
   grab(f.lodFrontier[1], size_t{frontier} * 4);
   grab(f.lodCosts, size_t{frontier} * 8);
+  grab(f.lodOffsets, size_t{frontier} * 16);
   grab(f.lodPackets, size_t{frontier} * 16);
   grab(f.lodState, 256);
   grab(f.lodStatus, size_t{tiles} * 3 * 8);
@@ -297,6 +298,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     a.frontier[0] = static_cast<uint32_t*>(f.lodFrontier[0].ptr);
     a.frontier[1] = static_cast<uint32_t*>(f.lodFrontier[1].ptr);
     a.costs = static_cast<uint2*>(f.lodCosts.ptr);
+    a.offsets = static_cast<uint4*>(f.lodOffsets.ptr);
     a.packets = static_cast<uint4*>(f.lodPackets.ptr);
     a.indices = static_cast<uint32_t*>(f.lodIndices.ptr);
     a.state = static_cast<LodState*>(f.lodState.ptr);

@@ -91,7 +91,7 @@ struct FrameScratch {
   DeviceBuffer instKeys, instValues, instKeysSorted, instValuesSorted, tileSortWorkspace;
   DeviceBuffer ranges, rangeBuffer, rangeStarts, counters;
   DeviceBuffer cellLists;  // direct cell-major lists: block x cell counts and starts
-  DeviceBuffer lodIndices, lodFrontier[2], lodCosts, lodPackets, lodState, lodStatus,
+  DeviceBuffer lodIndices, lodFrontier[2], lodCosts, lodOffsets, lodPackets, lodState, lodStatus,
       lodCounters;
   uint32_t lodFrontierCapacity = 0;
   FrameScratch() = default;
