@@ -229,6 +229,8 @@ struct LodArgs {
   float colorWeight;
   uint32_t cull;
   uint32_t rounds;
+  uint32_t fanout;    // most child clusters of any cluster: round r's frontier holds at most
+                      // fanout^r clusters (0: unknown)
   uint32_t frontierCapacity;
   uint32_t* frontier[2];
   uint2* costs;     // (extra | flags, exclusive prefix of extra)

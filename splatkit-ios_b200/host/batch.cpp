@@ -211,6 +211,7 @@ sk_status Batch::prepare(BatchLane& l, const sk_batch_view* views, uint32_t coun
       plan.capacity = w.lodCapacity;
       plan.limit = ctx->lodLimit == 0 ? w.lodCapacity : std::min(ctx->lodLimit, w.lodCapacity);
       plan.rounds = w.rounds;
+      plan.fanout = w.lodFanout;
       plan.pixelLimit = ctx->threshold.pixels();
       plan.indexOffset = lodIndices;
       if (uint64_t{lodIndices} + n > 0x7fffffffu) return fail(SK_E_INVALID, "batch too large");
@@ -369,6 +370,7 @@ sk_status Batch::enqueueStages(BatchLane& l, bool clearStatus) {
     a.colorWeight = 4.0f;
     a.cull = policy.enable_frustum_culling ? 1u : 0u;
     a.rounds = p.rounds;
+    a.fanout = p.fanout;
     a.frontierCapacity = l.lodFrontierCapacity;
     a.frontier[0] = static_cast<uint32_t*>(l.lodFrontier[0].ptr);
     a.frontier[1] = static_cast<uint32_t*>(l.lodFrontier[1].ptr);

@@ -43,7 +43,7 @@ struct LodPlan {
   uint32_t view = 0;            // index in the submission
   const LodCluster* clusters = nullptr;
   const uint32_t* leaves = nullptr;
-  uint32_t clusterCount = 0, capacity = 0, limit = 0, rounds = 0;
+  uint32_t clusterCount = 0, capacity = 0, limit = 0, rounds = 0, fanout = 0;
   float pixelLimit = 1.0f;
   uint32_t indexOffset = 0;     // where its cut starts in the lane's index buffer
 };

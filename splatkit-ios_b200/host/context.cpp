@@ -294,6 +294,7 @@ sk_status Context::enqueuePipeline(FrameScratch& f, const ViewTarget& view, cons
     a.colorWeight = 4.0f;
     a.cull = policy.enable_frustum_culling ? 1u : 0u;
     a.rounds = world.rounds;
+    a.fanout = world.lodFanout;
     a.frontierCapacity = f.lodFrontierCapacity;
     a.frontier[0] = static_cast<uint32_t*>(f.lodFrontier[0].ptr);
     a.frontier[1] = static_cast<uint32_t*>(f.lodFrontier[1].ptr);
@@ -886,6 +887,7 @@ sk_status sk_upload_lod_world(sk_context* handle, const sk_lod_view* tree, int32
   fresh.clusterCount = static_cast<uint32_t>(clusters.size());
   fresh.leafRefCount = static_cast<uint32_t>(leaves.size());
   fresh.rounds = static_cast<uint32_t>(depth) + 1;
+  for (const sk::LodCluster& c : clusters) fresh.lodFanout = std::max(fresh.lodFanout, c.childCount);
   fresh.lodCapacity = capacity;
   st = ctx->reserveLod(ctx->scratch, fresh, ctx->stream);
   if (st != SK_OK) return st;

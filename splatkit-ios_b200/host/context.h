@@ -81,6 +81,7 @@ struct World {
   bool lod = false;
   DeviceBuffer clusters, leaves;
   uint32_t clusterCount = 0, leafRefCount = 0, rounds = 0, lodCapacity = 0;
+  uint32_t lodFanout = 0;  // most child clusters of any cluster
 };
 
 // Everything one pipeline run writes besides its outputs; reused frame after frame on one
