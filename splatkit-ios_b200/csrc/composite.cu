@@ -116,8 +116,9 @@ __device__ __forceinline__ float exp2Approx(float x) {
 // Both pixels against one splat. px = the two pixel centres' x; m01dy, m11dy = m01 dy and
 // m11 dy, shared by the row. The coverage terms u, v, q are the oracle's FP32 sequence per pixel
 // (px - cx is px + (-cx) exactly); an uncovered or finished pixel takes alpha 0, which leaves
-// its colour and transmittance bit for bit as they were. alpha = min(1, 2^(log2 peak - q log2(e) / 2))
-// and T -= T alpha.
+// its colour and transmittance bit for bit as they were, so a warp none of whose pixels the splat
+// covers runs the blend all the same (no vote: the unrolled sweep keeps no branch between
+// entries). alpha = min(1, 2^(log2 peak - q log2(e) / 2)) and T -= T alpha.
 template <bool kCount>
 __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const float4 w1,
                                           const float4 c, float2 px, float m01dy, float m11dy,
@@ -132,7 +133,6 @@ __device__ __forceinline__ void blendPair(PixelPair& p, const float4 w0, const f
   // still fails as the separate bounds would)
   const bool c0 = p.T.x >= cutoff && fmaxf(fabsf(u.x), fabsf(v.x)) <= w1.z && q.x <= w1.w;
   const bool c1 = p.T.y >= cutoff && fmaxf(fabsf(u.y), fabsf(v.y)) <= w1.z && q.y <= w1.w;
-  if (!__any_sync(0xffffffffu, c0 || c1)) return;  // the whole quadrant misses this splat
   const float2 e = __ffma2_rn(q, pair(-0.7213475204444817f), pair(c.x));  // -q log2(e) / 2
   const float a0 = c0 ? fminf(exp2Approx(e.x), 1.0f) : 0.0f;
   const float a1 = c1 ? fminf(exp2Approx(e.y), 1.0f) : 0.0f;
