@@ -209,3 +209,39 @@ def test_overlapped_frames_equal_frames_drawn_alone(cuda_device):
     stats = r.stats()
     r.close()
     assert stats["submitted_frames"] == stats["completed_frames"] == len(frames) + 3
+
+
+@pytest.mark.gpu
+def test_a_lod_world_after_overlapped_flat_frames_reads_back_its_own_frames(cuda_device):
+    # flat frames in flight on both slots, then a LOD world (one slot): its cut, survivors, order
+    # and image are a fresh renderer's, not what the second slot's scratch last held
+    w, h = 320, 240
+    flat = synthetic.random_cloud(60_000, seed=3, sh_degree=1)
+    cloud = synthetic.clustered_cloud(24, 400, seed=5, half_extent=8.0, rms=1.0)
+    pos = np.asarray(cloud.positions, np.float32)
+    cloud.bounds_min, cloud.bounds_max = pos.min(axis=0), pos.max(axis=0)
+    tree = sk.build_lod_tree(cloud)
+    used = sk.Renderer(w, h, image_format=sk.FORMAT_RGBA8)
+    used.upload_world(flat, 1)
+    for f in frames_for(flat, w, h, range(0, 30, 5)):
+        used.draw(f)
+    fresh = sk.Renderer(w, h, image_format=sk.FORMAT_RGBA8)
+    for r in (used, fresh):
+        r.apply_render_policy(sk.Policy(lod_error_pixels=1.5, sort_depth_bits=16))
+        r.upload_lod_world(tree, 0, 100_000)
+    for step in (0, 7, 13):
+        view, eye = skcam.orbit_view(step, radius=12.0)
+        frame = sk.Frame(view, skcam.perspective(math.radians(60.0), w / h, 0.05, 200.0), eye, [], 0)
+        got = []
+        for r in (used, fresh):
+            r.draw(frame)
+            cut, _ = r.read_cut()
+            keys, projected = r.read_visible()
+            got.append((cut, keys, projected.tobytes(), r.read_order(), r.read_image(sk.FORMAT_RGBA8)))
+        (cut, keys, projected, order, image), want = got
+        assert len(cut) > 0 and len(keys) > 0
+        assert np.array_equal(cut, want[0]) and np.array_equal(keys, want[1])
+        assert projected == want[2] and np.array_equal(order, want[3])
+        assert np.array_equal(image, want[4])
+    used.close()
+    fresh.close()
