@@ -3,7 +3,7 @@
 // Binning + a stable sort of (cell, projected index) pairs by cell + a ranges pass build the
 // same lists (binning.cu, radix_sort.cu). On a target of at most kDirectMaxCells cells this file
 // builds them without the sort:
-//   1. count: every block of 512 depth ranks histograms its instances by cell;
+//   1. count: every block of 512 depth ranks (1024 in a batch) histograms its instances by cell;
 //   2. scan: per cell, the running sum of the block histograms (32 cells per block of this pass,
 //      the rows held in registers) gives each block's first slot in the cell's list; the lists'
 //      starts come from a decoupled look-back across the groups of 32 cells, in cell order; the
@@ -33,10 +33,11 @@ namespace {
 
 constexpr uint32_t kThreads = 256;
 constexpr uint32_t kWarps = kThreads / 32;
-constexpr uint32_t kItems = 2;                    // ranks per lane
-constexpr uint32_t kChunk = 32 * kItems;          // ranks per warp
-constexpr uint32_t kBlockRanks = kThreads * kItems;  // 512: twice the blocks of 1024-rank ones,
-                                                     // 100.8 -> 81.8 us for the three passes
+// Ranks per lane: a frame's blocks take 512 depth ranks (100.8 -> 81.8 us for the three passes
+// against 1024-rank blocks), a batch's 1024 (it holds every view's block rows at once, and twice
+// the rows cost the 64-view batch more than the smaller blocks save).
+constexpr uint32_t kFrameItems = 2;
+constexpr uint32_t kBatchItems = 4;
 constexpr uint32_t kScanThreads = 1024;
 constexpr uint32_t kScanWarps = kScanThreads / 32;
 constexpr uint32_t kRowsInRegisters = 32;         // block rows one scan warp keeps
@@ -64,7 +65,9 @@ struct Job {
 __host__ __device__ inline uint32_t cellWords(uint32_t cells) { return (cells + 1) / 2; }
 __host__ __device__ inline size_t align16(size_t n) { return (n + 15) & ~size_t{15}; }
 __host__ __device__ inline uint32_t cellGroups(uint32_t cells) { return (cells + 31) / 32; }
+template <uint32_t kItems>
 __host__ __device__ inline uint32_t blocksFor(uint32_t capacity) {
+  constexpr uint32_t kBlockRanks = kThreads * kItems;
   return (capacity + kBlockRanks - 1) / kBlockRanks;
 }
 
@@ -113,8 +116,10 @@ size_t workBytes(uint32_t blocks, uint32_t cells) {
 }
 
 // Pass 1: each block's instances per cell.
+template <uint32_t kItems>
 __global__ void __launch_bounds__(kThreads)
     cellCountKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells) {
+  constexpr uint32_t kBlockRanks = kThreads * kItems;
   chainedKernelStart();
   __shared__ uint32_t hist[kDirectMaxCells];
   const Job job = jobOf(a, work, cells, blockIdx.x, false, nullptr);
@@ -146,6 +151,7 @@ __global__ void __launch_bounds__(kThreads)
 // Pass 2: one block per group of 32 cells (groups handed out in start order, so a group only
 // waits on groups already running). Lane = cell of the group; warp w scans a contiguous share
 // of the block rows, the first 32 of them kept in registers between the two sweeps.
+template <uint32_t kItems>
 __global__ void __launch_bounds__(kScanThreads, 1)
     cellScanKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells, uint2* ranges,
                    uint32_t* counters, uint32_t epoch, uint32_t* error) {
@@ -155,7 +161,7 @@ __global__ void __launch_bounds__(kScanThreads, 1)
   const uint32_t group = takeTile(counters);  // over all views of a batch
   const Job job = jobOf(a, work, cells, group, true, ranges);
   cells = job.cells;
-  const uint32_t active = blocksFor(job.n);
+  const uint32_t active = blocksFor<kItems>(job.n);
   const uint32_t warp = threadIdx.x >> 5, lane = laneId();
   const uint32_t cell = job.block * 32 + lane;
   const bool valid = cell < cells;
@@ -257,14 +263,17 @@ __device__ __forceinline__ void visitPositions(const uint4 s, uint32_t tilesX, u
 }
 
 // Pass 3. Dynamic shared memory: kWarps x words per-warp slot counters (16-bit halves: a warp's
-// slots count from the block's first slot in the cell, at most 512 on), then each cell's first
+// slots count from the block's first slot in the cell, at most 1024 on), then each cell's first
 // slot for the block. A warp's entries, in depth order, are staged as (cell, item) pairs kWindow
 // positions at a time: the counting walk stages the first window, and a warp with more entries
 // walks its items again for each further one.
 constexpr uint32_t kWindow = 1024;
 
+template <uint32_t kItems>
 __global__ void __launch_bounds__(kThreads)
     cellEmitKernel(const __grid_constant__ BinArgs a, Work work, uint32_t cells) {
+  constexpr uint32_t kChunk = 32 * kItems;  // ranks per warp
+  constexpr uint32_t kBlockRanks = kThreads * kItems;
   chainedKernelStart();
   extern __shared__ uint32_t cellSmem[];
   __shared__ uint32_t stageValue[kWarps][kChunk];
@@ -392,15 +401,18 @@ bool cellListsFit(uint32_t capacity, uint32_t cells) {
 }
 
 size_t cellListBytes(uint32_t capacity, uint32_t cells) {
-  return workBytes(blocksFor(std::max(capacity, 1u)), std::max(cells, 1u));
+  return workBytes(blocksFor<kFrameItems>(std::max(capacity, 1u)), std::max(cells, 1u));
 }
 
 cudaError_t cellListsConfigure() {
   static bool configured = false;
   if (configured) return cudaSuccess;
-  const cudaError_t e =
-      cudaFuncSetAttribute(cellEmitKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e =
+      cudaFuncSetAttribute(cellEmitKernel<kFrameItems>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(emitDynamicBytes(kDirectMaxCells)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(cellEmitKernel<kBatchItems>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(emitDynamicBytes(kDirectMaxCells)));
   if (e == cudaSuccess) configured = true;
   return e;
 }
@@ -411,18 +423,18 @@ cudaError_t launchCellLists(const BinArgs& a, const CellLists& lists, cudaStream
     return cudaErrorInvalidValue;
   cudaError_t e = cellListsConfigure();
   if (e != cudaSuccess) return e;
-  const uint32_t blocks = blocksFor(a.capacity);
+  const uint32_t blocks = blocksFor<kFrameItems>(a.capacity);
   const Work work = workOf(lists.workspace, blocks, cells);
-  e = launchChained(cellCountKernel, blocks, kThreads, stream, a, work, cells);
+  e = launchChained(cellCountKernel<kFrameItems>, blocks, kThreads, stream, a, work, cells);
   if (e != cudaSuccess) return e;
-  e = launchChained(cellScanKernel, cellGroups(cells), kScanThreads, stream, a, work, cells,
+  e = launchChained(cellScanKernel<kFrameItems>, cellGroups(cells), kScanThreads, stream, a, work, cells,
                     lists.ranges, lists.counters, lists.epoch, lists.error);
   if (e != cudaSuccess) return e;
-  return launchChainedShared(cellEmitKernel, blocks, kThreads, emitDynamicBytes(cells), stream, a,
+  return launchChainedShared(cellEmitKernel<kFrameItems>, blocks, kThreads, emitDynamicBytes(cells), stream, a,
                              work, cells);
 }
 
-uint32_t cellListBlocks(uint32_t capacity) { return blocksFor(std::max(capacity, 1u)); }
+uint32_t cellListBlocks(uint32_t capacity) { return blocksFor<kBatchItems>(std::max(capacity, 1u)); }
 
 size_t cellListRowBytes(uint32_t capacity, uint32_t cells) {
   return align16(size_t{cellListBlocks(capacity)} * cells * 4);
@@ -441,12 +453,12 @@ cudaError_t launchCellListsBatch(const BinArgs& a, const CellListBatch& lists, c
   work.viewFirst = lists.viewFirst;
   work.base = static_cast<uint8_t*>(lists.workspace);
   const uint32_t cells = lists.mostCells;  // each block reads its own view's from the table
-  e = launchChained(cellCountKernel, lists.blocks, kThreads, stream, a, work, cells);
+  e = launchChained(cellCountKernel<kBatchItems>, lists.blocks, kThreads, stream, a, work, cells);
   if (e != cudaSuccess) return e;
-  e = launchChained(cellScanKernel, lists.groups, kScanThreads, stream, a, work, cells,
+  e = launchChained(cellScanKernel<kBatchItems>, lists.groups, kScanThreads, stream, a, work, cells,
                     lists.ranges, lists.counters, lists.epoch, lists.error);
   if (e != cudaSuccess) return e;
-  return launchChainedShared(cellEmitKernel, lists.blocks, kThreads, emitDynamicBytes(cells),
+  return launchChainedShared(cellEmitKernel<kBatchItems>, lists.blocks, kThreads, emitDynamicBytes(cells),
                              stream, a, work, cells);
 }
 

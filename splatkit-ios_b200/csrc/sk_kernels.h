@@ -147,7 +147,7 @@ cudaError_t launchTileRanges(const uint32_t* sortedKeys, const uint32_t* instanc
 
 // Direct cell-major lists (cell_lists.cu): the per-cell lists that binning + stable tile sort +
 // ranges produce, written in place on targets of at most kDirectMaxCells binning cells. A count
-// pass histograms every block of 512 depth ranks by cell, a scan pass turns the histograms
+// pass histograms every block of 512 depth ranks (1024 in a batch) by cell, a scan pass turns the histograms
 // into each block's first position in every cell's list (and the lists' ranges, by look-back
 // across groups of cells), and the emission pass writes each instance there in depth order.
 // args.instanceValues receives the lists; instanceKeys and blockSums are unused.
