@@ -32,7 +32,8 @@ namespace sk {
 namespace {
 
 constexpr uint32_t kThreads = 256;
-constexpr uint32_t kItems = 4;
+constexpr uint32_t kItems = 2;  // 512 clusters per tile: 0.229 -> 0.189 ms of walk selection
+                                // against 1024
 constexpr uint32_t kTileClusters = kThreads * kItems;
 constexpr uint32_t kSplit = 0x80000000u;
 constexpr uint32_t kDrop = 0x40000000u;
