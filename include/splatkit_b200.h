@@ -383,7 +383,10 @@ sk_status sk_batch_set_tuning(sk_batch* batch, const sk_batch_tuning* tuning);
  * is priced at the scene's cut capacity; its cut is selected with the scene's LOD threshold,
  * which every completed request of the scene then adapts (LodThreshold::update,
  * splatkit-engine/include/splatkit/rendering/LodThreshold.h:27-36), as the scene's own frames
- * would. Results equal sk_draw's for the same view (16-bit depth keys, default policy). */
+ * would. Results equal sk_draw's for the same view (16-bit depth keys, default policy).
+ * At creation the server gives the device's memory pool its lanes' working size (about 192
+ * bytes per drawn record of max_batch_splats per lane, at most a quarter of memory_budget), so
+ * lanes that grow while requests wait take pooled memory instead of a driver allocation. */
 typedef struct sk_server sk_server;
 
 typedef struct {

@@ -266,6 +266,18 @@ sk_status sk_server_create(const sk_server_config* config, sk_server** out) {
   }
   s->work = std::vector<sk::LaneWork>(config->lanes);
   sk::holdPooledMemory(config->device);
+  // The lanes grow from the device's memory pool; give the pool their working size now (one
+  // driver allocation here, not while requests wait): about 192 bytes per drawn record of
+  // max_batch_splats per lane, within a quarter of the memory budget.
+  {
+    const uint64_t want = std::min<uint64_t>(uint64_t{config->lanes} * config->max_batch_splats * 192,
+                                             config->memory_budget / 4);
+    cudaStream_t first = s->batch.lanes[0].stream;
+    void* block = nullptr;
+    if (want > 0 && cudaMallocAsync(&block, want, first) == cudaSuccess) cudaFreeAsync(block, first);
+    cudaGetLastError();  // the pool simply starts empty when that fails
+    cudaStreamSynchronize(first);
+  }
   Server* raw = s.get();
   s->scheduler = std::thread([raw] { raw->run(); });
   *out = reinterpret_cast<sk_server*>(s.release());
